@@ -1,0 +1,239 @@
+/*
+ * hamlss.h -- C ABI of the B200 sparse iterative solve engine.
+ *
+ * This is the drop-in boundary for the HAMLSS solve path (namespace `hsps` in the
+ * reference C++17 code).  The reference has no FFI of its own: its path sits behind
+ * plain C++ virtual classes.  Each entry point below replaces one of those calls and
+ * cites it as `file:line` inside the reference project:
+ *
+ *   SparseMatrix / Vector        include/core/sparse_matrix.hpp:34-170, include/core/vector.hpp:16-69
+ *   SolverBase::solve            include/solvers/solver_base.hpp:32-35
+ *   PreconditionerBase           include/preconditioners/preconditioner_base.hpp:16-48
+ *   SolverFactory                include/solvers/solver_factory.hpp:40-88
+ *   AdaptiveSelector             include/adaptive/adaptive_selector.hpp:49-161
+ *
+ * Conventions
+ *   - Every function returns an int status: HAMLSS_OK (0) or a negative error code.
+ *     hamlss_last_error() returns a thread-local message for the last failure.
+ *   - Non-convergence is NOT an error (as in the reference, where solve() returns
+ *     false): the call returns HAMLSS_OK and stats->converged == 0.
+ *   - Matrices are CSR with int32 row pointers / column indices and FP64 values,
+ *     columns sorted inside each row (what SparseMatrix::from_coo produces).
+ *   - Vector arguments are host pointers when `where == HAMLSS_HOST`, device
+ *     pointers on the context's device when `where == HAMLSS_DEVICE`.
+ *   - A context owns one CUDA stream.  Calls on one context are serialised by the
+ *     caller; different contexts may be used from different threads.
+ */
+#ifndef HAMLSS_H
+#define HAMLSS_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status codes */
+enum {
+    HAMLSS_OK              = 0,
+    HAMLSS_ERR_INVALID     = -1,  /* bad argument / unknown name (std::invalid_argument)        */
+    HAMLSS_ERR_SIZE        = -2,  /* dimension mismatch (vector.cpp:42, sparse_matrix.cpp:69)    */
+    HAMLSS_ERR_ZERO_DIAG   = -3,  /* Jacobi zero diagonal (jacobi.cpp:28-30)                     */
+    HAMLSS_ERR_ZERO_PIVOT  = -4,  /* ILU near-zero pivot (ilu.cpp:65-67, ilu.cpp:257-259)        */
+    HAMLSS_ERR_CUDA        = -5,  /* CUDA runtime failure                                         */
+    HAMLSS_ERR_NOMEM       = -6,  /* device allocation failed                                     */
+    HAMLSS_ERR_NOT_READY   = -7,  /* preconditioner used before setup                             */
+    HAMLSS_ERR_TIMEOUT     = -8,  /* a bounded device-side wait ran out                           */
+    HAMLSS_ERR_NONFINITE   = -9,  /* NaN / Inf in an input vector or matrix                       */
+    HAMLSS_ERR_BUDGET      = -10, /* request does not fit the memory budget                       */
+    HAMLSS_ERR_MALFORMED   = -11, /* CSR not well formed (row_ptr, bounds, unsorted columns)      */
+    HAMLSS_ERR_CANCELLED   = -12  /* serving request cancelled before it ran                      */
+};
+
+enum { HAMLSS_HOST = 0, HAMLSS_DEVICE = 1 };
+
+/* Same numeric values as hsps::SolverType / PrecondType / AdaptiveState
+ * (include/core/types.hpp:30-54). */
+enum { HAMLSS_SOLVER_CG = 0, HAMLSS_SOLVER_FGMRES = 1, HAMLSS_SOLVER_BICGSTAB = 2,
+       HAMLSS_SOLVER_SSTEP_CG = 3, HAMLSS_SOLVER_ASYNC_FGMRES = 4 };
+enum { HAMLSS_PREC_NONE = 0, HAMLSS_PREC_JACOBI = 1, HAMLSS_PREC_ILU = 2, HAMLSS_PREC_AMG = 3,
+       HAMLSS_PREC_BLOCK_JACOBI = 4, HAMLSS_PREC_CHEBYSHEV = 5 };
+enum { HAMLSS_STATE_EASY = 0, HAMLSS_STATE_MODERATE = 1, HAMLSS_STATE_HARD = 2 };
+
+/* Arithmetic of the inner solve. */
+enum { HAMLSS_FP64 = 0,        /* everything FP64, iteration-for-iteration like the reference      */
+       HAMLSS_MIXED = 1 };     /* FP32 values/vectors inside an FP64 iterative-refinement loop      */
+
+/* ------------------------------------------------------------------ parameters
+ * Field-for-field mirror of hsps::SolverParams (include/core/types.hpp:119-143),
+ * followed by engine fields that have no counterpart there.
+ * hamlss_params_default() fills the reference defaults. */
+typedef struct hamlss_params {
+    double  tol;              /* 1e-8   relative residual tolerance              */
+    int32_t max_iter;         /* 2000   Krylov iteration budget                  */
+    int32_t restart_size;     /* 50     FGMRES restart length m                  */
+    double  drop_tol;         /* 1e-4   ILU threshold; 0 selects ILU(0)          */
+    int32_t amg_levels;       /* 10     maximum hierarchy depth                  */
+    double  amg_strength;     /* 0.25                                            */
+    double  amg_strong;       /* 0.25   strength threshold the factory forwards  */
+    int32_t amg_smooth_pre;   /* 2                                               */
+    int32_t amg_smooth_post;  /* 2                                               */
+    int32_t stall_window;     /* 15                                              */
+    double  stall_threshold;  /* 0.95                                            */
+    int32_t verbose;          /* 0                                               */
+    int32_t print_every;      /* 25                                              */
+    int32_t sstep_k;          /* 1                                               */
+    double  sstep_cond_tol;   /* 1e12                                            */
+    int32_t async_enabled;    /* 0                                               */
+    int32_t async_max_stale;  /* 3                                               */
+    int32_t fill_per_row;     /* 0                                               */
+    int32_t block_size;       /* 1                                               */
+    int32_t record_hw_energy; /* 0  1: read the NVML energy counter around solves */
+    /* ---- engine fields ---- */
+    int32_t precision;        /* HAMLSS_FP64 (default) or HAMLSS_MIXED                       */
+    double  ir_inner_tol;     /* relative reduction asked of each FP32 inner solve (1e-5)    */
+    int32_t ir_max_outer;     /* cap on refinement steps (30)                                */
+    double  amg_omega;        /* AMG Jacobi damping; reference value 0.67 (amg.hpp:101)      */
+    int32_t amg_coarse_limit; /* direct solve at or below this many rows; reference 50       */
+    double  jacobi_omega;     /* Jacobi preconditioner damping; reference 1.0 (jacobi.hpp:33) */
+    int32_t ladder_mode;      /* 0: escalate when an attempt exhausts max_iter (reference)   */
+                              /* 1: also escalate on the device-side stall / budget checks   */
+    int32_t check_every;      /* iterations between device->host convergence polls (8)      */
+} hamlss_params;
+
+/* ----------------------------------------------------------------- statistics
+ * Field-for-field mirror of hsps::SolverStats (include/core/types.hpp:91-114),
+ * followed by engine fields. */
+typedef struct hamlss_stats {
+    int32_t iterations;
+    double  initial_residual;
+    double  final_residual;
+    int32_t converged;
+    double  solve_time_s;
+    double  setup_time_s;
+    double  energy_joules;    /* proxy model 2e-10 J/flop + 5e-9 J/byte (cg_solver.cpp:186-188) */
+    int64_t flop_count;
+    int64_t mem_bytes;
+    int32_t solver_used;
+    int32_t precond_used;
+    int32_t state_used;
+    int32_t restarts;
+    double  energy_joules_hw; /* NVML total-energy delta around the solve (0 if unavailable) */
+    double  rapl_start_j;
+    double  rapl_end_j;
+    int32_t sstep_k;
+    int32_t async_mode;
+    int64_t comm_bytes;
+    double  comm_time_s;
+    /* ---- engine fields ---- */
+    double  true_residual;    /* ||b - A x|| / ||b|| in FP64 after the solve                 */
+    int32_t outer_iterations; /* refinement steps (HAMLSS_MIXED), else 1                     */
+    int32_t status;           /* 0 ok, else the HAMLSS_ERR_* that ended the solve            */
+    double  device_time_s;    /* CUDA-event time of the solve on the context stream          */
+} hamlss_stats;
+
+/* Escalation log entry; mirrors hsps::EscalationRecord (adaptive_selector.hpp:38-44). */
+typedef struct hamlss_escalation {
+    int32_t at_iteration;
+    int32_t from_state;
+    int32_t to_state;
+    double  residual_at_escalation;
+    int32_t reason;           /* 0 attempt exhausted max_iter, 1 stall, 2 budget, 3 divergence */
+} hamlss_escalation;
+
+typedef struct hamlss_ctx  hamlss_ctx;
+typedef struct hamlss_mat  hamlss_mat;
+typedef struct hamlss_prec hamlss_prec;
+
+/* ------------------------------------------------------------------- library */
+const char* hamlss_version(void);
+const char* hamlss_last_error(void);
+void        hamlss_params_default(hamlss_params* p);
+
+/* ------------------------------------------------------------------- context */
+int hamlss_ctx_create(int device, hamlss_ctx** out);
+int hamlss_ctx_destroy(hamlss_ctx* ctx);
+int hamlss_ctx_synchronize(hamlss_ctx* ctx);
+/* The context's cudaStream_t, as an opaque pointer, so callers can order their own work. */
+int hamlss_ctx_stream(hamlss_ctx* ctx, void** stream);
+
+/* -------------------------------------------------------------------- matrix
+ * Replaces hsps::SparseMatrix(rows, cols, row_ptr, col_idx, values)
+ * (sparse_matrix.cpp:22-27): a deep copy into device memory.  The engine keeps the
+ * FP64 values and derives an FP32 copy on first use by a mixed-precision solve.
+ * The CSR is validated on the device (row_ptr monotone, column bounds, sorted rows);
+ * a malformed matrix returns HAMLSS_ERR_MALFORMED. */
+int hamlss_mat_upload(hamlss_ctx* ctx, int32_t rows, int32_t cols, int32_t nnz,
+                      const int32_t* row_ptr, const int32_t* col_idx, const double* values,
+                      int where, hamlss_mat** out);
+int hamlss_mat_update_values(hamlss_mat* A, const double* values, int where);
+int hamlss_mat_info(const hamlss_mat* A, int32_t* rows, int32_t* cols, int32_t* nnz);
+int hamlss_mat_download(const hamlss_mat* A, int32_t* row_ptr, int32_t* col_idx, double* values);
+int hamlss_mat_release(hamlss_mat* A);
+
+/* y = A x.  Replaces SparseMatrix::spmv (sparse_matrix.cpp:68-87). */
+int hamlss_spmv(hamlss_ctx* ctx, const hamlss_mat* A, const double* x, double* y, int where);
+
+/* Vector BLAS-1 on device pointers.  Replace Vector::dot / norm2 / axpy / axpby / scale
+ * (vector.cpp:39-89).  Results of reductions land in host memory. */
+int hamlss_dot(hamlss_ctx* ctx, int32_t n, const double* x, const double* y, double* result);
+int hamlss_norm2(hamlss_ctx* ctx, int32_t n, const double* x, double* result);
+int hamlss_axpy(hamlss_ctx* ctx, int32_t n, double alpha, const double* x, double* y);
+int hamlss_axpby(hamlss_ctx* ctx, int32_t n, double a, const double* x, double b, double* y);
+int hamlss_scale(hamlss_ctx* ctx, int32_t n, double alpha, double* x);
+
+/* ------------------------------------------------------------ preconditioners
+ * Replaces SolverFactory::make_precond (solver_factory.cpp:54-97) followed by
+ * PreconditionerBase::setup.  kind = HAMLSS_PREC_*; HAMLSS_PREC_NONE yields *out == NULL
+ * like the reference's nullptr.  HAMLSS_PREC_ILU with params->drop_tol > 0 or
+ * fill_per_row > 0 is ILUT in the reference (ilu.cpp:31-36); the engine implements
+ * ILU(0) only and returns HAMLSS_ERR_INVALID for that request. */
+int hamlss_precond_setup(hamlss_ctx* ctx, const hamlss_mat* A, int kind,
+                         const hamlss_params* params, hamlss_prec** out, double* setup_time_s);
+/* z = M^-1 r.  Replaces PreconditionerBase::apply (preconditioner_base.hpp:32). */
+int hamlss_precond_apply(hamlss_ctx* ctx, const hamlss_prec* M, const double* r, double* z,
+                         int where);
+int hamlss_precond_type(const hamlss_prec* M, int32_t* kind);
+int hamlss_precond_release(hamlss_prec* M);
+
+/* --------------------------------------------------------------------- solve
+ * Replaces SolverBase::solve (solver_base.hpp:32-35) for CGSolver (cg_solver.cpp:37-191)
+ * and FGMRESSolver (fgmres_solver.cpp:165-241).  x holds the initial guess on entry
+ * and the solution on exit.  M may be NULL (no preconditioner). */
+int hamlss_solve(hamlss_ctx* ctx, int solver, const hamlss_mat* A, const hamlss_prec* M,
+                 const double* b, double* x, int where, const hamlss_params* params,
+                 hamlss_stats* stats);
+
+/* Replaces AdaptiveSelector::solve (adaptive_selector.cpp:298-394): features, initial
+ * state, then the CG+Jacobi -> FGMRES+ILU(0) -> FGMRES+AMG ladder with warm starts.
+ * `log` receives up to `log_cap` escalation records; *n_log their count. */
+int hamlss_solve_adaptive(hamlss_ctx* ctx, const hamlss_mat* A, const double* b, double* x,
+                          int where, const hamlss_params* params, hamlss_stats* stats,
+                          hamlss_escalation* log, int32_t log_cap, int32_t* n_log,
+                          int32_t* initial_state);
+
+/* AdaptiveSelector::extract_features + select_initial_state (adaptive_selector.cpp:37-233):
+ * the 24-entry feature vector of MatrixFeatures::to_feature_vector (:418-446). */
+int hamlss_extract_features(hamlss_ctx* ctx, const hamlss_mat* A, double features[24],
+                            int32_t* initial_state);
+
+/* ------------------------------------------------------- inspection (parity)
+ * Internals that the reference keeps private but that parity is checked on. */
+/* Greedy aggregation of one matrix (amg.cpp:30-67): agg[rows]; returns the count. */
+int hamlss_amg_aggregate(hamlss_ctx* ctx, const hamlss_mat* A, double theta,
+                         int32_t* agg, int32_t* n_agg);
+int hamlss_amg_num_levels(const hamlss_prec* M, int32_t* levels);
+/* Level `l` of the hierarchy: which = 0 A, 1 P, 2 R.  Pass NULL arrays to query sizes. */
+int hamlss_amg_level_matrix(const hamlss_prec* M, int32_t level, int32_t which,
+                            int32_t* rows, int32_t* cols, int32_t* nnz,
+                            int32_t* row_ptr, int32_t* col_idx, double* values);
+/* ILU(0) factor values in the pattern of A (ilu.cpp:41-89's lu_val_). */
+int hamlss_ilu_factors(const hamlss_prec* M, double* lu_values);
+/* Level sets of the lower (which = 0) or upper (which = 1) triangle of an ILU(0)
+ * preconditioner: level[rows]; *n_levels their count. */
+int hamlss_ilu_levels(const hamlss_prec* M, int32_t which, int32_t* level, int32_t* n_levels);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HAMLSS_H */

@@ -1,0 +1,221 @@
+"""Pin the oracle (oracle/oracle.c) before trusting it.
+
+1. The reference's own known-answer tests (tests/test_sparse_matrix.cpp,
+   test_preconditioners.cpp, test_solvers.cpp in the reference project), restated.
+2. The committed golden fixtures (tests/golden/*.npz, written by the reference itself).
+3. Where the reference is built from source here (oracle/_ref), bit-for-bit agreement
+   with it on fresh seeded inputs.
+CPU only.
+"""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+from hsps_b200 import problems as P
+from hsps_b200._abi import default_params
+
+GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.npz")))
+
+
+def coo_csr(rows, r, c, v):
+    order = np.lexsort((c, r))
+    r, c, v = np.asarray(r)[order], np.asarray(c)[order], np.asarray(v, float)[order]
+    rp = np.zeros(rows + 1, np.int32)
+    np.add.at(rp, np.asarray(r) + 1, 1)
+    return np.cumsum(rp).astype(np.int32), c.astype(np.int32), v
+
+
+# ------------------------------------------------------------ reference KATs, restated
+
+def test_kat_spmv_identity_and_tridiag(orc):
+    # test_sparse_matrix.cpp:28-64
+    rp, ci, v = coo_csr(4, range(4), range(4), [1.0] * 4)
+    assert np.array_equal(orc.spmv(rp, ci, v, [1.0, 2.0, 3.0, 4.0]), [1.0, 2.0, 3.0, 4.0])
+    r, c, vals = [], [], []
+    for i in range(4):
+        for j, a in ((i - 1, -1.0), (i, 2.0), (i + 1, -1.0)):
+            if 0 <= j < 4:
+                r.append(i); c.append(j); vals.append(a)
+    rp, ci, v = coo_csr(4, r, c, vals)
+    assert np.allclose(orc.spmv(rp, ci, v, np.ones(4)), [1.0, 0.0, 0.0, 1.0])
+
+
+def test_kat_poisson_symmetric_diag4(orc):
+    # test_sparse_matrix.cpp:66-78
+    rp, ci, v = orc.poisson_2d(8)
+    rows = np.repeat(np.arange(64), np.diff(rp))
+    dense = np.zeros((64, 64))
+    dense[rows, ci] = v
+    assert np.array_equal(dense, dense.T)
+    assert np.all(np.diag(dense) == 4.0)
+
+
+def test_kat_convdiff_nonsymmetric(orc):
+    # test_sparse_matrix.cpp:113-117
+    rp, ci, v = orc.convdiff_2d(8, 0.1, 1.0, 0.5)
+    rows = np.repeat(np.arange(64), np.diff(rp))
+    dense = np.zeros((64, 64))
+    dense[rows, ci] = v
+    assert not np.array_equal(dense, dense.T)
+
+
+def test_kat_cg_1x1_and_diagonal(orc):
+    # test_solvers.cpp:42-76
+    p = default_params(tol=1e-9, max_iter=3000, restart_size=40)
+    rc, x, s = orc.solve(0, 1, [0, 1], [0], [2.0], [4.0], params=p)
+    assert rc == 1 and abs(x[0] - 2.0) < 1e-10
+    rp, ci, v = coo_csr(4, range(4), range(4), [2.0, 3.0, 5.0, 7.0])
+    rc, x, s = orc.solve(0, 1, rp, ci, v, [4.0, 9.0, 15.0, 21.0], params=p)
+    assert np.allclose(x, [2.0, 3.0, 3.0, 3.0], atol=1e-10)
+
+
+def test_kat_cg_zero_rhs_and_poisson(orc):
+    # test_solvers.cpp:78-129
+    p = default_params(tol=1e-9, max_iter=3000, restart_size=40)
+    A = orc.poisson_2d(8)
+    rc, x, s = orc.solve(0, 1, *A, np.zeros(64), params=p)
+    assert rc == 1 and s.iterations == 0
+    A = orc.poisson_2d(16)
+    b = np.ones(256)
+    rc, x, s = orc.solve(0, 1, *A, b, params=p)
+    r = b - orc.spmv(*A, x)
+    assert rc == 1 and np.linalg.norm(r) / np.linalg.norm(b) < 1e-8
+    rc2, x2, s2 = orc.solve(0, 2, *A, b, params=default_params(tol=1e-9, max_iter=3000, drop_tol=0.0))
+    assert s2.iterations < s.iterations
+
+
+def test_kat_jacobi(orc):
+    # test_preconditioners.cpp:26-58
+    rp, ci, v = coo_csr(3, range(3), range(3), [2.0, 4.0, 8.0])
+    rc, z = orc.precond_apply(1, rp, ci, v, [4.0, 8.0, 16.0])
+    assert np.array_equal(z, [2.0, 2.0, 2.0])
+    rc, z = orc.precond_apply(1, *orc.poisson_2d(8), np.ones(64))
+    assert np.all(z == 0.25)
+
+
+def test_kat_ilu_diagonal_and_amg_levels(orc):
+    # test_preconditioners.cpp:71-122
+    rp, ci, v = coo_csr(3, range(3), range(3), [2.0, 4.0, 8.0])
+    rc, z = orc.precond_apply(2, rp, ci, v, [2.0, 4.0, 8.0], default_params(drop_tol=0.0))
+    assert np.allclose(z, 1.0)
+    hier = orc.amg_hierarchy(*orc.poisson_2d(16))
+    assert len(hier) >= 2
+
+
+def test_kat_fgmres_amg_and_convdiff(orc):
+    # test_solvers.cpp:195-224
+    p = default_params(tol=1e-9, max_iter=3000, restart_size=40)
+    A = orc.poisson_2d(16)
+    b = np.ones(256)
+    rc, x, s = orc.solve(1, 3, *A, b, params=p)
+    assert rc == 1
+    A = orc.convdiff_2d(12, 0.1, 5.0, 0.0)
+    rc, x, s = orc.solve(1, 2, *A, np.ones(144), params=default_params(
+        tol=1e-9, max_iter=3000, restart_size=40, drop_tol=0.0))
+    assert rc == 1
+
+
+def test_kat_level_sets(orc):
+    # no reference counterpart: the level of row (i, j) of an n x n 5-point grid in natural
+    # order is i + j for the lower triangle and (n-1-i) + (n-1-j) for the upper one
+    n = 9
+    A = orc.poisson_2d(n)
+    nl, lev = orc.levels(A[0], A[1], 0)
+    ii, jj = np.divmod(np.arange(n * n), n)
+    assert nl == 2 * n - 1 and np.array_equal(lev, ii + jj)
+    nu, lev = orc.levels(A[0], A[1], 1)
+    assert nu == 2 * n - 1 and np.array_equal(lev, (n - 1 - ii) + (n - 1 - jj))
+
+
+# ------------------------------------------------------------------ golden fixtures
+
+@pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p) for p in GOLDEN])
+def test_oracle_matches_golden(orc, path):
+    g = np.load(path)
+    rp, ci, v, b = g["rp"], g["ci"], g["v"], g["b"]
+    m, agg = orc.aggregate(rp, ci, v, 0.25)
+    assert np.array_equal(agg, g["agg"])
+    hier = orc.amg_hierarchy(rp, ci, v)
+    assert len(hier) == int(g["amg_levels"])
+    for l, lev in enumerate(hier):
+        for k, (rows, cols, hrp, hci, hv) in lev.items():
+            assert [rows, cols] == list(g[f"amg{l}_{k}_shape"])
+            assert np.array_equal(hrp, g[f"amg{l}_{k}_rp"])
+            assert np.array_equal(hci, g[f"amg{l}_{k}_ci"])
+            assert np.array_equal(hv, g[f"amg{l}_{k}_v"])
+    rc, lu = orc.ilu0(rp, ci, v)
+    assert np.array_equal(lu, g["ilu0"])
+    p0 = default_params(drop_tol=0.0)
+    for kind, tag in ((1, "jacobi"), (2, "ilu"), (3, "amg")):
+        rc, z = orc.precond_apply(kind, rp, ci, v, b, p0)
+        assert np.array_equal(z, g[f"apply_{tag}"])
+    for solver, prec, tag in ((0, 1, "cg_jacobi"), (1, 2, "fgmres_ilu"), (1, 3, "fgmres_amg"),
+                              (0, 3, "cg_amg"), (1, 1, "fgmres_jacobi")):
+        p = default_params(drop_tol=0.0, tol=1e-8, max_iter=1000, restart_size=30)
+        rc, x, s = orc.solve(solver, prec, rp, ci, v, b, params=p)
+        st = g[f"{tag}_stats"]
+        assert rc == int(st[0]) and s.iterations == int(st[1]) and s.restarts == int(st[3])
+        assert s.final_residual == st[2] and s.initial_residual == st[4]
+        assert np.array_equal(x, g[f"{tag}_x"])
+    f, st = orc.features(rp, ci, v)
+    assert np.array_equal(f, g["features"]) and st == int(g["initial_state"])
+
+
+def test_generators_match_oracle(orc):
+    for n in (1, 3, 16, 33):
+        for a, b in zip(P.poisson_2d(n), orc.poisson_2d(n)):
+            assert np.array_equal(a, b)
+    for n, pe in ((7, 1.0), (20, 10.0), (31, 100.0)):
+        bx, by = P.convdiff_wind(n, pe)
+        for a, b in zip(P.convection_diffusion_2d(n, 1.0, bx, by), orc.convdiff_2d(n, 1.0, bx, by)):
+            assert np.array_equal(a, b)
+        for a, b in zip(P.convection_diffusion_2d(n, 0.5, -bx, by), orc.convdiff_2d(n, 0.5, -bx, by)):
+            assert np.array_equal(a, b)
+
+
+# ---------------------------------------------------- live pin against the reference
+
+def _cases():
+    yield "poisson24", P.poisson_2d(24)
+    yield "varkappa32", P.varkappa_poisson_2d(32, 1.0, 11)
+    bx, by = P.convdiff_wind(18, 100.0)
+    yield "convdiff18_pe100", P.convection_diffusion_2d(18, 1.0, bx, by)
+    yield "helmholtz10", P.helmholtz_2d(10, 7.0)
+
+
+@pytest.mark.parametrize("name,A", list(_cases()), ids=[c[0] for c in _cases()])
+def test_oracle_equals_reference(orc, ref, name, A):
+    n = len(A[0]) - 1
+    b = P.rhs(n, 5)
+    assert np.array_equal(orc.spmv(*A, b), ref.spmv(*A, b))
+    assert orc.dot(b, b) == ref.dot(b, b)
+    assert np.array_equal(orc.aggregate(*A)[1], ref.aggregate(*A)[1])
+    for (l1, l2) in zip(orc.amg_hierarchy(*A), ref.amg_hierarchy(*A)):
+        for k in l1:
+            for a, c in zip(l1[k][2:], l2[k][2:]):
+                assert np.array_equal(a, c)
+    assert np.array_equal(orc.ilu0(*A)[1], ref.ilu0(*A)[1])
+    for solver, prec in ((0, 1), (1, 2), (1, 3), (0, 0), (1, 0)):
+        p = default_params(drop_tol=0.0, tol=1e-8, max_iter=600, restart_size=25)
+        r1 = orc.solve(solver, prec, *A, b, params=p)
+        r2 = ref.solve(solver, prec, *A, b, params=p)
+        assert r1[0] == r2[0] and r1[2].iterations == r2[2].iterations
+        assert np.array_equal(r1[1], r2[1])
+    f1, s1 = orc.features(*A)
+    f2, s2 = ref.features(*A)
+    assert np.array_equal(f1, f2) and s1 == s2
+    p = default_params(drop_tol=0.0, max_iter=150)
+    o = orc.solve_adaptive(*A, b, params=p)
+    q = ref.solve_adaptive(*A, b, params=p)
+    assert o[0] == q[0] and o[2].iterations == q[2].iterations
+    assert [(e.from_state, e.to_state, e.at_iteration) for e in o[3]] == \
+           [(e.from_state, e.to_state, e.at_iteration) for e in q[3]]
+    assert np.array_equal(o[1], q[1])
+
+
+def test_reference_from_coo_matches_generators(ref):
+    # from_coo sorts by (row, col) and accumulates duplicates (sparse_matrix.cpp:242-282)
+    rp, ci, v = ref.from_coo(3, 3, [2, 0, 0, 1, 0], [1, 2, 0, 1, 0], [1.0, 2.0, 3.0, 4.0, 5.0])
+    assert list(rp) == [0, 2, 3, 4] and list(ci) == [0, 2, 1, 1] and list(v) == [8.0, 2.0, 4.0, 1.0]
