@@ -1,0 +1,501 @@
+// capi.cu -- the extern "C" boundary (include/hamlss.h).  Every entry point catches
+// engine errors and returns a HAMLSS_ERR_* code; hamlss_last_error() explains it.
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <string>
+
+#include "krylov.cuh"
+#include "nvml_energy.cuh"
+
+using namespace hamlss;
+
+namespace {
+
+thread_local std::string g_err;
+
+int set_err(int code, const std::string& m) {
+    g_err = m;
+    return code;
+}
+
+template <typename F>
+int guarded(F&& f) {
+    try {
+        return f();
+    } catch (const Error& e) {
+        return set_err(e.code, e.what());
+    } catch (const std::bad_alloc&) {
+        return set_err(HAMLSS_ERR_NOMEM, "host allocation failed");
+    } catch (const std::exception& e) {
+        return set_err(HAMLSS_ERR_INVALID, e.what());
+    }
+}
+
+double now_s() {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+// flop_model (energy_monitor.hpp:163-177)
+long long spmv_flops(long long nz) { return 2LL * nz; }
+long long spmv_bytes(long long n, long long nz) { return (n + 1 + nz) * 4 + nz * 8 + n * 16; }
+
+void cg_cost(long long n, long long nz, const SolveResult& r, long long* flops, long long* bytes) {
+    long long trips = r.iterations, partial = 0;
+    if (r.converged && trips > 0) { partial = 1; trips -= 1; }
+    long long restart_trips = std::min<long long>(r.restarts, trips);
+    trips -= restart_trips;
+    long long f_full = spmv_flops(nz) + 2 * n + 2 * (2 * n) + 2 * n + 2 * n;
+    long long b_full = spmv_bytes(n, nz) + 16 * n + 2 * (24 * n) + 16 * n + 24 * n;
+    long long f_part = spmv_flops(nz) + 2 * n + 2 * (2 * n);
+    long long b_part = spmv_bytes(n, nz) + 16 * n + 2 * (24 * n);
+    long long f_rs = spmv_flops(nz) + 2 * n, b_rs = spmv_bytes(n, nz) + 16 * n;
+    *flops = trips * f_full + partial * f_part + restart_trips * f_rs;
+    *bytes = trips * b_full + partial * b_part + restart_trips * b_rs;
+}
+
+void fgmres_cost(long long n, long long nz, const SolveResult& r, long long* flops, long long* bytes) {
+    *flops = (long long)r.iterations * (spmv_flops(nz) + 4 * n);
+    *bytes = (long long)r.iterations * (spmv_bytes(n, nz) + 4 * n * 8);
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* hamlss_version(void) { return "hamlss-b200 0.1 (sm_100a)"; }
+const char* hamlss_last_error(void) { return g_err.c_str(); }
+
+void hamlss_params_default(hamlss_params* p) {
+    if (!p) return;
+    std::memset(p, 0, sizeof(*p));
+    p->tol = 1e-8;
+    p->max_iter = 2000;
+    p->restart_size = 50;
+    p->drop_tol = 1e-4;
+    p->amg_levels = 10;
+    p->amg_strength = 0.25;
+    p->amg_strong = 0.25;
+    p->amg_smooth_pre = 2;
+    p->amg_smooth_post = 2;
+    p->stall_window = 15;
+    p->stall_threshold = 0.95;
+    p->print_every = 25;
+    p->sstep_k = 1;
+    p->sstep_cond_tol = 1e12;
+    p->async_max_stale = 3;
+    p->block_size = 1;
+    p->precision = HAMLSS_FP64;
+    p->ir_inner_tol = 1e-5;
+    p->ir_max_outer = 30;
+    p->amg_omega = 0.67;
+    p->amg_coarse_limit = 50;
+    p->jacobi_omega = 1.0;
+    p->ladder_mode = 0;
+    p->check_every = 8;
+}
+
+// ------------------------------------------------------------------------ context
+int hamlss_ctx_create(int device, hamlss_ctx** out) {
+    return guarded([&]() -> int {
+        if (!out) return set_err(HAMLSS_ERR_INVALID, "out is null");
+        int count = 0;
+        HAMLSS_CUDA(cudaGetDeviceCount(&count));
+        if (device < 0 || device >= count) return set_err(HAMLSS_ERR_INVALID, "no such device");
+        HAMLSS_CUDA(cudaSetDevice(device));
+        auto* c = new hamlss_ctx();
+        c->c.device = device;
+        HAMLSS_CUDA(cudaDeviceGetAttribute(&c->c.sm_count, cudaDevAttrMultiProcessorCount, device));
+        lane_init(c->c.lane, c->c.sm_count);
+        HAMLSS_CUDA(cudaEventCreate(&c->c.ev0));
+        HAMLSS_CUDA(cudaEventCreate(&c->c.ev1));
+        c->c.host_poll.alloc(4096);
+        *out = c;
+        return HAMLSS_OK;
+    });
+}
+
+int hamlss_ctx_destroy(hamlss_ctx* ctx) {
+    return guarded([&]() -> int {
+        if (!ctx) return HAMLSS_OK;
+        cudaSetDevice(ctx->c.device);
+        lane_destroy(ctx->c.lane);
+        if (ctx->c.ev0) cudaEventDestroy(ctx->c.ev0);
+        if (ctx->c.ev1) cudaEventDestroy(ctx->c.ev1);
+        delete ctx;
+        return HAMLSS_OK;
+    });
+}
+
+int hamlss_ctx_synchronize(hamlss_ctx* ctx) {
+    return guarded([&]() -> int {
+        if (!ctx) return set_err(HAMLSS_ERR_INVALID, "ctx is null");
+        HAMLSS_CUDA(cudaStreamSynchronize(ctx->c.lane.stream));
+        return HAMLSS_OK;
+    });
+}
+
+int hamlss_ctx_stream(hamlss_ctx* ctx, void** stream) {
+    if (!ctx || !stream) return set_err(HAMLSS_ERR_INVALID, "null argument");
+    *stream = (void*)ctx->c.lane.stream;
+    return HAMLSS_OK;
+}
+
+// ------------------------------------------------------------------------- matrix
+int hamlss_mat_upload(hamlss_ctx* ctx, int32_t rows, int32_t cols, int32_t nnz,
+                      const int32_t* row_ptr, const int32_t* col_idx, const double* values,
+                      int where, hamlss_mat** out) {
+    return guarded([&]() -> int {
+        if (!ctx || !out || rows < 0 || cols < 0 || nnz < 0 || !row_ptr ||
+            (nnz > 0 && (!col_idx || !values)))
+            return set_err(HAMLSS_ERR_INVALID, "hamlss_mat_upload: bad arguments");
+        HAMLSS_CUDA(cudaSetDevice(ctx->c.device));
+        auto* M = new hamlss_mat();
+        M->ctx = ctx;
+        DevMat& A = M->A;
+        A.n = rows;
+        A.m = cols;
+        A.nnz = nnz;
+        cudaStream_t s = ctx->c.lane.stream;
+        A.rp.ensure((size_t)rows + 1);
+        A.ci.ensure(nnz);
+        A.v.ensure(nnz);
+        auto kind = where == HAMLSS_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+        HAMLSS_CUDA(cudaMemcpyAsync(A.rp.p, row_ptr, sizeof(int) * ((size_t)rows + 1), kind, s));
+        if (nnz) {
+            HAMLSS_CUDA(cudaMemcpyAsync(A.ci.p, col_idx, sizeof(int) * (size_t)nnz, kind, s));
+            HAMLSS_CUDA(cudaMemcpyAsync(A.v.p, values, sizeof(double) * (size_t)nnz, kind, s));
+        }
+        int rc = validate_csr(ctx->c, A.f64());
+        if (rc != HAMLSS_OK) {
+            delete M;
+            return set_err(rc, "hamlss_mat_upload: malformed CSR (row_ptr, column range or "
+                               "unsorted/duplicate columns)");
+        }
+        *out = M;
+        return HAMLSS_OK;
+    });
+}
+
+int hamlss_mat_update_values(hamlss_mat* M, const double* values, int where) {
+    return guarded([&]() -> int {
+        if (!M || (M->A.nnz && !values)) return set_err(HAMLSS_ERR_INVALID, "null argument");
+        auto kind = where == HAMLSS_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+        if (M->A.nnz)
+            HAMLSS_CUDA(cudaMemcpyAsync(M->A.v.p, values, sizeof(double) * M->A.nnz, kind,
+                                        M->ctx->c.lane.stream));
+        M->A.v32_valid = false;
+        M->diag_valid = false;
+        M->version++;
+        return HAMLSS_OK;
+    });
+}
+
+int hamlss_mat_info(const hamlss_mat* M, int32_t* rows, int32_t* cols, int32_t* nnz) {
+    if (!M) return set_err(HAMLSS_ERR_INVALID, "null matrix");
+    if (rows) *rows = M->A.n;
+    if (cols) *cols = M->A.m;
+    if (nnz) *nnz = M->A.nnz;
+    return HAMLSS_OK;
+}
+
+int hamlss_mat_download(const hamlss_mat* M, int32_t* row_ptr, int32_t* col_idx, double* values) {
+    return guarded([&]() -> int {
+        if (!M) return set_err(HAMLSS_ERR_INVALID, "null matrix");
+        cudaStream_t s = M->ctx->c.lane.stream;
+        if (row_ptr) M->A.rp.download(row_ptr, (size_t)M->A.n + 1, s);
+        if (col_idx) M->A.ci.download(col_idx, M->A.nnz, s);
+        if (values) M->A.v.download(values, M->A.nnz, s);
+        HAMLSS_CUDA(cudaStreamSynchronize(s));
+        return HAMLSS_OK;
+    });
+}
+
+int hamlss_mat_release(hamlss_mat* M) {
+    return guarded([&]() -> int {
+        if (!M) return HAMLSS_OK;
+        cudaStreamSynchronize(M->ctx->c.lane.stream);
+        delete M;
+        return HAMLSS_OK;
+    });
+}
+
+// ------------------------------------------------------------------ SpMV / BLAS-1
+}  // extern "C"
+
+namespace {
+struct BodyDot {
+    const double* x;
+    const double* y;
+    HAMLSS_NO_LOAD
+    template <int NV>
+    __device__ __forceinline__ void operator()(int i, double (&acc)[NV]) const { acc[0] += x[i] * y[i]; }
+};
+struct FinStore1 {
+    double* out;
+    template <int NV>
+    __device__ void operator()(const double (&t)[NV]) const { out[0] = t[0]; }
+};
+struct BodyAxpby {
+    double a, b;
+    const double* x;
+    double* y;
+    HAMLSS_NO_LOAD
+    template <int NV>
+    __device__ __forceinline__ void operator()(int i, double (&)[NV]) const {
+        // Vector::axpby (vector.cpp:82-89): y = a*x + b*y, no fused multiply-add
+        y[i] = __dadd_rn(__dmul_rn(a, x[i]), __dmul_rn(b, y[i]));
+    }
+};
+struct BodyAxpy {
+    double a;
+    const double* x;
+    double* y;
+    HAMLSS_NO_LOAD
+    template <int NV>
+    __device__ __forceinline__ void operator()(int i, double (&)[NV]) const {
+        y[i] = __dadd_rn(y[i], __dmul_rn(a, x[i]));   // vector.cpp:79
+    }
+};
+struct BodyScale {
+    double a;
+    double* x;
+    HAMLSS_NO_LOAD
+    template <int NV>
+    __device__ __forceinline__ void operator()(int i, double (&)[NV]) const { x[i] = __dmul_rn(x[i], a); }
+};
+
+int dot_impl(hamlss_ctx* ctx, int32_t n, const double* x, const double* y, double* result) {
+    if (!ctx || n < 0 || !result || (n && (!x || !y))) return set_err(HAMLSS_ERR_INVALID, "bad arguments");
+    Ctx& c = ctx->c;
+    DBuf<double> out(1);
+    out.zero(c.lane.stream);
+    if (n) launch_vec<1>(c.sm_count, c.lane, n, BodyDot{x, y}, FinStore1{out.p});
+    out.download(result, 1, c.lane.stream);
+    HAMLSS_CUDA(cudaStreamSynchronize(c.lane.stream));
+    return HAMLSS_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int hamlss_spmv(hamlss_ctx* ctx, const hamlss_mat* A, const double* x, double* y, int where) {
+    return guarded([&]() -> int {
+        if (!ctx || !A || (A->A.n && (!x || !y))) return set_err(HAMLSS_ERR_INVALID, "null argument");
+        Ctx& c = ctx->c;
+        cudaStream_t s = c.lane.stream;
+        auto* Am = const_cast<hamlss_mat*>(A);
+        const double* dx = x;
+        double* dy = y;
+        Workspace& ws = Am->ws;
+        if (where == HAMLSS_HOST) {
+            ws.d[6].upload(x, A->A.m, s);
+            ws.d[7].ensure(A->A.n);
+            dx = ws.d[6].p;
+            dy = ws.d[7].p;
+        }
+        if (A->A.n) launch_spmv<double, 0>(c.sm_count, c.lane, A->A.f64(), XVec<double>{dx},
+                                           EpiStore<double>{dy});
+        if (where == HAMLSS_HOST) ws.d[7].download(y, A->A.n, s);
+        HAMLSS_CUDA(cudaStreamSynchronize(s));
+        return HAMLSS_OK;
+    });
+}
+
+int hamlss_dot(hamlss_ctx* ctx, int32_t n, const double* x, const double* y, double* result) {
+    return guarded([&]() -> int { return dot_impl(ctx, n, x, y, result); });
+}
+
+int hamlss_norm2(hamlss_ctx* ctx, int32_t n, const double* x, double* result) {
+    return guarded([&]() -> int {
+        int rc = dot_impl(ctx, n, x, x, result);
+        if (rc == HAMLSS_OK) *result = std::sqrt(*result);
+        return rc;
+    });
+}
+
+int hamlss_axpy(hamlss_ctx* ctx, int32_t n, double alpha, const double* x, double* y) {
+    return guarded([&]() -> int {
+        if (!ctx || n < 0 || (n && (!x || !y))) return set_err(HAMLSS_ERR_INVALID, "bad arguments");
+        if (n) launch_vec<0>(ctx->c.sm_count, ctx->c.lane, n, BodyAxpy{alpha, x, y});
+        HAMLSS_CUDA(cudaStreamSynchronize(ctx->c.lane.stream));
+        return HAMLSS_OK;
+    });
+}
+
+int hamlss_axpby(hamlss_ctx* ctx, int32_t n, double a, const double* x, double b, double* y) {
+    return guarded([&]() -> int {
+        if (!ctx || n < 0 || (n && (!x || !y))) return set_err(HAMLSS_ERR_INVALID, "bad arguments");
+        if (n) launch_vec<0>(ctx->c.sm_count, ctx->c.lane, n, BodyAxpby{a, b, x, y});
+        HAMLSS_CUDA(cudaStreamSynchronize(ctx->c.lane.stream));
+        return HAMLSS_OK;
+    });
+}
+
+int hamlss_scale(hamlss_ctx* ctx, int32_t n, double alpha, double* x) {
+    return guarded([&]() -> int {
+        if (!ctx || n < 0 || (n && !x)) return set_err(HAMLSS_ERR_INVALID, "bad arguments");
+        if (n) launch_vec<0>(ctx->c.sm_count, ctx->c.lane, n, BodyScale{alpha, x});
+        HAMLSS_CUDA(cudaStreamSynchronize(ctx->c.lane.stream));
+        return HAMLSS_OK;
+    });
+}
+
+// ---------------------------------------------------------------- preconditioners
+int hamlss_precond_setup(hamlss_ctx* ctx, const hamlss_mat* A, int kind,
+                         const hamlss_params* params, hamlss_prec** out, double* setup_time_s) {
+    return guarded([&]() -> int {
+        if (!ctx || !A || !out) return set_err(HAMLSS_ERR_INVALID, "null argument");
+        hamlss_params p;
+        if (params) p = *params; else hamlss_params_default(&p);
+        *out = nullptr;
+        double t0 = now_s();
+        auto* Am = const_cast<hamlss_mat*>(A);
+        std::unique_ptr<Prec> P;
+        switch (kind) {
+            case HAMLSS_PREC_NONE:
+                if (setup_time_s) *setup_time_s = 0.0;
+                return HAMLSS_OK;
+            case HAMLSS_PREC_JACOBI:
+                P = make_jacobi(ctx->c, Am, p.jacobi_omega);
+                break;
+            case HAMLSS_PREC_ILU:
+                if (p.drop_tol > 0.0 || p.fill_per_row > 0)
+                    return set_err(HAMLSS_ERR_INVALID,
+                                   "ILUT (drop_tol > 0 or fill_per_row > 0) is not provided by "
+                                   "the engine; pass drop_tol = 0 for ILU(0)");
+                P = make_ilu0(ctx->c, Am);
+                break;
+            case HAMLSS_PREC_AMG:
+                P = make_amg(ctx->c, Am, p);
+                break;
+            default:
+                return set_err(HAMLSS_ERR_INVALID, "SolverFactory: unknown PrecondType");
+        }
+        HAMLSS_CUDA(cudaStreamSynchronize(ctx->c.lane.stream));
+        auto* h = new hamlss_prec();
+        h->ctx = ctx;
+        h->A = Am;
+        h->p = std::move(P);
+        *out = h;
+        if (setup_time_s) *setup_time_s = now_s() - t0;
+        return HAMLSS_OK;
+    });
+}
+
+int hamlss_precond_apply(hamlss_ctx* ctx, const hamlss_prec* M, const double* r, double* z,
+                         int where) {
+    return guarded([&]() -> int {
+        if (!ctx || !M || !r || !z) return set_err(HAMLSS_ERR_INVALID, "null argument");
+        Ctx& c = ctx->c;
+        cudaStream_t s = c.lane.stream;
+        const int n = M->p->n;
+        Workspace& ws = M->A->ws;
+        const double* dr = r;
+        double* dz = z;
+        if (where == HAMLSS_HOST) {
+            ws.d[6].upload(r, n, s);
+            ws.d[7].ensure(n);
+            dr = ws.d[6].p;
+            dz = ws.d[7].p;
+        }
+        M->p->apply(c, c.lane, dr, dz, nullptr);
+        if (where == HAMLSS_HOST) ws.d[7].download(z, n, s);
+        HAMLSS_CUDA(cudaStreamSynchronize(s));
+        return HAMLSS_OK;
+    });
+}
+
+int hamlss_precond_type(const hamlss_prec* M, int32_t* kind) {
+    if (!M || !kind) return set_err(HAMLSS_ERR_INVALID, "null argument");
+    *kind = M->p->kind;
+    return HAMLSS_OK;
+}
+
+int hamlss_precond_release(hamlss_prec* M) {
+    return guarded([&]() -> int {
+        if (!M) return HAMLSS_OK;
+        cudaStreamSynchronize(M->ctx->c.lane.stream);
+        delete M;
+        return HAMLSS_OK;
+    });
+}
+
+// -------------------------------------------------------------------------- solve
+int hamlss_solve(hamlss_ctx* ctx, int solver, const hamlss_mat* A, const hamlss_prec* M,
+                 const double* b, double* x, int where, const hamlss_params* params,
+                 hamlss_stats* stats) {
+    return guarded([&]() -> int {
+        if (!ctx || !A || !b || !x) return set_err(HAMLSS_ERR_INVALID, "null argument");
+        if (A->A.n != A->A.m) return set_err(HAMLSS_ERR_SIZE, "solve needs a square matrix");
+        if (M && M->A != A && M->p->n != A->A.n)
+            return set_err(HAMLSS_ERR_SIZE, "preconditioner size differs from the matrix");
+        hamlss_params p;
+        if (params) p = *params; else hamlss_params_default(&p);
+        if (solver == HAMLSS_SOLVER_BICGSTAB) solver = HAMLSS_SOLVER_FGMRES;  // solver_factory.cpp:34-37
+        if (solver != HAMLSS_SOLVER_CG && solver != HAMLSS_SOLVER_FGMRES)
+            return set_err(HAMLSS_ERR_INVALID, "solver type not provided by the engine");
+        Ctx& c = ctx->c;
+        HAMLSS_CUDA(cudaSetDevice(c.device));
+        cudaStream_t s = c.lane.stream;
+        auto* Am = const_cast<hamlss_mat*>(A);
+        Prec* P = M ? M->p.get() : nullptr;
+        const int n = A->A.n;
+        Workspace& ws = Am->ws;
+        const double* db = b;
+        double* dx = x;
+        if (where == HAMLSS_HOST) {
+            ws.d[6].upload(b, n, s);
+            ws.d[7].upload(x, n, s);
+            db = ws.d[6].p;
+            dx = ws.d[7].p;
+        }
+        double e0 = p.record_hw_energy ? nvml_energy_j(c.device) : 0.0;
+        double t0 = now_s();
+        SolveResult r;
+        int outer = 1;
+        if (p.precision == HAMLSS_MIXED) {
+            r = mixed_solve(c, solver, Am, P, db, dx, p, ws, &outer);
+        } else if (solver == HAMLSS_SOLVER_CG) {
+            r = cg_solve<double>(c, Am, P, db, dx, p.tol, p.max_iter, p.check_every, ws);
+        } else {
+            r = fgmres_solve(c, Am, P, db, dx, p.tol, p.max_iter, p.restart_size, ws);
+        }
+        double t1 = now_s();
+        double e1 = p.record_hw_energy ? nvml_energy_j(c.device) : 0.0;
+        if (stats) {
+            hamlss_stats st;
+            std::memset(&st, 0, sizeof(st));
+            st.iterations = r.iterations;
+            st.initial_residual = r.initial_residual;
+            st.final_residual = r.final_residual;
+            st.converged = r.converged;
+            st.solve_time_s = t1 - t0;
+            st.solver_used = solver;
+            st.precond_used = P ? P->kind : HAMLSS_PREC_NONE;
+            st.state_used = HAMLSS_STATE_EASY;
+            st.restarts = r.restarts;
+            long long fl = 0, by = 0;
+            if (solver == HAMLSS_SOLVER_CG) cg_cost(n, A->A.nnz, r, &fl, &by);
+            else fgmres_cost(n, A->A.nnz, r, &fl, &by);
+            st.flop_count = fl;
+            st.mem_bytes = by;
+            st.energy_joules = 2.0e-10 * (double)fl + 5.0e-9 * (double)by;
+            st.energy_joules_hw = (e1 > e0) ? e1 - e0 : 0.0;
+            st.rapl_start_j = e0;
+            st.rapl_end_j = e1;
+            st.outer_iterations = outer;
+            st.status = r.status;
+            st.device_time_s = r.device_time_s;
+            st.true_residual = true_relative_residual(c, Am, db, dx, ws);
+            *stats = st;
+        }
+        if (where == HAMLSS_HOST) ws.d[7].download(x, n, s);
+        HAMLSS_CUDA(cudaStreamSynchronize(s));
+        if (r.status != HAMLSS_OK)
+            return set_err(r.status, "non-finite values met during the solve");
+        return HAMLSS_OK;
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,113 @@
+// engine.cuh -- context, device matrices and launch helpers shared by all solvers.
+#pragma once
+
+#include <memory>
+#include <mutex>
+
+#include "common.cuh"
+#include "spmv.cuh"
+
+namespace hamlss {
+
+// A stream plus the scratch its reductions use.  Kernels on one lane run in order, so
+// one reducer (partials + ticket) per lane is enough.
+struct Lane {
+    cudaStream_t stream = nullptr;
+    DBuf<double> partials;
+    DBuf<unsigned> ticket;
+    Reducer red() const { return Reducer{partials.p, ticket.p}; }
+};
+
+struct Ctx {
+    int device = 0;
+    int sm_count = 148;
+    Lane lane;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    HBuf<char> host_poll;      // pinned landing zone for polled device state
+    std::mutex mu;
+};
+
+// Max co-resident blocks of a kernel (cached per kernel instantiation by the caller).
+template <typename K>
+int occupancy_blocks(K kernel, int threads, size_t dyn_smem = 0) {
+    int b = 0;
+    HAMLSS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kernel, threads, dyn_smem));
+    return b > 0 ? b : 1;
+}
+
+constexpr int kMaxBlocksPerSm = 8;
+constexpr int kMaxRed = 72;   // widest reduction (multi-dot of an FGMRES basis + 2)
+constexpr int kPartialCap = 148 * kMaxBlocksPerSm * kMaxRed;
+
+void lane_init(Lane& L, int sm_count);
+void lane_destroy(Lane& L);
+
+// Device view of a CSR matrix.
+template <typename T>
+struct Csr {
+    int n = 0, m = 0, nnz = 0;
+    const int* rp = nullptr;
+    const int* ci = nullptr;
+    const T* v = nullptr;
+};
+
+// Owning device CSR (structure + FP64 values, FP32 values on demand).
+struct DevMat {
+    int n = 0, m = 0, nnz = 0;
+    DBuf<int> rp, ci;
+    DBuf<double> v;
+    DBuf<float> v32;
+    bool v32_valid = false;
+    Csr<double> f64() const { return Csr<double>{n, m, nnz, rp.p, ci.p, v.p}; }
+    Csr<float> f32(cudaStream_t s);
+};
+
+template <typename T, int NRED, typename XOp, typename Epi, typename Fin = NoFin>
+void launch_spmv(int sm_count, const Lane& L, const Csr<T>& A, const XOp& xop, const Epi& epi,
+                 const Fin& fin = Fin{}, const int* gate = nullptr) {
+    static int per_sm = 0;
+    auto kern = k_spmv<T, NRED, XOp, Epi, Fin>;
+    if (!per_sm) per_sm = std::min(occupancy_blocks(kern, kSpmvThreads), kMaxBlocksPerSm);
+    const int ntiles = ceil_div(A.n, 32);
+    int blocks = std::max(1, std::min(ceil_div(ntiles, kSpmvWarps), sm_count * per_sm));
+    kern<<<blocks, kSpmvThreads, 0, L.stream>>>(A.n, A.rp, A.ci, A.v, xop, epi, L.red(), fin, gate);
+    HAMLSS_LAUNCH_CHECK();
+}
+
+template <int NRED, typename Body, typename Fin = NoFin>
+void launch_vec(int sm_count, const Lane& L, int n, const Body& body, const Fin& fin = Fin{},
+                const int* gate = nullptr) {
+    int blocks = std::max(1, std::min(ceil_div(n, 256), sm_count * kMaxBlocksPerSm));
+    k_vec<NRED, Body, Fin><<<blocks, 256, 0, L.stream>>>(n, body, L.red(), fin, gate);
+    HAMLSS_LAUNCH_CHECK();
+}
+
+// Buffers a solve needs, cached on the matrix (allocated once per size and kind; the
+// solve loops themselves allocate nothing).
+struct Workspace {
+    DBuf<double> d[8];
+    DBuf<float> f[8];
+    DBuf<double> basis;     // FGMRES V (m+1) x n and Z m x n
+    DBuf<double> small;     // Hessenberg, Givens, scalars
+    DBuf<char> state;
+};
+
+// Validate a CSR already on the device: row_ptr monotone from 0 to nnz, columns in
+// [0, m), strictly increasing within a row.  Returns HAMLSS_OK or HAMLSS_ERR_MALFORMED.
+int validate_csr(Ctx& ctx, const Csr<double>& A);
+
+}  // namespace hamlss
+
+// Opaque ABI types.
+struct hamlss_ctx {
+    hamlss::Ctx c;
+};
+
+struct hamlss_mat {
+    hamlss_ctx* ctx = nullptr;
+    hamlss::DevMat A;
+    hamlss::DBuf<double> diag;      // a_ii (0 where the row has no diagonal entry)
+    bool diag_valid = false;
+    uint64_t version = 0;           // bumped by hamlss_mat_update_values
+    hamlss::Workspace ws;
+};

@@ -1,0 +1,43 @@
+// krylov.cuh -- device PCG and FGMRES(m) drivers.
+#pragma once
+
+#include "precond.cuh"
+
+namespace hamlss {
+
+// Solve status codes kept in device state (polled by the host).
+enum : int { ST_RUN = 0, ST_CONV = 1, ST_MAXIT = 2, ST_RESTART = 3, ST_NONFINITE = 4 };
+
+struct SolveResult {
+    int iterations = 0;
+    int restarts = 0;
+    int converged = 0;
+    int status = HAMLSS_OK;
+    double initial_residual = 0.0;
+    double final_residual = 0.0;
+    double device_time_s = 0.0;
+};
+
+// CGSolver::solve (cg_solver.cpp:37-191) on device vectors.  T = double runs the FP64
+// path; T = float is the FP32 inner solve of the mixed-precision scheme.  b, x have n
+// entries of type T on the device.  `jac` (may be null) selects the fused Jacobi kernels.
+template <typename T>
+SolveResult cg_solve(Ctx& ctx, hamlss_mat* A, Prec* M, const T* b, T* x, double tol,
+                     int max_iter, int check_every, Workspace& ws);
+
+// FGMRESSolver::solve (fgmres_solver.cpp:165-241) with CGS2 Arnoldi; FP64.
+SolveResult fgmres_solve(Ctx& ctx, hamlss_mat* A, Prec* M, const double* b, double* x,
+                         double tol, int max_iter, int restart, Workspace& ws);
+
+// Mixed precision: FP64 iterative refinement around an FP32 inner PCG / FGMRES.
+SolveResult mixed_solve(Ctx& ctx, int solver, hamlss_mat* A, Prec* M, const double* b,
+                        double* x, const hamlss_params& p, Workspace& ws, int* outer_iters);
+
+// ||b - A x|| / ||b|| in FP64 on the device (SolverBase::relative_residual,
+// solver_base.cpp:9-17).
+double true_relative_residual(Ctx& ctx, hamlss_mat* A, const double* b, const double* x,
+                              Workspace& ws);
+
+inline Workspace& workspace_of(hamlss_mat* A) { return A->ws; }
+
+}  // namespace hamlss

@@ -1,0 +1,9 @@
+// nvml_energy.cuh -- NVML total-energy counter, loaded at run time with dlopen so the
+// library has no link dependency on NVML (NVMLMonitor::read_energy_j,
+// src/parallel/nvml_monitor.cpp:85-100 in the reference, replaces its RAPL reading).
+#pragma once
+
+namespace hamlss {
+// Joules consumed by `device` since driver load; 0.0 when NVML or the counter is missing.
+double nvml_energy_j(int device);
+}  // namespace hamlss

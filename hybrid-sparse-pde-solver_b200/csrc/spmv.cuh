@@ -1,0 +1,142 @@
+// spmv.cuh -- the CSR SpMV kernel template every solver kernel is built from.
+//
+// Layout: CSR, int32 row_ptr / col_idx, values in T (double or float), columns sorted per
+// row.  Scheduling: one warp owns a tile of 32 consecutive rows; it stages the tile's
+// nonzeros (values + column indices) into shared memory with fully coalesced loads
+// (256 B / 128 B per warp instruction) in chunks of kChunk entries, then lane l sums row
+// tile+l from shared memory in column order.  A persistent grid walks the tiles.
+//
+// Fusion: the kernel is parameterised by
+//   XOp  x(j)            -> value of the multiplied vector at column j (may be computed on
+//                           the fly, e.g. p_j = z_j + beta * p_old_j)
+//   Epi  epi(i, ax, acc) -> consumes (A x)_i for own row i; may write vectors and add into
+//                           the NRED per-thread accumulators
+//   Fin  fin(tot)        -> runs once, in the last block, on the grid-wide sums of acc
+// so SpMV + following dot / residual / update / smoother step cost one pass over A.
+// Row sums follow the reference's order (sparse_matrix.cpp:80-86); for double they use
+// separate multiply and add, so A x is bit-identical to the reference's spmv.
+#pragma once
+
+#include "common.cuh"
+
+namespace hamlss {
+
+constexpr int kSpmvThreads = 256;             // 8 warps per block
+constexpr int kSpmvWarps = kSpmvThreads / 32;
+constexpr int kChunk = 256;                   // staged nonzeros per warp and round
+
+template <typename T>
+__device__ __forceinline__ double mul_add(double acc, T a, double x) {
+    return acc + (double)a * x;
+}
+template <>
+__device__ __forceinline__ double mul_add<double>(double acc, double a, double x) {
+    return __dadd_rn(acc, __dmul_rn(a, x));
+}
+
+// Sum of row (row0 + lane) of A against x(); every lane of the warp must call it.
+template <typename T, typename XOp>
+__device__ __forceinline__ double warp_tile_rows(int row0, int n, const int* __restrict__ rp,
+                                                 const int* __restrict__ ci,
+                                                 const T* __restrict__ v, const XOp& x,
+                                                 T* sv, int* sc) {
+    const int lane = threadIdx.x & 31;
+    const int row = row0 + lane;
+    const int rs = __ldg(&rp[row < n ? row : n]);
+    const int re = row < n ? __ldg(&rp[row + 1]) : rs;
+    const int ts = __shfl_sync(0xffffffffu, rs, 0);
+    const int te = __shfl_sync(0xffffffffu, re, 31);
+    double sum = 0.0;
+    for (int base = ts; base < te; base += kChunk) {
+        const int cnt = min(kChunk, te - base);
+#pragma unroll 4
+        for (int k = lane; k < cnt; k += 32) {
+            sv[k] = __ldg(&v[base + k]);
+            sc[k] = __ldg(&ci[base + k]);
+        }
+        __syncwarp();
+        const int lo = max(rs, base), hi = min(re, base + cnt);
+        for (int k = lo; k < hi; ++k) sum = mul_add<T>(sum, sv[k - base], x(sc[k - base]));
+        __syncwarp();
+    }
+    return sum;
+}
+
+struct NoFin {
+    template <int NV>
+    __device__ void operator()(const double (&)[NV]) const {}
+};
+
+// gate: when non-null and *gate != 0 the whole launch is a no-op (the solve it belongs
+// to has stopped; the flag is only written by earlier kernels on the same stream).
+template <typename T, int NRED, typename XOp, typename Epi, typename Fin>
+__global__ void __launch_bounds__(kSpmvThreads)
+k_spmv(int n, const int* __restrict__ rp, const int* __restrict__ ci, const T* __restrict__ v,
+       XOp xop, Epi epi, Reducer red, Fin fin, const int* gate) {
+    __shared__ T sv[kSpmvWarps][kChunk];
+    __shared__ int sc[kSpmvWarps][kChunk];
+    __shared__ double rsh[kSpmvWarps * (NRED > 0 ? NRED : 1)];
+    if (gate && *(volatile const int*)gate) return;
+    XOp xop_l = xop;
+    Epi epi_l = epi;
+    xop_l.load();
+    epi_l.load();
+    const int wid = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const int ntiles = (n + 31) >> 5;
+    double acc[NRED > 0 ? NRED : 1];
+#pragma unroll
+    for (int k = 0; k < (NRED > 0 ? NRED : 1); ++k) acc[k] = 0.0;
+    for (int t = blockIdx.x * kSpmvWarps + wid; t < ntiles; t += gridDim.x * kSpmvWarps) {
+        const int row0 = t << 5;
+        double ax = warp_tile_rows<T>(row0, n, rp, ci, v, xop_l, sv[wid], sc[wid]);
+        const int row = row0 + lane;
+        if (row < n) epi_l(row, ax, acc);
+    }
+    if constexpr (NRED > 0) {
+        double tot[NRED];
+        if (grid_reduce<NRED>(red, acc, rsh, tot)) fin(tot);
+    }
+}
+
+// Elementwise kernel with the same reduction / finalize machinery (no matrix).
+template <int NRED, typename Body, typename Fin>
+__global__ void __launch_bounds__(256)
+k_vec(int n, Body body, Reducer red, Fin fin, const int* gate) {
+    __shared__ double rsh[8 * (NRED > 0 ? NRED : 1)];
+    if (gate && *(volatile const int*)gate) return;
+    Body b = body;
+    b.load();
+    double acc[NRED > 0 ? NRED : 1];
+#pragma unroll
+    for (int k = 0; k < (NRED > 0 ? NRED : 1); ++k) acc[k] = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        b(i, acc);
+    if constexpr (NRED > 0) {
+        double tot[NRED];
+        if (grid_reduce<NRED>(red, acc, rsh, tot)) fin(tot);
+    }
+}
+
+// ------------------------------------------------------------------ common operators
+// Operators may read device scalars once per launch in load() (called at kernel entry,
+// after the gate check).
+#define HAMLSS_NO_LOAD \
+    __device__ __forceinline__ void load() {}
+
+template <typename T>
+struct XVec {
+    const T* x;
+    HAMLSS_NO_LOAD
+    __device__ __forceinline__ double operator()(int j) const { return (double)__ldg(&x[j]); }
+};
+
+template <typename T>
+struct EpiStore {
+    T* y;
+    HAMLSS_NO_LOAD
+    template <int NV>
+    __device__ __forceinline__ void operator()(int i, double ax, double (&)[NV]) const { y[i] = (T)ax; }
+};
+
+}  // namespace hamlss
