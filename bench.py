@@ -1,0 +1,460 @@
+#!/usr/bin/env python
+"""Headline benchmark: solves/s of the variable-coefficient 2-D Poisson problem.
+
+Workload (one "step" = one complete solve of one system, preconditioner setup included):
+  -div(kappa grad u) = f, 5-point, 2048 x 2048 interior grid (n = 4,194,304,
+  nnz = 20,963,328), kappa lognormal (sigma = 1) per cell with harmonic face averages,
+  rhs uniform [-1, 1) from the seed, x0 = 0, solved to 1e-10 relative residual.
+  Inputs are synthetic (seeded); the matrix (335 MB in FP64) is larger than L2 (126 MB),
+  so no L2 flush is needed between steps.
+
+  value : solves/s with the matrix and rhs resident in HBM (device pointers), per-step
+          device time from CUDA events on the engine's stream; whole-job aggregate over
+          all ranks (each rank solves its own seeded instance: weak scaling, no collective
+          on the data path).
+  e2e   : the same solve through the public C ABI with HOST buffers -- upload of the CSR
+          and rhs from pinned host memory, setup, solve, download of x -- all timed.
+
+--impl reference times the reference's own CPU implementation (built from its sources
+by oracle/Makefile into oracle/_ref/) on the host cores, on the same problem.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "hybrid-sparse-pde-solver_b200"))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+N_SIDE = 2048
+SIGMA = 1.0
+TOL = 1e-10
+METRIC = "solves/sec at 1e-10 rel-res (var-kappa Poisson 2048^2)"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--solver", default="auto",
+                    choices=["auto", "cg_jacobi", "amg_fp64", "amg_mixed"])
+    ap.add_argument("--n-side", type=int, default=N_SIDE)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-sample-iters", type=int, default=40)
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def problem(n_side, seed):
+    from hsps_b200 import problems as P
+
+    rp, ci, v = P.varkappa_poisson_2d(n_side, SIGMA, seed)
+    b = P.rhs(len(rp) - 1, seed, -1.0, 1.0)
+    return rp, ci, v, b
+
+
+# ----------------------------------------------------------------- clocks sampling
+class Clocks:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.rows = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows for k in range(4)
+                          if r[5 + k].lower().startswith("active")})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        d = json.load(open(path))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic(kernel_family):
+    """Per-launch DRAM bytes of the dominant kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    if not os.path.exists(path):
+        return None
+    try:
+        d = json.load(open(path))
+        return d.get(kernel_family, {}).get("dram_bytes_per_launch")
+    except (ValueError, OSError):
+        return None
+
+
+# ------------------------------------------------------------------ CPU reference
+def reference_cpu_sample(rp, ci, v, b, iters, threads):
+    """Time `iters` CG+Jacobi iterations of the reference (release build) on the host.
+
+    The reference's AMG cannot be set up at this size (its smoothed prolongation uses a
+    dense n_fine x n_coarse buffer), so its full-size path for this problem is
+    CGSolver + JacobiPreconditioner (SolverFactory::make(CG, JACOBI)).
+    """
+    import oracle
+    from hsps_b200._abi import default_params
+
+    R = oracle.Reference(fast=True, threads=threads)
+    p = default_params(tol=TOL, max_iter=iters)
+    t0 = time.perf_counter()
+    rc, x, st = R.solve(0, 1, rp, ci, v, b, params=p)
+    dt = time.perf_counter() - t0
+    return dt, st.iterations
+
+
+def cpu_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+# --------------------------------------------------------------------- our engine
+def solver_choice(name):
+    import hsps_b200 as H
+
+    if name != "auto":
+        return name
+    try:
+        A = H.SparseMatrix.poisson_2d(8)
+        M = H.AMGPreconditioner()
+        M.setup(A)
+        return "amg_mixed"
+    except Exception:
+        return "cg_jacobi"
+
+
+def make_params(solver):
+    import hsps_b200 as H
+
+    if solver == "cg_jacobi":
+        return H.SolverParams(tol=TOL, max_iter=100000), H.SOLVER_CG, H.PREC_JACOBI
+    prec = 0 if solver == "amg_fp64" else 1
+    p = H.SolverParams(tol=TOL, max_iter=1000, precision=prec, amg_omega=2.0 / 3.0,
+                       amg_coarse_limit=512, amg_levels=25)
+    return p, H.SOLVER_CG, H.PREC_AMG
+
+
+def run_ours(args, rank, world, local):
+    import ctypes as C
+
+    import torch
+
+    import hsps_b200 as H
+    from hsps_b200 import _abi
+
+    torch.cuda.set_device(local)
+    ctx = H.Context(local)
+    L = _abi.lib()
+    solver = solver_choice(args.solver)
+    params, stype, ptype = make_params(solver)
+    rp, ci, v, b = problem(args.n_side, 1000 + rank)
+    n, nnz = len(rp) - 1, len(v)
+    A = H.SparseMatrix(n, n, rp, ci, v, ctx)
+    db = torch.from_numpy(b).cuda()
+    dx = torch.zeros(n, dtype=torch.float64, device="cuda")
+    stream = torch.cuda.ExternalStream(ctx.stream())
+
+    def one_solve():
+        dx.zero_()
+        torch.cuda.synchronize()
+        h = C.c_void_p()
+        if ptype != H.PREC_NONE:
+            rc = L.hamlss_precond_setup(ctx.h, A.h, ptype, C.byref(params), C.byref(h), None)
+            if rc:
+                raise RuntimeError(L.hamlss_last_error())
+        st = _abi.Stats()
+        rc = L.hamlss_solve(ctx.h, stype, A.h, h, C.c_void_p(db.data_ptr()),
+                            C.c_void_p(dx.data_ptr()), H.DEVICE, C.byref(params), C.byref(st))
+        if rc:
+            raise RuntimeError(L.hamlss_last_error())
+        if h:
+            L.hamlss_precond_release(h)
+        return st
+
+    for _ in range(args.warmup):
+        st = one_solve()
+    if not st.converged or st.true_residual > 1.5 * TOL:
+        raise RuntimeError(f"warm-up solve did not reach tolerance: {st.as_dict()}")
+
+    # ---- timed region: device-resident inputs
+    clocks = Clocks(local)
+    dist = world > 1
+    if dist:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    L.hamlss_profile_enable(ctx.h, 1, 2_000_000)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    iters, true_res = [], []
+    for _ in range(args.steps):
+        st = one_solve()
+        iters.append(st.iterations)
+        true_res.append(st.true_residual)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    dev_ms = ev0.elapsed_time(ev1)
+    cap = 64
+    names = C.create_string_buffer(32 * cap)
+    launches = (C.c_int32 * cap)()
+    tms = (C.c_double * cap)()
+    tby = (C.c_double * cap)()
+    cnt = C.c_int32()
+    L.hamlss_profile_read(ctx.h, cap, names, launches, tms, tby, C.byref(cnt))
+    L.hamlss_profile_enable(ctx.h, 0, 0)
+    clocks.stop()
+    fams = []
+    for i in range(cnt.value):
+        nm = names.raw[32 * i:32 * i + 32].split(b"\0")[0].decode()
+        fams.append((nm, launches[i], tms[i], tby[i]))
+    total_launches = sum(f[1] for f in fams)
+    max_ms = dev_ms
+    if dist:
+        t = torch.tensor([dev_ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        max_ms = float(t.item())
+    value = world * args.steps / (max_ms / 1e3)
+
+    # ---- end to end through the C ABI with host buffers (pinned)
+    hb = torch.from_numpy(b).pin_memory()
+    hx = torch.zeros(n, dtype=torch.float64).pin_memory()
+    hrp = torch.from_numpy(rp).pin_memory()
+    hci = torch.from_numpy(ci).pin_memory()
+    hv = torch.from_numpy(v).pin_memory()
+
+    def e2e_step():
+        hx.zero_()
+        mh = C.c_void_p()
+        rc = L.hamlss_mat_upload(ctx.h, n, n, nnz, C.c_void_p(hrp.data_ptr()),
+                                 C.c_void_p(hci.data_ptr()), C.c_void_p(hv.data_ptr()), H.HOST,
+                                 C.byref(mh))
+        if rc:
+            raise RuntimeError(L.hamlss_last_error())
+        ph = C.c_void_p()
+        if ptype != H.PREC_NONE:
+            L.hamlss_precond_setup(ctx.h, mh, ptype, C.byref(params), C.byref(ph), None)
+        st = _abi.Stats()
+        rc = L.hamlss_solve(ctx.h, stype, mh, ph, C.c_void_p(hb.data_ptr()),
+                            C.c_void_p(hx.data_ptr()), H.HOST, C.byref(params), C.byref(st))
+        if rc:
+            raise RuntimeError(L.hamlss_last_error())
+        if ph:
+            L.hamlss_precond_release(ph)
+        L.hamlss_mat_release(mh)
+        return st
+
+    e2e_step()
+    if dist:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    e_steps = max(1, min(args.steps, 3))
+    t0 = time.perf_counter()
+    for _ in range(e_steps):
+        e2e_step()
+    torch.cuda.synchronize()
+    e_dt = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([e_dt], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e_dt = float(t.item())
+    e2e_value = world * e_steps / e_dt
+    h2d = 4 * (n + 1) + 12 * nnz + 8 * n + 8 * n       # CSR + b + initial x
+    d2h = 8 * n                                         # solution
+
+    # ---- roofline of the dominant kernel family
+    peak, peak_kind = peaks()
+    dom = max(fams, key=lambda f: f[2]) if fams else ("none", 0, 0.0, 0.0)
+    achieved = (dom[3] / (dom[2] / 1e3)) / 1e9 if dom[2] > 0 else 0.0
+    traffic = ncu_traffic(dom[0])
+    roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "traffic": traffic,
+                "kernel": dom[0], "launches": dom[1],
+                "bytes_per_launch": dom[3] / max(dom[1], 1),
+                "share_of_device_time": round(dom[2] / max(sum(f[2] for f in fams), 1e-9), 4),
+                "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback 6.65 TB/s"}
+
+    out = {
+        "metric": METRIC, "value": round(value, 4), "unit": "solves/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(max_ms / args.steps, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if solver == "amg_mixed" else "f64",
+        "data": "synthetic (seeded lognormal kappa, uniform rhs)",
+        "config": {"workload": f"var-kappa Poisson {args.n_side}^2 5-point, sigma={SIGMA}, "
+                               f"rtol {TOL}, PCG + {solver}",
+                   "n": n, "nnz": nnz, "solver": solver, "global_batch": world,
+                   "l2": "inputs larger than L2 (no flush)", "parallelism": f"replicas x{world}"},
+        "iterations": int(np.median(iters)), "true_residual_max": float(max(true_res)),
+        "e2e": {"value": round(e2e_value, 4), "unit": "solves/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "roofline": roofline,
+        "gpu_launches": int(total_launches),
+        "kernel_families": {f[0]: {"launches": f[1], "ms": round(f[2], 3),
+                                   "GB/s": round(f[3] / max(f[2], 1e-9) / 1e6, 1)} for f in fams},
+        "clocks": clocks.summary(),
+    }
+    return out, (rp, ci, v, b)
+
+
+def cpu_baseline(args, data, device_iters_fp64):
+    rp, ci, v, b = data
+    threads = cpu_threads()
+    dt, it = reference_cpu_sample(rp, ci, v, b, args.cpu_sample_iters, threads)
+    per_iter = dt / max(it, 1)
+    value = 1.0 / (per_iter * device_iters_fp64)
+    return {"value": value, "unit": "solves/s", "cores": threads, "kind": "reference",
+            "sample": f"{it} CG+Jacobi iterations of the reference (release build, "
+                      f"{threads} OpenMP threads) on the same 2048^2 system, {dt:.1f} s; "
+                      f"solve time = per-iteration time x {device_iters_fp64} iterations "
+                      f"(the count FP64 CG+Jacobi needs for 1e-10 on this system)"}
+
+
+def fp64_cg_iterations(data):
+    """Iterations FP64 CG+Jacobi needs on the system (engine run, same algorithm)."""
+    import ctypes as C
+
+    import torch
+
+    import hsps_b200 as H
+
+    rp, ci, v, b = data
+    n = len(rp) - 1
+    A = H.SparseMatrix(n, n, rp, ci, v)
+    s, _ = H.SolverFactory.make("CG", "JACOBI", A, H.SolverParams(tol=TOL, max_iter=100000))
+    db = torch.from_numpy(b).cuda()
+    dx = torch.zeros(n, dtype=torch.float64, device="cuda")
+    st = H.SolverStats()
+    s.solve(A, db, dx, st)
+    return st.iterations
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return None
+    import oracle
+
+    if not oracle.reference_available(fast=True):
+        return {"impl": "reference", "unavailable": "reference not built from source (oracle/_ref)"}
+    data = problem(args.n_side, 1000)
+    rp, ci, v, b = data
+    threads = cpu_threads()
+    # iteration count of the full solve: CG+Jacobi to 1e-10 (the reference's own full-size
+    # path for this problem); sampled below at `cpu-sample-iters` iterations per step
+    n_full = int(os.environ.get("HAMLSS_REF_FULL_ITERS", "0")) or None
+    if n_full is None:
+        try:
+            n_full = fp64_cg_iterations(data)
+        except Exception:
+            n_full = 8210
+    for _ in range(max(0, min(args.warmup, 1))):
+        reference_cpu_sample(rp, ci, v, b, 5, threads)
+    times = []
+    for _ in range(args.steps):
+        dt, it = reference_cpu_sample(rp, ci, v, b, args.cpu_sample_iters, threads)
+        times.append(dt / max(it, 1))
+    per_iter = float(np.median(times))
+    value = 1.0 / (per_iter * n_full)
+    return {"impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": per_iter * n_full * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+            "config": {"workload": f"var-kappa Poisson {args.n_side}^2 5-point, sigma={SIGMA}, "
+                                   f"rtol {TOL}, reference CGSolver + JacobiPreconditioner",
+                       "n": len(rp) - 1, "nnz": len(v)},
+            "cpu_baseline": {"value": value, "unit": "solves/s", "cores": threads,
+                             "kind": "reference",
+                             "sample": f"{args.cpu_sample_iters} CG iterations per step, "
+                                       f"scaled to the {n_full} iterations of the full solve"},
+            "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        out = run_reference(args, rank, world)
+        if out is not None:
+            print(json.dumps(out), flush=True)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+
+        torch.cuda.set_device(local)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                             device_id=torch.device("cuda", local))
+    out, data = run_ours(args, rank, world, local)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        iters_fp64 = out["iterations"] if out["config"]["solver"] == "cg_jacobi" else fp64_cg_iterations(data)
+        out["cpu_baseline"] = cpu_baseline(args, data, iters_fp64)
+    if world > 1:
+        import torch
+
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()

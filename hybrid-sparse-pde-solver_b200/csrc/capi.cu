@@ -4,6 +4,7 @@
 #include <cmath>
 #include <cstring>
 #include <string>
+#include <vector>
 
 #include "krylov.cuh"
 #include "nvml_energy.cuh"
@@ -107,6 +108,7 @@ int hamlss_ctx_create(int device, hamlss_ctx** out) {
         c->c.device = device;
         HAMLSS_CUDA(cudaDeviceGetAttribute(&c->c.sm_count, cudaDevAttrMultiProcessorCount, device));
         lane_init(c->c.lane, c->c.sm_count);
+        c->c.lane.prof = &c->c.prof;
         HAMLSS_CUDA(cudaEventCreate(&c->c.ev0));
         HAMLSS_CUDA(cudaEventCreate(&c->c.ev1));
         c->c.host_poll.alloc(4096);
@@ -120,6 +122,7 @@ int hamlss_ctx_destroy(hamlss_ctx* ctx) {
         if (!ctx) return HAMLSS_OK;
         cudaSetDevice(ctx->c.device);
         lane_destroy(ctx->c.lane);
+        for (auto e : ctx->c.prof.ev) cudaEventDestroy(e);
         if (ctx->c.ev0) cudaEventDestroy(ctx->c.ev0);
         if (ctx->c.ev1) cudaEventDestroy(ctx->c.ev1);
         delete ctx;
@@ -139,6 +142,50 @@ int hamlss_ctx_stream(hamlss_ctx* ctx, void** stream) {
     if (!ctx || !stream) return set_err(HAMLSS_ERR_INVALID, "null argument");
     *stream = (void*)ctx->c.lane.stream;
     return HAMLSS_OK;
+}
+
+int hamlss_profile_enable(hamlss_ctx* ctx, int enable, int32_t max_launches) {
+    return guarded([&]() -> int {
+        if (!ctx) return set_err(HAMLSS_ERR_INVALID, "null context");
+        Profiler& P = ctx->c.prof;
+        HAMLSS_CUDA(cudaStreamSynchronize(ctx->c.lane.stream));
+        P.marks.clear();
+        P.next = 0;
+        P.on = enable != 0;
+        if (P.on) P.reserve(std::max(1, max_launches));
+        return HAMLSS_OK;
+    });
+}
+
+int hamlss_profile_read(hamlss_ctx* ctx, int32_t cap, char* names, int32_t* launches,
+                        double* total_ms, double* total_bytes, int32_t* count) {
+    return guarded([&]() -> int {
+        if (!ctx || !count) return set_err(HAMLSS_ERR_INVALID, "null argument");
+        Profiler& P = ctx->c.prof;
+        HAMLSS_CUDA(cudaStreamSynchronize(ctx->c.lane.stream));
+        std::vector<std::string> fam;
+        std::vector<int> nl;
+        std::vector<double> ms, by;
+        for (auto& m : P.marks) {
+            float t = 0.f;
+            HAMLSS_CUDA(cudaEventElapsedTime(&t, P.ev[m.e0], P.ev[m.e0 + 1]));
+            size_t k = 0;
+            while (k < fam.size() && fam[k] != m.name) ++k;
+            if (k == fam.size()) { fam.push_back(m.name); nl.push_back(0); ms.push_back(0); by.push_back(0); }
+            nl[k] += 1;
+            ms[k] += t;
+            by[k] += m.bytes;
+        }
+        int32_t c = 0;
+        for (size_t k = 0; k < fam.size() && c < cap; ++k, ++c) {
+            if (names) { std::strncpy(names + 32 * c, fam[k].c_str(), 31); names[32 * c + 31] = 0; }
+            if (launches) launches[c] = nl[k];
+            if (total_ms) total_ms[c] = ms[k];
+            if (total_bytes) total_bytes[c] = by[k];
+        }
+        *count = c;
+        return HAMLSS_OK;
+    });
 }
 
 // ------------------------------------------------------------------------- matrix
@@ -418,6 +465,21 @@ int hamlss_precond_release(hamlss_prec* M) {
         cudaStreamSynchronize(M->ctx->c.lane.stream);
         delete M;
         return HAMLSS_OK;
+    });
+}
+
+int hamlss_ilu_factors(const hamlss_prec* M, double* lu_values) {
+    return guarded([&]() -> int {
+        if (!M || !lu_values) return set_err(HAMLSS_ERR_INVALID, "null argument");
+        return ilu_copy_factors(M->p.get(), lu_values, M->ctx->c.lane.stream);
+    });
+}
+
+int hamlss_ilu_levels(const hamlss_prec* M, int32_t which, int32_t* level, int32_t* n_levels) {
+    return guarded([&]() -> int {
+        if (!M || !level || !n_levels || (which != 0 && which != 1))
+            return set_err(HAMLSS_ERR_INVALID, "bad arguments");
+        return ilu_copy_levels(M->p.get(), which, level, n_levels, M->ctx->c.lane.stream);
     });
 }
 

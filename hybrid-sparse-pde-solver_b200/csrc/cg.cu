@@ -268,6 +268,7 @@ SolveResult cg_impl(Ctx& ctx, hamlss_mat* A, Prec* M, const T* b, T* x, double t
     T* p[2] = {wvec<T>(ws, 2, n), wvec<T>(ws, 3, n)};
     T* q = wvec<T>(ws, 4, n);
     const T* dinv = JAC ? jacobi_diag<T>(ctx, M) : nullptr;
+    const double wb = (double)sizeof(T) * n;     // bytes of one vector
     ws.state.ensure(sizeof(CgState));
     CgState* s = reinterpret_cast<CgState*>(ws.state.p);
     int* halt = &s->halt;
@@ -282,9 +283,9 @@ SolveResult cg_impl(Ctx& ctx, hamlss_mat* A, Prec* M, const T* b, T* x, double t
 
     auto restart_seq = [&](bool first) {
         launch_spmv<T, 2>(sm, L, Ad, XVec<T>{x}, EpiInitRes<T>{b, r}, FinInit{s, first},
-                          first ? nullptr : halt);
+                          first ? nullptr : halt, "cg_residual", 3.0 * wb);
         if (!JAC && M) precond_apply<T>(ctx, M, r, z, halt);
-        launch_vec<1>(sm, L, n, BodyRho<T, JAC>{r, z, dinv}, FinRho{s}, halt);
+        launch_vec<1>(sm, L, n, BodyRho<T, JAC>{r, z, dinv}, FinRho{s}, halt, "cg_dot", 2.0 * wb);
     };
     auto poll = [&](CgState& h) {
         HAMLSS_CUDA(cudaMemcpyAsync(ctx.host_poll.p, s, sizeof(CgState), cudaMemcpyDeviceToHost, st));
@@ -304,12 +305,13 @@ SolveResult cg_impl(Ctx& ctx, hamlss_mat* A, Prec* M, const T* b, T* x, double t
             T* pold = p[parity];
             T* pnew = p[parity ^ 1];
             XP<T, JAC> xp{JAC ? r : z, dinv, pold, s, 0.0};
-            launch_spmv<T, 1>(sm, L, Ad, xp, EpiQ<T, JAC>{xp, pnew, q}, FinPQ{s}, halt);
+            launch_spmv<T, 1>(sm, L, Ad, xp, EpiQ<T, JAC>{xp, pnew, q}, FinPQ{s}, halt,
+                              "cg_spmv", (JAC ? 5.0 : 4.0) * wb);
             launch_vec<JAC ? 2 : 1>(sm, L, n, BodyUpd<T, JAC>{x, r, pnew, q, dinv, s, 0.0},
-                                    FinUpd<JAC>{s}, halt);
+                                    FinUpd<JAC>{s}, halt, "cg_update", (JAC ? 7.0 : 6.0) * wb);
             if (!JAC) {
                 if (M) precond_apply<T>(ctx, M, r, z, halt);
-                launch_vec<1>(sm, L, n, BodyRz<T>{r, z}, FinRz{s}, halt);
+                launch_vec<1>(sm, L, n, BodyRz<T>{r, z}, FinRz{s}, halt, "cg_dot", 2.0 * wb);
             }
             parity ^= 1;
         }

@@ -109,6 +109,7 @@ void ensure_diag(Ctx& ctx, hamlss_mat* M) {
     if (M->diag_valid) return;
     M->diag.ensure(M->A.n);
     if (M->A.n) {
+        ProfScope ps(ctx.lane, "setup", 16.0 * M->A.n + 12.0 * M->A.nnz);
         k_diag<<<std::min(ceil_div(M->A.n, 256), ctx.sm_count * 8), 256, 0, ctx.lane.stream>>>(
             M->A.n, M->A.rp.p, M->A.ci.p, M->A.v.p, M->diag.p);
         HAMLSS_LAUNCH_CHECK();
@@ -119,6 +120,7 @@ void ensure_diag(Ctx& ctx, hamlss_mat* M) {
 // ---------------------------------------------------------------------------- Jacobi
 void JacobiPrec::apply(Ctx& ctx, const Lane& L, const double* r, double* z, const int* gate) {
     if (!n) return;
+    ProfScope ps(L, "jacobi", 24.0 * n);
     k_jacobi_apply<double><<<std::min(ceil_div(n, 256), ctx.sm_count * 8), 256, 0, L.stream>>>(
         n, inv.p, r, z, gate);
     HAMLSS_LAUNCH_CHECK();
@@ -137,6 +139,7 @@ void JacobiPrec::prepare32(Ctx& ctx) {
 void JacobiPrec::apply32(Ctx& ctx, const Lane& L, const float* r, float* z, const int* gate) {
     prepare32(ctx);
     if (!n) return;
+    ProfScope ps(L, "jacobi", 12.0 * n);
     k_jacobi_apply<float><<<std::min(ceil_div(n, 256), ctx.sm_count * 8), 256, 0, L.stream>>>(
         n, inv32.p, r, z, gate);
     HAMLSS_LAUNCH_CHECK();
@@ -152,6 +155,7 @@ std::unique_ptr<Prec> make_jacobi(Ctx& ctx, hamlss_mat* A, double omega) {
     int init = 0x7fffffff;
     bad.upload(&init, 1, ctx.lane.stream);
     if (J->n) {
+        ProfScope ps(ctx.lane, "setup", 16.0 * J->n);
         k_jacobi_setup<<<std::min(ceil_div(J->n, 256), ctx.sm_count * 8), 256, 0, ctx.lane.stream>>>(
             J->n, A->diag.p, omega, J->inv.p, bad.p);
         HAMLSS_LAUNCH_CHECK();

@@ -9,19 +9,61 @@
 
 namespace hamlss {
 
+// Optional per-launch timing: when enabled, each engine launch is bracketed by a pair of
+// CUDA events on its own stream and tagged with its kernel family and the algorithmic
+// bytes it must move.  Used by bench.py for the live roofline figure.
+struct Profiler {
+    bool on = false;
+    std::vector<cudaEvent_t> ev;
+    size_t next = 0;
+    struct Mark { const char* name; double bytes; size_t e0; };
+    std::vector<Mark> marks;
+    void reserve(size_t pairs) {
+        while (ev.size() < 2 * pairs) {
+            cudaEvent_t e;
+            HAMLSS_CUDA(cudaEventCreate(&e));
+            ev.push_back(e);
+        }
+    }
+    // returns the slot of the start event, or -1 when off / out of events
+    long begin(cudaStream_t s) {
+        if (!on || next + 2 > ev.size()) return -1;
+        HAMLSS_CUDA(cudaEventRecord(ev[next], s));
+        return (long)next;
+    }
+    void end(cudaStream_t s, long slot, const char* name, double bytes) {
+        if (slot < 0) return;
+        HAMLSS_CUDA(cudaEventRecord(ev[slot + 1], s));
+        marks.push_back(Mark{name, bytes, (size_t)slot});
+        next = slot + 2;
+    }
+};
+
 // A stream plus the scratch its reductions use.  Kernels on one lane run in order, so
 // one reducer (partials + ticket) per lane is enough.
 struct Lane {
     cudaStream_t stream = nullptr;
     DBuf<double> partials;
     DBuf<unsigned> ticket;
+    Profiler* prof = nullptr;
     Reducer red() const { return Reducer{partials.p, ticket.p}; }
+};
+
+struct ProfScope {
+    const Lane& L;
+    long slot;
+    const char* name;
+    double bytes;
+    ProfScope(const Lane& l, const char* nm, double b)
+        : L(l), slot(l.prof ? l.prof->begin(l.stream) : -1), name(nm), bytes(b) {}
+    ~ProfScope() { if (L.prof) L.prof->end(L.stream, slot, name, bytes); }
 };
 
 struct Ctx {
     int device = 0;
     int sm_count = 148;
     Lane lane;
+    Profiler prof;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     HBuf<char> host_poll;      // pinned landing zone for polled device state
     std::mutex mu;
@@ -62,9 +104,18 @@ struct DevMat {
     Csr<float> f32(cudaStream_t s);
 };
 
+// Algorithmic bytes of one CSR SpMV pass: row_ptr + (index + value) per nonzero; the
+// vector traffic is added by the caller (vec_bytes; default: read x once, write y).
+template <typename T>
+double csr_bytes(const Csr<T>& A) {
+    return 4.0 * (A.n + 1) + (4.0 + sizeof(T)) * (double)A.nnz;
+}
+
 template <typename T, int NRED, typename XOp, typename Epi, typename Fin = NoFin>
 void launch_spmv(int sm_count, const Lane& L, const Csr<T>& A, const XOp& xop, const Epi& epi,
-                 const Fin& fin = Fin{}, const int* gate = nullptr) {
+                 const Fin& fin = Fin{}, const int* gate = nullptr, const char* name = "spmv",
+                 double vec_bytes = -1.0) {
+    ProfScope ps(L, name, csr_bytes(A) + (vec_bytes >= 0 ? vec_bytes : 2.0 * sizeof(T) * A.n));
     static int per_sm = 0;
     auto kern = k_spmv<T, NRED, XOp, Epi, Fin>;
     if (!per_sm) per_sm = std::min(occupancy_blocks(kern, kSpmvThreads), kMaxBlocksPerSm);
@@ -76,7 +127,8 @@ void launch_spmv(int sm_count, const Lane& L, const Csr<T>& A, const XOp& xop, c
 
 template <int NRED, typename Body, typename Fin = NoFin>
 void launch_vec(int sm_count, const Lane& L, int n, const Body& body, const Fin& fin = Fin{},
-                const int* gate = nullptr) {
+                const int* gate = nullptr, const char* name = "vec", double bytes = 0.0) {
+    ProfScope ps(L, name, bytes);
     int blocks = std::max(1, std::min(ceil_div(n, 256), sm_count * kMaxBlocksPerSm));
     k_vec<NRED, Body, Fin><<<blocks, 256, 0, L.stream>>>(n, body, L.red(), fin, gate);
     HAMLSS_LAUNCH_CHECK();

@@ -36,6 +36,9 @@ std::unique_ptr<Prec> make_jacobi(Ctx& ctx, hamlss_mat* A, double omega);
 std::unique_ptr<Prec> make_ilu0(Ctx& ctx, hamlss_mat* A);
 std::unique_ptr<Prec> make_amg(Ctx& ctx, hamlss_mat* A, const hamlss_params& p);
 
+int ilu_copy_factors(const Prec* M, double* out, cudaStream_t s);
+int ilu_copy_levels(const Prec* M, int which, int* level, int* nlev, cudaStream_t s);
+
 // Extract a_ii into A->diag (once per value version).
 void ensure_diag(Ctx& ctx, hamlss_mat* A);
 

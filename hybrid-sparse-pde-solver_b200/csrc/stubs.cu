@@ -1,9 +1,7 @@
 // stubs.cu -- temporary: solvers not yet implemented.
 #include "krylov.cuh"
 namespace hamlss {
-std::unique_ptr<Prec> make_ilu0(Ctx&, hamlss_mat*) { fail(HAMLSS_ERR_INVALID, "ILU(0) not built yet"); }
 std::unique_ptr<Prec> make_amg(Ctx&, hamlss_mat*, const hamlss_params&) { fail(HAMLSS_ERR_INVALID, "AMG not built yet"); }
-SolveResult fgmres_solve(Ctx&, hamlss_mat*, Prec*, const double*, double*, double, int, int, Workspace&) { fail(HAMLSS_ERR_INVALID, "FGMRES not built yet"); }
 SolveResult mixed_solve(Ctx&, int, hamlss_mat*, Prec*, const double*, double*, const hamlss_params&, Workspace&, int*) { fail(HAMLSS_ERR_INVALID, "mixed not built yet"); }
 }
 extern "C" {
@@ -12,6 +10,4 @@ int hamlss_extract_features(hamlss_ctx*, const hamlss_mat*, double*, int32_t*) {
 int hamlss_amg_aggregate(hamlss_ctx*, const hamlss_mat*, double, int32_t*, int32_t*) { return HAMLSS_ERR_INVALID; }
 int hamlss_amg_num_levels(const hamlss_prec*, int32_t*) { return HAMLSS_ERR_INVALID; }
 int hamlss_amg_level_matrix(const hamlss_prec*, int32_t, int32_t, int32_t*, int32_t*, int32_t*, int32_t*, int32_t*, double*) { return HAMLSS_ERR_INVALID; }
-int hamlss_ilu_factors(const hamlss_prec*, double*) { return HAMLSS_ERR_INVALID; }
-int hamlss_ilu_levels(const hamlss_prec*, int32_t, int32_t*, int32_t*) { return HAMLSS_ERR_INVALID; }
 }

@@ -164,6 +164,8 @@ def _declare(L: C.CDLL) -> None:
         "hamlss_ctx_destroy": (C.c_int, [P]),
         "hamlss_ctx_synchronize": (C.c_int, [P]),
         "hamlss_ctx_stream": (C.c_int, [P, pp]),
+        "hamlss_profile_enable": (C.c_int, [P, C.c_int, I32]),
+        "hamlss_profile_read": (C.c_int, [P, I32, V, V, V, V, pi]),
         "hamlss_mat_upload": (C.c_int, [P, I32, I32, I32, V, V, V, C.c_int, pp]),
         "hamlss_mat_update_values": (C.c_int, [P, V, C.c_int]),
         "hamlss_mat_info": (C.c_int, [P, pi, pi, pi]),

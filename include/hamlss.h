@@ -157,6 +157,17 @@ int hamlss_ctx_synchronize(hamlss_ctx* ctx);
 /* The context's cudaStream_t, as an opaque pointer, so callers can order their own work. */
 int hamlss_ctx_stream(hamlss_ctx* ctx, void** stream);
 
+/* Measurement support (no counterpart in the reference): when enabled, every engine
+ * launch on this context is bracketed by a pair of CUDA events on the context stream and
+ * tagged with its kernel family and the algorithmic bytes it must move.  Up to
+ * max_launches launches are recorded; enabling again clears the record. */
+int hamlss_profile_enable(hamlss_ctx* ctx, int enable, int32_t max_launches);
+/* Totals per kernel family, at most `cap` families: names[i*32..] (NUL-terminated),
+ * launches[i], total_ms[i] (sum of event-measured durations), total_bytes[i]
+ * (algorithmic).  *count = number of families written.  Synchronises the stream. */
+int hamlss_profile_read(hamlss_ctx* ctx, int32_t cap, char* names, int32_t* launches,
+                        double* total_ms, double* total_bytes, int32_t* count);
+
 /* -------------------------------------------------------------------- matrix
  * Replaces hsps::SparseMatrix(rows, cols, row_ptr, col_idx, values)
  * (sparse_matrix.cpp:22-27): a deep copy into device memory.  The engine keeps the
