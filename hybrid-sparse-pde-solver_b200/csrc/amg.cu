@@ -1,0 +1,952 @@
+// amg.cu -- smoothed-aggregation AMG on the device (AMGPreconditioner, amg.cpp).
+//
+// Setup (amg.cpp:183-237), every step a device kernel:
+//   aggregate   greedy aggregation of amg.cpp:30-67, bit for bit.  The sequential pass
+//               makes node i a seed iff no earlier seed s < i holds i as a strong, still
+//               unassigned neighbour, where strong means |a_si| >= theta * max_{l != s}|a_sl|.
+//               Every node before s is assigned when s is visited, so this is exactly:
+//                 seed(i)  <=>  no seed in IN(i) = { s < i : s -> i strong }
+//                 agg(i)    =  number of seeds before i            (seed)
+//                           =  agg(min seed in IN(i))              (otherwise)
+//               IN(i) only holds lower indices, so the decisions follow the DAG's
+//               topological levels: one cooperative kernel pops each level's frontier
+//               (Kahn order), one grid barrier per level, then a scan numbers the seeds.
+//   prolong     Jacobi-smoothed tentative prolongation (amg.cpp:101-178) computed
+//               sparsely: row i starts at e_agg(i) and subtracts (omega/a_ii) a_ij at column
+//               agg(j) in row order, then drops |v| <= 1e-14.  Same operations in the same
+//               order as the reference's dense buffer, so P is identical bit for bit.
+//   transpose   R = P^T with rows in increasing fine index (sparse_matrix.cpp:138-165).
+//   Galerkin    A_c = R (A P) by a row-wise k-way merge SpGEMM: each output column sums
+//               its products in the order of the left row, starting from 0.0, and drops
+//               |v| <= eps^2 (sparse_matrix.cpp:171-237) -- bit for bit again.
+//   coarsest    dense LU with partial pivoting, factored once (amg.cpp:260-291 redoes it
+//               every cycle; the pivots and multipliers are the same).
+// V-cycle (amg.cpp:296-343), FP64 (bit-exact with the reference) or FP32 (mixed
+// precision): the first pre-smoothing sweep on x = 0 is the elementwise x = w D^-1 b and is
+// fused into the restriction that produces b; every other sweep, the residual, the
+// restriction and the prolongation+correction are single fused SpMV passes.
+#include <cooperative_groups.h>
+
+#include <climits>
+#include <cmath>
+#include <cstring>
+
+#include "krylov.cuh"
+#include "scan.cuh"
+
+namespace cg = cooperative_groups;
+
+namespace hamlss {
+
+namespace {
+
+constexpr double kEps = 2.220446049250313e-16;
+
+struct DCsr {
+    int n = 0, m = 0, nnz = 0;
+    DBuf<int> rp, ci;
+    DBuf<double> v;
+    DBuf<float> v32;
+    Csr<double> f64() const { return Csr<double>{n, m, nnz, rp.p, ci.p, v.p}; }
+    Csr<float> f32() const { return Csr<float>{n, m, nnz, rp.p, ci.p, v32.p}; }
+};
+
+inline int grid_for(Ctx& ctx, long long n) {
+    return std::max(1, std::min(ceil_div(n, 256), ctx.sm_count * 8));
+}
+
+// ------------------------------------------------------------------ aggregation
+__global__ void k_rowmax(int n, const int* __restrict__ rp, const int* __restrict__ ci,
+                         const double* __restrict__ v, double* rmax) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double m = 0.0;
+        for (int k = rp[i]; k < rp[i + 1]; ++k)
+            if (ci[k] != i) m = fmax(m, fabs(v[k]));
+        rmax[i] = m;
+    }
+}
+
+// in_cnt[j] = |IN(j)|
+__global__ void k_in_count(int n, const int* __restrict__ rp, const int* __restrict__ ci,
+                           const double* __restrict__ v, const double* __restrict__ rmax,
+                           double theta, int* in_cnt) {
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+        const double th = theta * rmax[s];
+        for (int k = rp[s]; k < rp[s + 1]; ++k) {
+            int j = ci[k];
+            if (j > s && fabs(v[k]) >= th) atomicAdd(&in_cnt[j], 1);
+        }
+    }
+}
+
+__global__ void k_in_fill(int n, const int* __restrict__ rp, const int* __restrict__ ci,
+                          const double* __restrict__ v, const double* __restrict__ rmax,
+                          double theta, int* fillpos, int* in_src) {
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+        const double th = theta * rmax[s];
+        for (int k = rp[s]; k < rp[s + 1]; ++k) {
+            int j = ci[k];
+            if (j > s && fabs(v[k]) >= th) in_src[atomicAdd(&fillpos[j], 1)] = s;
+        }
+    }
+}
+
+// Decide seed / non-seed in the topological order of the IN-DAG.
+// status: 1 seed, 2 non-seed.  indeg starts at |IN(i)|; order/cnt are frontier storage.
+__global__ void k_aggregate_levels(int n, const int* __restrict__ rp, const int* __restrict__ ci,
+                                   const double* __restrict__ v, const double* __restrict__ rmax,
+                                   double theta, const int* __restrict__ in_rp,
+                                   const int* __restrict__ in_src, int* indeg, int* status,
+                                   int* order, int* cnt, int* nlev) {
+    cg::grid_group grid = cg::this_grid();
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nth = gridDim.x * blockDim.x;
+    for (int i = tid; i < n; i += nth)
+        if (indeg[i] == 0) order[atomicAdd(&cnt[0], 1)] = i;
+    grid.sync();
+    int start = 0;
+    for (int l = 0;; ++l) {
+        const int c = *(volatile int*)&cnt[l];
+        if (c == 0) {
+            if (tid == 0) *nlev = l;
+            break;
+        }
+        const int next = start + c;
+        for (int t = tid; t < c; t += nth) {
+            const int i = order[start + t];
+            bool captured = false;
+            for (int k = in_rp[i]; k < in_rp[i + 1]; ++k)
+                if (status[in_src[k]] == 1) { captured = true; break; }
+            status[i] = captured ? 2 : 1;
+            const double th = theta * rmax[i];
+            for (int k = rp[i]; k < rp[i + 1]; ++k) {
+                const int d = ci[k];
+                if (d > i && fabs(v[k]) >= th)
+                    if (atomicSub(&indeg[d], 1) == 1) order[next + atomicAdd(&cnt[l + 1], 1)] = d;
+            }
+        }
+        start = next;
+        grid.sync();
+    }
+}
+
+__global__ void k_seed_flags(int n, const int* __restrict__ status, int* flag) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        flag[i] = status[i] == 1 ? 1 : 0;
+}
+
+// flag holds the exclusive seed count; assign every node
+__global__ void k_assign(int n, const int* __restrict__ status, const int* __restrict__ seedno,
+                         const int* __restrict__ in_rp, const int* __restrict__ in_src, int* agg) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        if (status[i] == 1) { agg[i] = seedno[i]; continue; }
+        int best = INT_MAX;
+        for (int k = in_rp[i]; k < in_rp[i + 1]; ++k) {
+            int s = in_src[k];
+            if (status[s] == 1 && s < best) best = s;
+        }
+        agg[i] = (best == INT_MAX) ? -1 : seedno[best];
+    }
+}
+
+// ------------------------------------------------------- smoothed prolongation
+// Row i of P: candidates in first-occurrence order: agg(i), then agg(j) for off-diagonal
+// j in row order.  Values computed exactly as amg.cpp:139-154 would for column c.
+__device__ double p_value(int i, int c, int s, int e, const int* __restrict__ ci,
+                          const double* __restrict__ v, const int* __restrict__ agg, double id,
+                          bool raw) {
+    double val = (c == agg[i]) ? 1.0 : 0.0;
+    if (raw) return val;
+    for (int k = s; k < e; ++k) {
+        int j = ci[k];
+        if (j == i) continue;
+        if (agg[j] == c) val = __dsub_rn(val, __dmul_rn(id, v[k]));
+    }
+    return val;
+}
+
+template <bool FILL>
+__global__ void k_smooth_p(int n, const int* __restrict__ rp, const int* __restrict__ ci,
+                           const double* __restrict__ v, const int* __restrict__ agg, double omega,
+                           int* pcnt, const int* __restrict__ prp, int* pci, double* pv) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int s = rp[i], e = rp[i + 1];
+        double id = 0.0;
+        for (int k = s; k < e; ++k)
+            if (ci[k] == i) { id = (fabs(v[k]) > kEps) ? omega / v[k] : 0.0; break; }
+        const bool raw = fabs(id) < kEps;
+        // candidate list: index -1 = agg(i), then off-diagonal entries
+        int count = 0;
+        for (int a = -1; a < e - s; ++a) {
+            int c;
+            if (a < 0) c = agg[i];
+            else { int j = ci[s + a]; if (j == i || raw) continue; c = agg[j]; }
+            // first occurrence?
+            bool first = (a < 0) || (c != agg[i]);
+            if (first && a >= 0)
+                for (int b = 0; b < a; ++b) {
+                    int jb = ci[s + b];
+                    if (jb != i && agg[jb] == c) { first = false; break; }
+                }
+            if (!first) continue;
+            double val = p_value(i, c, s, e, ci, v, agg, id, raw);
+            if (!(fabs(val) > 1e-14)) continue;
+            if (FILL) {
+                // rank among surviving candidates with a smaller column
+                int rank = 0;
+                for (int a2 = -1; a2 < e - s; ++a2) {
+                    int c2;
+                    if (a2 < 0) c2 = agg[i];
+                    else { int j2 = ci[s + a2]; if (j2 == i || raw) continue; c2 = agg[j2]; }
+                    if (c2 >= c) continue;
+                    bool f2 = (a2 < 0) || (c2 != agg[i]);
+                    if (f2 && a2 >= 0)
+                        for (int b = 0; b < a2; ++b) {
+                            int jb = ci[s + b];
+                            if (jb != i && agg[jb] == c2) { f2 = false; break; }
+                        }
+                    if (!f2) continue;
+                    if (fabs(p_value(i, c2, s, e, ci, v, agg, id, raw)) > 1e-14) ++rank;
+                }
+                pci[prp[i] + rank] = c;
+                pv[prp[i] + rank] = val;
+            }
+            ++count;
+        }
+        if (!FILL) pcnt[i] = count;
+    }
+}
+
+// ------------------------------------------------------------------- transpose
+__global__ void k_t_count(int n, const int* __restrict__ rp, const int* __restrict__ ci, int* cnt) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        for (int k = rp[i]; k < rp[i + 1]; ++k) atomicAdd(&cnt[ci[k]], 1);
+}
+
+__global__ void k_t_fill(int n, const int* __restrict__ rp, const int* __restrict__ ci,
+                         const double* __restrict__ v, int* fillpos, int* tci, double* tv) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        for (int k = rp[i]; k < rp[i + 1]; ++k) {
+            int p = atomicAdd(&fillpos[ci[k]], 1);
+            tci[p] = i;
+            tv[p] = v[k];
+        }
+}
+
+// rows of the transpose hold distinct source rows: sort each by index
+__global__ void k_t_sort(int m, const int* __restrict__ trp, int* tci, double* tv) {
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < m; r += gridDim.x * blockDim.x) {
+        const int s = trp[r], e = trp[r + 1];
+        for (int a = s + 1; a < e; ++a) {
+            int c = tci[a];
+            double x = tv[a];
+            int b = a - 1;
+            while (b >= s && tci[b] > c) { tci[b + 1] = tci[b]; tv[b + 1] = tv[b]; --b; }
+            tci[b + 1] = c;
+            tv[b + 1] = x;
+        }
+    }
+}
+
+// -------------------------------------------------------------------- SpGEMM
+// Row i of C = A B by a k-way merge of the rows of B selected by row i of A.  Each output
+// column is the sum, starting at 0.0, of a_ij * b_jl in the order of row i of A, with
+// separate multiply and add: mat_mat_product's dense accumulator (sparse_matrix.cpp:196-212)
+// value for value.  Rows of A longer than kHeads keep their merge heads in `heads`
+// (3 ints per nonzero of A at 3 * rp[i]).
+constexpr int kHeads = 24;
+
+template <bool FILL>
+__global__ void k_spgemm(int m, const int* __restrict__ arp, const int* __restrict__ aci,
+                         const double* __restrict__ av, const int* __restrict__ brp,
+                         const int* __restrict__ bci, const double* __restrict__ bv, int* ccnt,
+                         const int* __restrict__ crp, int* cci, double* cv, int* heads) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+        const int s = arp[i], k = arp[i + 1] - s;
+        int lpos[kHeads], lend[kHeads], lcur[kHeads];
+        int* pos = k <= kHeads ? lpos : heads + 3LL * s;
+        int* end = k <= kHeads ? lend : heads + 3LL * s + k;
+        int* cur = k <= kHeads ? lcur : heads + 3LL * s + 2 * k;
+        for (int t = 0; t < k; ++t) {
+            int j = aci[s + t];
+            pos[t] = brp[j];
+            end[t] = brp[j + 1];
+            cur[t] = pos[t] < end[t] ? bci[pos[t]] : INT_MAX;
+        }
+        int o = FILL ? crp[i] : 0;
+        for (;;) {
+            int cmin = INT_MAX;
+            for (int t = 0; t < k; ++t) cmin = min(cmin, cur[t]);
+            if (cmin == INT_MAX) break;
+            double sum = 0.0;
+            for (int t = 0; t < k; ++t) {
+                if (cur[t] != cmin) continue;
+                sum = __dadd_rn(sum, __dmul_rn(av[s + t], bv[pos[t]]));
+                ++pos[t];
+                cur[t] = pos[t] < end[t] ? bci[pos[t]] : INT_MAX;
+            }
+            if (fabs(sum) > kEps * kEps) {
+                if (FILL) { cci[o] = cmin; cv[o] = sum; }
+                ++o;
+            }
+        }
+        if (!FILL) ccnt[i] = o;
+    }
+}
+
+__global__ void k_inv_diag(int n, const int* __restrict__ rp, const int* __restrict__ ci,
+                           const double* __restrict__ v, double* dinv) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double d = 0.0;
+        for (int k = rp[i]; k < rp[i + 1]; ++k)
+            if (ci[k] == i) { d = v[k]; break; }
+        dinv[i] = (fabs(d) > kEps) ? 1.0 / d : 0.0;     // amg.cpp:192-195
+    }
+}
+
+__global__ void k_d2f(const double* __restrict__ a, float* b, long long n) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        b[i] = (float)a[i];
+}
+
+// ------------------------------------------------------------- coarsest level
+// Dense Gaussian elimination with partial pivoting (amg.cpp:260-291), one block, on the
+// n x n matrix M (row-major).  Stores the multipliers below the diagonal, the pivot row
+// of each column and whether the column was skipped (|pivot| < 1e-14).
+__global__ void k_dense_factor(int n, double* M, int* piv, int* skip) {
+    __shared__ int sp;
+    for (int col = 0; col < n; ++col) {
+        if (threadIdx.x == 0) {
+            int p = col;
+            for (int r = col + 1; r < n; ++r)
+                if (fabs(M[(size_t)r * n + col]) > fabs(M[(size_t)p * n + col])) p = r;
+            piv[col] = p;
+            sp = p;
+        }
+        __syncthreads();
+        const int p = sp;
+        // columns < col hold multipliers that belong to the row position at their step
+        if (p != col)
+            for (int c = col + threadIdx.x; c < n; c += blockDim.x) {
+                double t = M[(size_t)col * n + c];
+                M[(size_t)col * n + c] = M[(size_t)p * n + c];
+                M[(size_t)p * n + c] = t;
+            }
+        __syncthreads();
+        const double d = M[(size_t)col * n + col];
+        const bool sk = fabs(d) < 1e-14;
+        if (threadIdx.x == 0) skip[col] = sk;
+        if (!sk) {
+            const double inv = 1.0 / d;
+            for (int r = col + 1 + threadIdx.x; r < n; r += blockDim.x) {
+                double f = __dmul_rn(M[(size_t)r * n + col], inv);
+                for (int c = col + 1; c < n; ++c)
+                    M[(size_t)r * n + c] = __dsub_rn(M[(size_t)r * n + c], __dmul_rn(f, M[(size_t)col * n + c]));
+                M[(size_t)r * n + col] = f;       // multiplier (the reference's entry becomes 0)
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// x = A^-1 b with the stored factors, one warp, the reference's operation order.
+template <typename T>
+__global__ void k_dense_solve(int n, const double* __restrict__ M, const int* __restrict__ piv,
+                              const int* __restrict__ skip, const T* __restrict__ b, T* x,
+                              double* work, const int* gate) {
+    if (gate && *(volatile const int*)gate) return;
+    double* y = work;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) y[i] = (double)b[i];
+    __syncwarp();
+    for (int col = 0; col < n; ++col) {
+        const int p = piv[col];
+        if (p != col && threadIdx.x == 0) { double t = y[col]; y[col] = y[p]; y[p] = t; }
+        __syncwarp();
+        if (!skip[col]) {
+            const double yc = y[col];
+            for (int r = col + 1 + threadIdx.x; r < n; r += blockDim.x)
+                y[r] = __dsub_rn(y[r], __dmul_rn(M[(size_t)r * n + col], yc));
+        }
+        __syncwarp();
+    }
+    if (threadIdx.x == 0) {
+        for (int i = n - 1; i >= 0; --i) {
+            double s = y[i];
+            for (int j = i + 1; j < n; ++j) s = __dsub_rn(s, __dmul_rn(M[(size_t)i * n + j], y[n + j]));
+            double d = M[(size_t)i * n + i];
+            y[n + i] = (fabs(d) > 1e-14) ? s / d : 0.0;
+        }
+    }
+    __syncwarp();
+    for (int i = threadIdx.x; i < n; i += blockDim.x) x[i] = (T)y[n + i];
+}
+
+// Columns of the inverse, one warp per unit right-hand side e_k: Minv[r][k].
+__global__ void k_dense_inverse(int n, const double* __restrict__ M, const int* __restrict__ piv,
+                                const int* __restrict__ skip, double* work, double* Minv) {
+    const int k = blockIdx.x;
+    double* y = work + (size_t)k * 2 * n;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) y[i] = (i == k) ? 1.0 : 0.0;
+    __syncwarp();
+    for (int col = 0; col < n; ++col) {
+        const int p = piv[col];
+        if (p != col && threadIdx.x == 0) { double t = y[col]; y[col] = y[p]; y[p] = t; }
+        __syncwarp();
+        if (!skip[col]) {
+            const double yc = y[col];
+            for (int r = col + 1 + threadIdx.x; r < n; r += blockDim.x)
+                y[r] = __dsub_rn(y[r], __dmul_rn(M[(size_t)r * n + col], yc));
+        }
+        __syncwarp();
+    }
+    if (threadIdx.x == 0) {
+        for (int i = n - 1; i >= 0; --i) {
+            double t = y[i];
+            for (int j = i + 1; j < n; ++j) t = __dsub_rn(t, __dmul_rn(M[(size_t)i * n + j], y[n + j]));
+            double d = M[(size_t)i * n + i];
+            y[n + i] = (fabs(d) > 1e-14) ? t / d : 0.0;
+        }
+    }
+    __syncwarp();
+    for (int i = threadIdx.x; i < n; i += blockDim.x) Minv[(size_t)i * n + k] = y[n + i];
+}
+
+// Explicit inverse applied as a dense matrix-vector product (large coarsest levels).
+template <typename T>
+__global__ void k_dense_gemv(int n, const double* __restrict__ Minv, const T* __restrict__ b, T* x,
+                             const int* gate) {
+    if (gate && *(volatile const int*)gate) return;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int r = warp; r < n; r += nw) {
+        double s = 0.0;
+        for (int c = lane; c < n; c += 32) s += Minv[(size_t)r * n + c] * (double)b[c];
+        s = warp_sum(s);
+        if (lane == 0) x[r] = (T)s;
+    }
+}
+
+__global__ void k_csr_to_dense(int n, const int* __restrict__ rp, const int* __restrict__ ci,
+                               const double* __restrict__ v, double* M) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        for (int k = rp[i]; k < rp[i + 1]; ++k) M[(size_t)i * n + ci[k]] = v[k];
+}
+
+// ------------------------------------------------------------ V-cycle operators
+template <typename T>
+struct LevelVecs {
+    T* b;     // right-hand side on this level
+    T* x;     // iterate
+    T* x2;    // second buffer for Jacobi sweeps
+    T* r;     // residual
+    const T* dinv;
+};
+
+// x_new = x + (w dinv) (b - A x)        (amg.cpp:250-252)
+template <typename T>
+struct EpiSmooth {
+    const T* b;
+    const T* x;
+    T* xn;
+    const T* dinv;
+    T omega;
+    HAMLSS_NO_LOAD
+    template <int NV>
+    __device__ __forceinline__ void operator()(int i, double ax, double (&)[NV]) const {
+        if constexpr (sizeof(T) == 8) {
+            double t = __dmul_rn((double)omega, (double)dinv[i]);
+            xn[i] = __dadd_rn((double)x[i], __dmul_rn(t, __dsub_rn((double)b[i], ax)));
+        } else {
+            xn[i] = (T)((double)x[i] + (double)(omega * dinv[i]) * ((double)b[i] - ax));
+        }
+    }
+};
+
+// last post-smoothing sweep on level 0 inside PCG: also r.z for the CG scalar
+template <typename T>
+struct EpiSmoothDot {
+    EpiSmooth<T> s;
+    HAMLSS_NO_LOAD
+    template <int NV>
+    __device__ __forceinline__ void operator()(int i, double ax, double (&acc)[NV]) const {
+        s(i, ax, acc);
+        acc[0] += (double)s.b[i] * (double)s.xn[i];
+    }
+};
+
+// r = b - A x
+template <typename T>
+struct EpiResid {
+    const T* b;
+    T* r;
+    HAMLSS_NO_LOAD
+    template <int NV>
+    __device__ __forceinline__ void operator()(int i, double ax, double (&)[NV]) const {
+        if constexpr (sizeof(T) == 8) r[i] = __dsub_rn((double)b[i], ax);
+        else r[i] = (T)((double)b[i] - ax);
+    }
+};
+
+// b_c = R r ; first coarse pre-smoothing sweep from x_c = 0: x_c = (w dinv_c) b_c
+template <typename T>
+struct EpiRestrict {
+    T* bc;
+    T* xc;
+    const T* dinvc;
+    T omega;
+    bool smooth;     // false when the coarse level is the direct-solve level
+    HAMLSS_NO_LOAD
+    template <int NV>
+    __device__ __forceinline__ void operator()(int i, double ax, double (&)[NV]) const {
+        T bi = (T)ax;
+        bc[i] = bi;
+        if (smooth) {
+            if constexpr (sizeof(T) == 8) xc[i] = __dmul_rn(__dmul_rn((double)omega, (double)dinvc[i]), (double)bi);
+            else xc[i] = (T)((double)(omega * dinvc[i]) * (double)bi);
+        }
+    }
+};
+
+// x += P e_c
+template <typename T>
+struct EpiProlong {
+    T* x;
+    HAMLSS_NO_LOAD
+    template <int NV>
+    __device__ __forceinline__ void operator()(int i, double ax, double (&)[NV]) const {
+        if constexpr (sizeof(T) == 8) x[i] = __dadd_rn((double)x[i], ax);
+        else x[i] = (T)((double)x[i] + ax);
+    }
+};
+
+template <typename T>
+struct BodyFirstSmooth {
+    const T* b;
+    T* x;
+    const T* dinv;
+    T omega;
+    HAMLSS_NO_LOAD
+    template <int NV>
+    __device__ __forceinline__ void operator()(int i, double (&)[NV]) const {
+        if constexpr (sizeof(T) == 8) x[i] = __dmul_rn(__dmul_rn((double)omega, (double)dinv[i]), (double)b[i]);
+        else x[i] = (T)((double)(omega * dinv[i]) * (double)b[i]);
+    }
+};
+
+template <typename T>
+struct BodyCopy {
+    const T* a;
+    T* b;
+    HAMLSS_NO_LOAD
+    template <int NV>
+    __device__ __forceinline__ void operator()(int i, double (&)[NV]) const { b[i] = a[i]; }
+};
+
+}  // namespace
+
+// ----------------------------------------------------------------- the object
+struct AmgLevel {
+    DCsr A;          // level >= 1 (level 0 uses the user's matrix)
+    DCsr P, R;
+    DBuf<double> dinv;
+    DBuf<float> dinv32;
+    DBuf<double> b, x, x2, r;
+    DBuf<float> b32, x32, x232, r32;
+    int n = 0;
+};
+
+struct AmgPrec : Prec {
+    hamlss_mat* A0 = nullptr;
+    std::vector<std::unique_ptr<AmgLevel>> lev;
+    double omega = 0.67;
+    int pre = 2, post = 2;
+    // coarsest dense data
+    int nc = 0;
+    bool coarse_inverse = false;
+    DBuf<double> Md, Minv, cwork;
+    DBuf<int> piv, skip;
+    bool f32_ready = false;
+
+    int levels() const { return (int)lev.size(); }
+
+    Csr<double> Aview64(int l) const { return l == 0 ? A0->A.f64() : lev[l]->A.f64(); }
+    Csr<float> Aview32(Ctx& ctx, int l) const {
+        return l == 0 ? A0->A.f32(ctx.lane.stream) : lev[l]->A.f32();
+    }
+
+    template <typename T>
+    LevelVecs<T> vecs(int l);
+
+    template <typename T>
+    Csr<T> Amat(Ctx& ctx, int l);
+    template <typename T>
+    Csr<T> Pmat(int l);
+    template <typename T>
+    Csr<T> Rmat(int l);
+
+    template <typename T>
+    void coarse_solve(Ctx& ctx, const Lane& L, const T* b, T* x, const int* gate) {
+        if (coarse_inverse) {
+            ProfScope ps(L, "amg_coarse", 8.0 * nc * nc);
+            k_dense_gemv<T><<<std::max(1, std::min(ceil_div(nc, 8), ctx.sm_count * 4)), 256, 0, L.stream>>>(
+                nc, Minv.p, b, x, gate);
+        } else {
+            ProfScope ps(L, "amg_coarse", 8.0 * nc * nc);
+            k_dense_solve<T><<<1, 32, 0, L.stream>>>(nc, Md.p, piv.p, skip.p, b, x, cwork.p, gate);
+        }
+        HAMLSS_LAUNCH_CHECK();
+    }
+
+    // One V-cycle: z = M^-1 r (z starts at 0).  rz: when non-null, the last level-0 sweep
+    // also accumulates r.z and hands the sum to `fin`.
+    template <typename T, typename Fin>
+    void vcycle(Ctx& ctx, const Lane& L, const T* rhs0, T* z, const int* gate, bool with_dot,
+                const Fin& fin) {
+        const int sm = ctx.sm_count;
+        const int nl = levels();
+        const T om = (T)omega;
+        const double w = sizeof(T);
+        if (nl == 1) {
+            coarse_solve<T>(ctx, L, rhs0, z, gate);
+            return;
+        }
+        // level 0: first pre-smoothing sweep from 0 (fused when pre >= 1)
+        for (int l = 0; l < nl - 1; ++l) {
+            LevelVecs<T> V = vecs<T>(l);
+            const T* b = l == 0 ? rhs0 : V.b;
+            T* x = l == 0 ? z : V.x;
+            const int n = lev[l]->n;
+            Csr<T> A = Amat<T>(ctx, l);
+            int done_sweeps = 0;
+            if (pre >= 1) {
+                if (l == 0) launch_vec<0>(sm, L, n, BodyFirstSmooth<T>{b, x, V.dinv, om}, NoFin{}, gate,
+                                          "amg_smooth", 3.0 * w * n);
+                done_sweeps = 1;   // levels >= 1 had it fused into the restriction
+            } else if (l == 0) {
+                HAMLSS_CUDA(cudaMemsetAsync(x, 0, sizeof(T) * n, L.stream));
+            }
+            for (int s = done_sweeps; s < pre; ++s) {
+                launch_spmv<T, 0>(sm, L, A, XVec<T>{x}, EpiSmooth<T>{b, x, V.x2, V.dinv, om}, NoFin{}, gate,
+                                  "amg_smooth", 4.0 * w * n);
+                launch_vec<0>(sm, L, n, BodyCopy<T>{V.x2, x}, NoFin{}, gate, "vec", 2.0 * w * n);
+            }
+            launch_spmv<T, 0>(sm, L, A, XVec<T>{x}, EpiResid<T>{b, V.r}, NoFin{}, gate, "amg_resid",
+                              3.0 * w * n);
+            LevelVecs<T> C = vecs<T>(l + 1);
+            const bool coarse_smooth = (l + 1 < nl - 1) && pre >= 1;
+            launch_spmv<T, 0>(sm, L, Rmat<T>(l), XVec<T>{V.r}, EpiRestrict<T>{C.b, C.x, C.dinv, om, coarse_smooth},
+                              NoFin{}, gate, "amg_restrict", w * n + (coarse_smooth ? 3.0 : 1.0) * w * lev[l + 1]->n);
+            if (!coarse_smooth && l + 1 < nl - 1)
+                HAMLSS_CUDA(cudaMemsetAsync(C.x, 0, sizeof(T) * lev[l + 1]->n, L.stream));
+        }
+        {
+            LevelVecs<T> C = vecs<T>(nl - 1);
+            coarse_solve<T>(ctx, L, C.b, C.x, gate);
+        }
+        for (int l = nl - 2; l >= 0; --l) {
+            LevelVecs<T> V = vecs<T>(l);
+            const T* b = l == 0 ? rhs0 : V.b;
+            T* x = l == 0 ? z : V.x;
+            const int n = lev[l]->n;
+            Csr<T> A = Amat<T>(ctx, l);
+            LevelVecs<T> C = vecs<T>(l + 1);
+            launch_spmv<T, 0>(sm, L, Pmat<T>(l), XVec<T>{C.x}, EpiProlong<T>{x}, NoFin{}, gate,
+                              "amg_prolong", w * lev[l + 1]->n + 2.0 * w * n);
+            for (int s = 0; s < post; ++s) {
+                const bool last = (l == 0 && s == post - 1);
+                if (last && with_dot) {
+                    launch_spmv<T, 1>(sm, L, A, XVec<T>{x}, EpiSmoothDot<T>{EpiSmooth<T>{b, x, V.x2, V.dinv, om}},
+                                      fin, gate, "amg_smooth", 4.0 * w * n);
+                } else {
+                    launch_spmv<T, 0>(sm, L, A, XVec<T>{x}, EpiSmooth<T>{b, x, V.x2, V.dinv, om}, NoFin{}, gate,
+                                      "amg_smooth", 4.0 * w * n);
+                }
+                launch_vec<0>(sm, L, n, BodyCopy<T>{V.x2, x}, NoFin{}, gate, "vec", 2.0 * w * n);
+            }
+        }
+    }
+
+    void apply(Ctx& ctx, const Lane& L, const double* r, double* z, const int* gate) override {
+        vcycle<double>(ctx, L, r, z, gate, false, NoFin{});
+    }
+    void prepare32(Ctx& ctx) override;
+    void apply32(Ctx& ctx, const Lane& L, const float* r, float* z, const int* gate) override {
+        prepare32(ctx);
+        vcycle<float>(ctx, L, r, z, gate, false, NoFin{});
+    }
+    bool has32() const override { return true; }
+};
+
+template <>
+LevelVecs<double> AmgPrec::vecs<double>(int l) {
+    AmgLevel& v = *lev[l];
+    return LevelVecs<double>{v.b.p, v.x.p, v.x2.p, v.r.p, v.dinv.p};
+}
+template <>
+LevelVecs<float> AmgPrec::vecs<float>(int l) {
+    AmgLevel& v = *lev[l];
+    return LevelVecs<float>{v.b32.p, v.x32.p, v.x232.p, v.r32.p, v.dinv32.p};
+}
+template <>
+Csr<double> AmgPrec::Amat<double>(Ctx&, int l) { return Aview64(l); }
+template <>
+Csr<float> AmgPrec::Amat<float>(Ctx& ctx, int l) { return Aview32(ctx, l); }
+template <>
+Csr<double> AmgPrec::Pmat<double>(int l) { return lev[l]->P.f64(); }
+template <>
+Csr<float> AmgPrec::Pmat<float>(int l) { return lev[l]->P.f32(); }
+template <>
+Csr<double> AmgPrec::Rmat<double>(int l) { return lev[l]->R.f64(); }
+template <>
+Csr<float> AmgPrec::Rmat<float>(int l) { return lev[l]->R.f32(); }
+
+void AmgPrec::prepare32(Ctx& ctx) {
+    if (f32_ready) return;
+    cudaStream_t s = ctx.lane.stream;
+    auto conv = [&](const DBuf<double>& a, DBuf<float>& b, long long n) {
+        b.ensure(n);
+        if (n) k_d2f<<<grid_for(ctx, n), 256, 0, s>>>(a.p, b.p, n);
+    };
+    for (int l = 0; l < levels(); ++l) {
+        AmgLevel& L = *lev[l];
+        if (l > 0) conv(L.A.v, L.A.v32, L.A.nnz);
+        if (L.P.nnz) { conv(L.P.v, L.P.v32, L.P.nnz); conv(L.R.v, L.R.v32, L.R.nnz); }
+        conv(L.dinv, L.dinv32, L.n);
+        L.b32.ensure(L.n); L.x32.ensure(L.n); L.x232.ensure(L.n); L.r32.ensure(L.n);
+    }
+    HAMLSS_LAUNCH_CHECK();
+    f32_ready = true;
+}
+
+// ------------------------------------------------------------------- building
+namespace {
+
+// Aggregation of one operator; returns the aggregate count (seeds).
+int aggregate_device(Ctx& ctx, const Csr<double>& A, double theta, DBuf<int>& agg) {
+    const int n = A.n;
+    cudaStream_t s = ctx.lane.stream;
+    const int g = grid_for(ctx, n);
+    agg.ensure(n);
+    if (n == 0) return 0;
+    ProfScope ps(ctx.lane, "setup", 0.0);
+    DBuf<double> rmax(n);
+    DBuf<int> in_rp(n + 1), fill(n), status(n), order(n), cnt(n + 2), nlev(1), flag(n + 1);
+    k_rowmax<<<g, 256, 0, s>>>(n, A.rp, A.ci, A.v, rmax.p);
+    HAMLSS_CUDA(cudaMemsetAsync(in_rp.p, 0, sizeof(int) * (n + 1), s));
+    k_in_count<<<g, 256, 0, s>>>(n, A.rp, A.ci, A.v, rmax.p, theta, in_rp.p);
+    HAMLSS_LAUNCH_CHECK();
+    DBuf<int> indeg(n);
+    HAMLSS_CUDA(cudaMemcpyAsync(indeg.p, in_rp.p, sizeof(int) * n, cudaMemcpyDeviceToDevice, s));
+    long long tot = exclusive_scan(ctx, in_rp.p, n + 1);
+    DBuf<int> in_src(std::max<long long>(tot, 1));
+    HAMLSS_CUDA(cudaMemcpyAsync(fill.p, in_rp.p, sizeof(int) * n, cudaMemcpyDeviceToDevice, s));
+    k_in_fill<<<g, 256, 0, s>>>(n, A.rp, A.ci, A.v, rmax.p, theta, fill.p, in_src.p);
+    HAMLSS_LAUNCH_CHECK();
+    HAMLSS_CUDA(cudaMemsetAsync(status.p, 0, sizeof(int) * n, s));
+    HAMLSS_CUDA(cudaMemsetAsync(cnt.p, 0, sizeof(int) * (n + 2), s));
+    {
+        static int per = 0;
+        if (!per) per = std::min(occupancy_blocks(k_aggregate_levels, 256), 4);
+        int blocks = std::max(1, std::min(per * ctx.sm_count, ceil_div(n, 256)));
+        const int* rp = A.rp;
+        const int* ci = A.ci;
+        const double* v = A.v;
+        const double* rm = rmax.p;
+        const int* irp = in_rp.p;
+        const int* isrc = in_src.p;
+        int* ideg = indeg.p;
+        int* st = status.p;
+        int* ord = order.p;
+        int* cn = cnt.p;
+        int* nl = nlev.p;
+        int nn = n;
+        double th = theta;
+        void* args[] = {&nn, &rp, &ci, &v, &rm, &th, &irp, &isrc, &ideg, &st, &ord, &cn, &nl};
+        HAMLSS_CUDA(cudaLaunchCooperativeKernel((const void*)k_aggregate_levels, dim3(blocks), dim3(256),
+                                                args, 0, s));
+    }
+    k_seed_flags<<<g, 256, 0, s>>>(n, status.p, flag.p);
+    HAMLSS_CUDA(cudaMemsetAsync(flag.p + n, 0, sizeof(int), s));
+    long long nseed = exclusive_scan(ctx, flag.p, n + 1);
+    k_assign<<<g, 256, 0, s>>>(n, status.p, flag.p, in_rp.p, in_src.p, agg.p);
+    HAMLSS_LAUNCH_CHECK();
+    HAMLSS_CUDA(cudaStreamSynchronize(s));
+    return (int)nseed;
+}
+
+void build_csr_counts(Ctx& ctx, DCsr& C, int rows, int cols, DBuf<int>& cnt) {
+    C.n = rows;
+    C.m = cols;
+    C.rp.ensure(rows + 1);
+    HAMLSS_CUDA(cudaMemcpyAsync(C.rp.p, cnt.p, sizeof(int) * rows, cudaMemcpyDeviceToDevice, ctx.lane.stream));
+    HAMLSS_CUDA(cudaMemsetAsync(C.rp.p + rows, 0, sizeof(int), ctx.lane.stream));
+    long long nnz = exclusive_scan(ctx, C.rp.p, rows + 1);
+    if (nnz > INT_MAX) fail(HAMLSS_ERR_NOMEM, "AMG operator exceeds 2^31 nonzeros");
+    C.nnz = (int)nnz;
+    C.ci.ensure(std::max(C.nnz, 1));
+    C.v.ensure(std::max(C.nnz, 1));
+}
+
+void smooth_prolongation(Ctx& ctx, const Csr<double>& A, const DBuf<int>& agg, int nc, double omega,
+                         DCsr& P) {
+    const int n = A.n;
+    cudaStream_t s = ctx.lane.stream;
+    const int g = grid_for(ctx, n);
+    DBuf<int> cnt(n);
+    k_smooth_p<false><<<g, 256, 0, s>>>(n, A.rp, A.ci, A.v, agg.p, omega, cnt.p, nullptr, nullptr, nullptr);
+    HAMLSS_LAUNCH_CHECK();
+    build_csr_counts(ctx, P, n, nc, cnt);
+    k_smooth_p<true><<<g, 256, 0, s>>>(n, A.rp, A.ci, A.v, agg.p, omega, nullptr, P.rp.p, P.ci.p, P.v.p);
+    HAMLSS_LAUNCH_CHECK();
+}
+
+void transpose(Ctx& ctx, const DCsr& P, DCsr& R) {
+    cudaStream_t s = ctx.lane.stream;
+    R.n = P.m;
+    R.m = P.n;
+    R.nnz = P.nnz;
+    R.rp.ensure(R.n + 1);
+    R.ci.ensure(std::max(R.nnz, 1));
+    R.v.ensure(std::max(R.nnz, 1));
+    HAMLSS_CUDA(cudaMemsetAsync(R.rp.p, 0, sizeof(int) * (R.n + 1), s));
+    k_t_count<<<grid_for(ctx, P.n), 256, 0, s>>>(P.n, P.rp.p, P.ci.p, R.rp.p);
+    HAMLSS_LAUNCH_CHECK();
+    exclusive_scan(ctx, R.rp.p, R.n + 1);
+    DBuf<int> fill(std::max(R.n, 1));
+    HAMLSS_CUDA(cudaMemcpyAsync(fill.p, R.rp.p, sizeof(int) * R.n, cudaMemcpyDeviceToDevice, s));
+    k_t_fill<<<grid_for(ctx, P.n), 256, 0, s>>>(P.n, P.rp.p, P.ci.p, P.v.p, fill.p, R.ci.p, R.v.p);
+    k_t_sort<<<grid_for(ctx, R.n), 256, 0, s>>>(R.n, R.rp.p, R.ci.p, R.v.p);
+    HAMLSS_LAUNCH_CHECK();
+}
+
+void spgemm(Ctx& ctx, const Csr<double>& A, const Csr<double>& B, DCsr& C) {
+    cudaStream_t s = ctx.lane.stream;
+    const int g = grid_for(ctx, A.n);
+    DBuf<int> heads(3LL * std::max(A.nnz, 1));
+    DBuf<int> cnt(std::max(A.n, 1));
+    k_spgemm<false><<<g, 256, 0, s>>>(A.n, A.rp, A.ci, A.v, B.rp, B.ci, B.v, cnt.p, nullptr, nullptr,
+                                      nullptr, heads.p);
+    HAMLSS_LAUNCH_CHECK();
+    build_csr_counts(ctx, C, A.n, B.m, cnt);
+    k_spgemm<true><<<g, 256, 0, s>>>(A.n, A.rp, A.ci, A.v, B.rp, B.ci, B.v, nullptr, C.rp.p, C.ci.p,
+                                     C.v.p, heads.p);
+    HAMLSS_LAUNCH_CHECK();
+}
+
+}  // namespace
+
+std::unique_ptr<Prec> make_amg(Ctx& ctx, hamlss_mat* A, const hamlss_params& p) {
+    if (A->A.n != A->A.m) fail(HAMLSS_ERR_SIZE, "AMG needs a square matrix");
+    auto M = std::make_unique<AmgPrec>();
+    M->kind = HAMLSS_PREC_AMG;
+    M->A0 = A;
+    M->n = A->A.n;
+    M->omega = p.amg_omega;
+    M->pre = p.amg_smooth_pre;
+    M->post = p.amg_smooth_post;
+    cudaStream_t s = ctx.lane.stream;
+    ProfScope ps(ctx.lane, "setup", 0.0);
+    const int max_levels = std::max(1, p.amg_levels);
+    {
+        auto L0 = std::make_unique<AmgLevel>();
+        L0->n = A->A.n;
+        L0->dinv.ensure(L0->n);
+        if (L0->n) k_inv_diag<<<grid_for(ctx, L0->n), 256, 0, s>>>(L0->n, A->A.rp.p, A->A.ci.p, A->A.v.p, L0->dinv.p);
+        HAMLSS_LAUNCH_CHECK();
+        M->lev.push_back(std::move(L0));
+    }
+    for (int lv = 0; lv < max_levels - 1; ++lv) {
+        AmgLevel& F = *M->lev.back();
+        Csr<double> Af = M->Aview64(M->levels() - 1);
+        if (Af.n <= p.amg_coarse_limit) break;
+        DBuf<int> agg;
+        int nc = aggregate_device(ctx, Af, p.amg_strong, agg);
+        if (nc >= Af.n) break;
+        smooth_prolongation(ctx, Af, agg, nc, M->omega, F.P);
+        transpose(ctx, F.P, F.R);
+        DCsr AP;
+        spgemm(ctx, Af, F.P.f64(), AP);
+        auto C = std::make_unique<AmgLevel>();
+        spgemm(ctx, F.R.f64(), AP.f64(), C->A);
+        C->n = C->A.n;
+        C->dinv.ensure(std::max(C->n, 1));
+        if (C->n) k_inv_diag<<<grid_for(ctx, C->n), 256, 0, s>>>(C->n, C->A.rp.p, C->A.ci.p, C->A.v.p, C->dinv.p);
+        HAMLSS_LAUNCH_CHECK();
+        HAMLSS_CUDA(cudaStreamSynchronize(s));
+        M->lev.push_back(std::move(C));
+    }
+    // work vectors (FP64)
+    for (int l = 0; l < M->levels(); ++l) {
+        AmgLevel& L = *M->lev[l];
+        int n = std::max(L.n, 1);
+        L.b.ensure(n); L.x.ensure(n); L.x2.ensure(n); L.r.ensure(n);
+    }
+    // coarsest level: dense factorisation (or explicit inverse for the large ones)
+    {
+        const int l = M->levels() - 1;
+        Csr<double> C = M->Aview64(l);
+        const int nc = C.n;
+        M->nc = nc;
+        if ((long long)nc * nc > (1LL << 28)) fail(HAMLSS_ERR_NOMEM, "coarsest AMG level too large for a dense solve");
+        M->Md.ensure((size_t)std::max(nc, 1) * std::max(nc, 1));
+        M->piv.ensure(std::max(nc, 1));
+        M->skip.ensure(std::max(nc, 1));
+        M->cwork.ensure(2 * std::max(nc, 1));
+        HAMLSS_CUDA(cudaMemsetAsync(M->Md.p, 0, sizeof(double) * (size_t)nc * nc, s));
+        if (nc) {
+            k_csr_to_dense<<<grid_for(ctx, nc), 256, 0, s>>>(nc, C.rp, C.ci, C.v, M->Md.p);
+            k_dense_factor<<<1, 256, 0, s>>>(nc, M->Md.p, M->piv.p, M->skip.p);
+            HAMLSS_LAUNCH_CHECK();
+        }
+        M->coarse_inverse = nc > 96;
+        if (M->coarse_inverse) {
+            M->Minv.ensure((size_t)nc * nc);
+            DBuf<double> work((size_t)nc * 2 * nc);
+            k_dense_inverse<<<nc, 32, 0, s>>>(nc, M->Md.p, M->piv.p, M->skip.p, work.p, M->Minv.p);
+            HAMLSS_LAUNCH_CHECK();
+            HAMLSS_CUDA(cudaStreamSynchronize(s));
+        }
+    }
+    HAMLSS_CUDA(cudaStreamSynchronize(s));
+    return M;
+}
+
+// ---------------------------------------------------------------- inspection
+int amg_num_levels(const Prec* P, int* levels) {
+    auto* M = dynamic_cast<const AmgPrec*>(P);
+    if (!M) return HAMLSS_ERR_INVALID;
+    *levels = M->levels();
+    return HAMLSS_OK;
+}
+
+int amg_level_matrix(const Prec* P, int level, int which, int* rows, int* cols, int* nnz, int* rp,
+                     int* ci, double* v, cudaStream_t s) {
+    auto* M = dynamic_cast<const AmgPrec*>(P);
+    if (!M || level < 0 || level >= M->levels() || which < 0 || which > 2) return HAMLSS_ERR_INVALID;
+    Csr<double> C;
+    if (which == 0) C = M->Aview64(level);
+    else {
+        if (level == M->levels() - 1) return HAMLSS_ERR_INVALID;
+        C = which == 1 ? M->lev[level]->P.f64() : M->lev[level]->R.f64();
+    }
+    if (rows) *rows = C.n;
+    if (cols) *cols = C.m;
+    if (nnz) *nnz = C.nnz;
+    if (rp) HAMLSS_CUDA(cudaMemcpyAsync(rp, C.rp, sizeof(int) * (C.n + 1), cudaMemcpyDeviceToHost, s));
+    if (ci && C.nnz) HAMLSS_CUDA(cudaMemcpyAsync(ci, C.ci, sizeof(int) * C.nnz, cudaMemcpyDeviceToHost, s));
+    if (v && C.nnz) HAMLSS_CUDA(cudaMemcpyAsync(v, C.v, sizeof(double) * C.nnz, cudaMemcpyDeviceToHost, s));
+    HAMLSS_CUDA(cudaStreamSynchronize(s));
+    return HAMLSS_OK;
+}
+
+int amg_aggregate_matrix(Ctx& ctx, hamlss_mat* A, double theta, int* agg_host, int* n_agg) {
+    DBuf<int> agg;
+    int nc = aggregate_device(ctx, A->A.f64(), theta, agg);
+    if (A->A.n) agg.download(agg_host, A->A.n, ctx.lane.stream);
+    HAMLSS_CUDA(cudaStreamSynchronize(ctx.lane.stream));
+    *n_agg = nc;
+    return HAMLSS_OK;
+}
+
+}  // namespace hamlss

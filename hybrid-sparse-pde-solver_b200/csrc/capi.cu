@@ -468,6 +468,31 @@ int hamlss_precond_release(hamlss_prec* M) {
     });
 }
 
+int hamlss_amg_aggregate(hamlss_ctx* ctx, const hamlss_mat* A, double theta, int32_t* agg,
+                         int32_t* n_agg) {
+    return guarded([&]() -> int {
+        if (!ctx || !A || !agg || !n_agg) return set_err(HAMLSS_ERR_INVALID, "null argument");
+        return amg_aggregate_matrix(ctx->c, const_cast<hamlss_mat*>(A), theta, agg, n_agg);
+    });
+}
+
+int hamlss_amg_num_levels(const hamlss_prec* M, int32_t* levels) {
+    if (!M || !levels) return set_err(HAMLSS_ERR_INVALID, "null argument");
+    int rc = amg_num_levels(M->p.get(), levels);
+    return rc ? set_err(rc, "not an AMG preconditioner") : HAMLSS_OK;
+}
+
+int hamlss_amg_level_matrix(const hamlss_prec* M, int32_t level, int32_t which, int32_t* rows,
+                            int32_t* cols, int32_t* nnz, int32_t* row_ptr, int32_t* col_idx,
+                            double* values) {
+    return guarded([&]() -> int {
+        if (!M) return set_err(HAMLSS_ERR_INVALID, "null argument");
+        int rc = amg_level_matrix(M->p.get(), level, which, rows, cols, nnz, row_ptr, col_idx, values,
+                                  M->ctx->c.lane.stream);
+        return rc ? set_err(rc, "no such AMG level / operator") : HAMLSS_OK;
+    });
+}
+
 int hamlss_ilu_factors(const hamlss_prec* M, double* lu_values) {
     return guarded([&]() -> int {
         if (!M || !lu_values) return set_err(HAMLSS_ERR_INVALID, "null argument");
@@ -484,13 +509,77 @@ int hamlss_ilu_levels(const hamlss_prec* M, int32_t which, int32_t* level, int32
 }
 
 // -------------------------------------------------------------------------- solve
+}  // extern "C"
+
+namespace {
+
+// One solve attempt with the given solver / preconditioner on device vectors.
+SolveResult solve_core(Ctx& c, int solver, hamlss_mat* Am, Prec* P, const double* db, double* dx,
+                       const hamlss_params& p, const LadderCfg* lad, int* outer) {
+    *outer = 1;
+    Workspace& ws = Am->ws;
+    if (p.precision == HAMLSS_MIXED) return mixed_solve(c, solver, Am, P, db, dx, p, ws, outer, lad);
+    if (solver == HAMLSS_SOLVER_CG)
+        return cg_solve<double>(c, Am, P, db, dx, p.tol, p.max_iter, p.check_every, ws, lad);
+    return fgmres_solve(c, Am, P, db, dx, p.tol, p.max_iter, p.restart_size, ws, lad);
+}
+
+void fill_stats(Ctx& c, hamlss_mat* Am, int solver, const Prec* P, const SolveResult& r,
+                double wall_s, int outer, double e0, double e1, const double* db, const double* dx,
+                hamlss_stats* out) {
+    hamlss_stats st;
+    std::memset(&st, 0, sizeof(st));
+    const long long n = Am->A.n, nnz = Am->A.nnz;
+    st.iterations = r.iterations;
+    st.initial_residual = r.initial_residual;
+    st.final_residual = r.final_residual;
+    st.converged = r.converged;
+    st.solve_time_s = wall_s;
+    st.solver_used = solver;
+    st.precond_used = P ? P->kind : HAMLSS_PREC_NONE;
+    st.state_used = HAMLSS_STATE_EASY;
+    st.restarts = r.restarts;
+    long long fl = 0, by = 0;
+    if (solver == HAMLSS_SOLVER_CG) cg_cost(n, nnz, r, &fl, &by);
+    else fgmres_cost(n, nnz, r, &fl, &by);
+    st.flop_count = fl;
+    st.mem_bytes = by;
+    st.energy_joules = 2.0e-10 * (double)fl + 5.0e-9 * (double)by;
+    st.energy_joules_hw = (e1 > e0) ? e1 - e0 : 0.0;
+    st.rapl_start_j = e0;
+    st.rapl_end_j = e1;
+    st.outer_iterations = outer;
+    st.status = r.status;
+    st.device_time_s = r.device_time_s;
+    st.true_residual = true_relative_residual(c, Am, db, dx, Am->ws);
+    *out = st;
+}
+
+struct IoVecs {
+    const double* b;
+    double* x;
+};
+
+IoVecs stage_in(hamlss_mat* Am, const double* b, double* x, int where, cudaStream_t s) {
+    if (where != HAMLSS_HOST) return IoVecs{b, x};
+    Workspace& ws = Am->ws;
+    const int n = Am->A.n;
+    ws.d[6].upload(b, n, s);
+    ws.d[7].upload(x, n, s);
+    return IoVecs{ws.d[6].p, ws.d[7].p};
+}
+
+}  // namespace
+
+extern "C" {
+
 int hamlss_solve(hamlss_ctx* ctx, int solver, const hamlss_mat* A, const hamlss_prec* M,
                  const double* b, double* x, int where, const hamlss_params* params,
                  hamlss_stats* stats) {
     return guarded([&]() -> int {
         if (!ctx || !A || !b || !x) return set_err(HAMLSS_ERR_INVALID, "null argument");
         if (A->A.n != A->A.m) return set_err(HAMLSS_ERR_SIZE, "solve needs a square matrix");
-        if (M && M->A != A && M->p->n != A->A.n)
+        if (M && M->p->n != A->A.n)
             return set_err(HAMLSS_ERR_SIZE, "preconditioner size differs from the matrix");
         hamlss_params p;
         if (params) p = *params; else hamlss_params_default(&p);
@@ -502,60 +591,107 @@ int hamlss_solve(hamlss_ctx* ctx, int solver, const hamlss_mat* A, const hamlss_
         cudaStream_t s = c.lane.stream;
         auto* Am = const_cast<hamlss_mat*>(A);
         Prec* P = M ? M->p.get() : nullptr;
-        const int n = A->A.n;
-        Workspace& ws = Am->ws;
-        const double* db = b;
-        double* dx = x;
-        if (where == HAMLSS_HOST) {
-            ws.d[6].upload(b, n, s);
-            ws.d[7].upload(x, n, s);
-            db = ws.d[6].p;
-            dx = ws.d[7].p;
-        }
+        IoVecs io = stage_in(Am, b, x, where, s);
         double e0 = p.record_hw_energy ? nvml_energy_j(c.device) : 0.0;
         double t0 = now_s();
-        SolveResult r;
         int outer = 1;
-        if (p.precision == HAMLSS_MIXED) {
-            r = mixed_solve(c, solver, Am, P, db, dx, p, ws, &outer);
-        } else if (solver == HAMLSS_SOLVER_CG) {
-            r = cg_solve<double>(c, Am, P, db, dx, p.tol, p.max_iter, p.check_every, ws);
-        } else {
-            r = fgmres_solve(c, Am, P, db, dx, p.tol, p.max_iter, p.restart_size, ws);
-        }
+        SolveResult r = solve_core(c, solver, Am, P, io.b, io.x, p, nullptr, &outer);
         double t1 = now_s();
         double e1 = p.record_hw_energy ? nvml_energy_j(c.device) : 0.0;
-        if (stats) {
-            hamlss_stats st;
-            std::memset(&st, 0, sizeof(st));
-            st.iterations = r.iterations;
-            st.initial_residual = r.initial_residual;
-            st.final_residual = r.final_residual;
-            st.converged = r.converged;
-            st.solve_time_s = t1 - t0;
-            st.solver_used = solver;
-            st.precond_used = P ? P->kind : HAMLSS_PREC_NONE;
-            st.state_used = HAMLSS_STATE_EASY;
-            st.restarts = r.restarts;
-            long long fl = 0, by = 0;
-            if (solver == HAMLSS_SOLVER_CG) cg_cost(n, A->A.nnz, r, &fl, &by);
-            else fgmres_cost(n, A->A.nnz, r, &fl, &by);
-            st.flop_count = fl;
-            st.mem_bytes = by;
-            st.energy_joules = 2.0e-10 * (double)fl + 5.0e-9 * (double)by;
-            st.energy_joules_hw = (e1 > e0) ? e1 - e0 : 0.0;
-            st.rapl_start_j = e0;
-            st.rapl_end_j = e1;
-            st.outer_iterations = outer;
-            st.status = r.status;
-            st.device_time_s = r.device_time_s;
-            st.true_residual = true_relative_residual(c, Am, db, dx, ws);
-            *stats = st;
-        }
-        if (where == HAMLSS_HOST) ws.d[7].download(x, n, s);
+        if (stats) fill_stats(c, Am, solver, P, r, t1 - t0, outer, e0, e1, io.b, io.x, stats);
+        if (where == HAMLSS_HOST) Am->ws.d[7].download(x, A->A.n, s);
         HAMLSS_CUDA(cudaStreamSynchronize(s));
         if (r.status != HAMLSS_OK)
             return set_err(r.status, "non-finite values met during the solve");
+        return HAMLSS_OK;
+    });
+}
+
+int hamlss_extract_features(hamlss_ctx* ctx, const hamlss_mat* A, double features[24],
+                            int32_t* initial_state) {
+    return guarded([&]() -> int {
+        if (!ctx || !A || !features) return set_err(HAMLSS_ERR_INVALID, "null argument");
+        int st = 0;
+        int rc = extract_features(ctx->c, const_cast<hamlss_mat*>(A), features, &st);
+        if (initial_state) *initial_state = st;
+        return rc;
+    });
+}
+
+// AdaptiveSelector::solve (adaptive_selector.cpp:298-394)
+int hamlss_solve_adaptive(hamlss_ctx* ctx, const hamlss_mat* A, const double* b, double* x,
+                          int where, const hamlss_params* params, hamlss_stats* stats,
+                          hamlss_escalation* log, int32_t log_cap, int32_t* n_log,
+                          int32_t* initial_state) {
+    return guarded([&]() -> int {
+        if (!ctx || !A || !b || !x) return set_err(HAMLSS_ERR_INVALID, "null argument");
+        if (A->A.n != A->A.m) return set_err(HAMLSS_ERR_SIZE, "solve needs a square matrix");
+        hamlss_params p;
+        if (params) p = *params; else hamlss_params_default(&p);
+        Ctx& c = ctx->c;
+        HAMLSS_CUDA(cudaSetDevice(c.device));
+        cudaStream_t s = c.lane.stream;
+        auto* Am = const_cast<hamlss_mat*>(A);
+        double feat[24];
+        int state = 0;
+        extract_features(c, Am, feat, &state);
+        if (initial_state) *initial_state = state;
+        IoVecs io = stage_in(Am, b, x, where, s);
+        int nlog = 0;
+        bool solved = false;
+        hamlss_stats last;
+        std::memset(&last, 0, sizeof(last));
+        SolveResult r;
+        for (;;) {
+            const int kind = state == HAMLSS_STATE_EASY ? HAMLSS_PREC_JACOBI
+                           : state == HAMLSS_STATE_MODERATE ? HAMLSS_PREC_ILU : HAMLSS_PREC_AMG;
+            const int solver = state == HAMLSS_STATE_EASY ? HAMLSS_SOLVER_CG : HAMLSS_SOLVER_FGMRES;
+            double t0 = now_s();
+            std::unique_ptr<Prec> P;
+            if (kind == HAMLSS_PREC_JACOBI) P = make_jacobi(c, Am, p.jacobi_omega);
+            else if (kind == HAMLSS_PREC_ILU) {
+                if (p.drop_tol > 0.0 || p.fill_per_row > 0)
+                    return set_err(HAMLSS_ERR_INVALID,
+                                   "the MODERATE state asks for ILUT (drop_tol > 0), which the "
+                                   "engine does not provide; pass drop_tol = 0 for ILU(0)");
+                P = make_ilu0(c, Am);
+            } else P = make_amg(c, Am, p);
+            HAMLSS_CUDA(cudaStreamSynchronize(s));
+            double setup = now_s() - t0;
+            LadderCfg lad;
+            lad.on = p.ladder_mode == 1 && state != HAMLSS_STATE_HARD;
+            lad.state = state;
+            lad.window = p.stall_window;
+            lad.threshold = p.stall_threshold;
+            lad.max_iter = p.max_iter;
+            double e0 = p.record_hw_energy ? nvml_energy_j(c.device) : 0.0;
+            double t1 = now_s();
+            int outer = 1;
+            r = solve_core(c, solver, Am, P.get(), io.b, io.x, p, &lad, &outer);
+            double t2 = now_s();
+            double e1 = p.record_hw_energy ? nvml_energy_j(c.device) : 0.0;
+            if (r.status != HAMLSS_OK) return set_err(r.status, "non-finite values met during the solve");
+            fill_stats(c, Am, solver, P.get(), r, t2 - t1, outer, e0, e1, io.b, io.x, &last);
+            last.setup_time_s = setup + setup;     // stats.setup_time_s counted twice (:350-351)
+            last.state_used = state;
+            solved = r.converged != 0;
+            if (solved || state == HAMLSS_STATE_HARD) break;
+            const int next = state + 1;
+            if (log && nlog < log_cap) {
+                log[nlog].at_iteration = r.iterations;
+                log[nlog].from_state = state;
+                log[nlog].to_state = next;
+                log[nlog].residual_at_escalation = r.final_residual;
+                log[nlog].reason = r.escalate;
+            }
+            ++nlog;
+            state = next;
+        }
+        last.state_used = state;
+        if (stats) *stats = last;
+        if (n_log) *n_log = nlog;
+        if (where == HAMLSS_HOST) Am->ws.d[7].download(x, A->A.n, s);
+        HAMLSS_CUDA(cudaStreamSynchronize(s));
         return HAMLSS_OK;
     });
 }

@@ -25,6 +25,7 @@ constexpr double kEps = 2.220446049250313e-16;
 struct CgState {
     double bnorm, r0, rel, tol, rho, rho_old, alpha, beta, pq;
     int iter, max_iter, halt, status, restart_kind, early;
+    LadderDev lad;
 };
 
 __device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
@@ -189,6 +190,7 @@ struct FinUpd {
         s->rel = rel;
         if (rel < s->tol) { s->iter += 1; s->status = ST_CONV; s->halt = 1; return; }
         if (!isfinite(rel)) { s->iter += 1; s->status = ST_NONFINITE; s->halt = 1; return; }
+        if (ladder_check(&s->lad, s->iter, rel)) { s->iter += 1; s->status = ST_ESCALATE; s->halt = 1; return; }
         if constexpr (JAC) rho_step(s, t[1]);
     }
 };
@@ -257,7 +259,7 @@ void precond_apply<float>(Ctx& ctx, Prec* M, const float* r, float* z, const int
 
 template <typename T, bool JAC>
 SolveResult cg_impl(Ctx& ctx, hamlss_mat* A, Prec* M, const T* b, T* x, double tol,
-                    int max_iter, int check_every, Workspace& ws) {
+                    int max_iter, int check_every, Workspace& ws, const LadderCfg* lad) {
     const int n = A->A.n;
     const Lane& L = ctx.lane;
     const int sm = ctx.sm_count;
@@ -276,6 +278,7 @@ SolveResult cg_impl(Ctx& ctx, hamlss_mat* A, Prec* M, const T* b, T* x, double t
     CgState h0{};
     h0.tol = tol;
     h0.max_iter = max_iter;
+    h0.lad = ladder_init(lad);
     HAMLSS_CUDA(cudaMemcpyAsync(s, &h0, sizeof(CgState), cudaMemcpyHostToDevice, st));
     launch_vec<0>(sm, L, n, BodyFill<T>{p[0], T(0)});
     launch_vec<0>(sm, L, n, BodyFill<T>{p[1], T(0)});
@@ -338,6 +341,7 @@ SolveResult cg_impl(Ctx& ctx, hamlss_mat* A, Prec* M, const T* b, T* x, double t
     res.final_residual = h.rel;
     res.converged = h.status == ST_CONV;
     if (h.status == ST_NONFINITE) res.status = HAMLSS_ERR_NONFINITE;
+    if (h.status == ST_ESCALATE) res.escalate = h.lad.reason;
     return res;
 }
 
@@ -345,15 +349,15 @@ SolveResult cg_impl(Ctx& ctx, hamlss_mat* A, Prec* M, const T* b, T* x, double t
 
 template <typename T>
 SolveResult cg_solve(Ctx& ctx, hamlss_mat* A, Prec* M, const T* b, T* x, double tol,
-                     int max_iter, int check_every, Workspace& ws) {
+                     int max_iter, int check_every, Workspace& ws, const LadderCfg* lad) {
     if (M && M->kind == HAMLSS_PREC_JACOBI)
-        return cg_impl<T, true>(ctx, A, M, b, x, tol, max_iter, check_every, ws);
-    return cg_impl<T, false>(ctx, A, M, b, x, tol, max_iter, check_every, ws);
+        return cg_impl<T, true>(ctx, A, M, b, x, tol, max_iter, check_every, ws, lad);
+    return cg_impl<T, false>(ctx, A, M, b, x, tol, max_iter, check_every, ws, lad);
 }
 
 template SolveResult cg_solve<double>(Ctx&, hamlss_mat*, Prec*, const double*, double*, double,
-                                      int, int, Workspace&);
+                                      int, int, Workspace&, const LadderCfg*);
 template SolveResult cg_solve<float>(Ctx&, hamlss_mat*, Prec*, const float*, float*, double, int,
-                                     int, Workspace&);
+                                     int, Workspace&, const LadderCfg*);
 
 }  // namespace hamlss

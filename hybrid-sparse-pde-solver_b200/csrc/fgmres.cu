@@ -27,7 +27,8 @@ constexpr double kEps = 2.220446049250313e-16;
 
 struct GmState {
     double bnorm, tol_abs, beta, res, inv_beta, hn_inv, hn;
-    int jcount, halt, status, m;
+    int jcount, halt, status, m, iter_base;
+    LadderDev lad;
 };
 
 // Device-side small arrays, laid out in ws.small: H (m+1) x m row-major, cs, sn, g, y,
@@ -192,7 +193,8 @@ struct FinNorm {
         s->res = res;
         s->jcount = j + 1;
         if (!isfinite(res)) { s->status = ST_NONFINITE; s->halt = 1; return; }
-        if (res < s->tol_abs) s->halt = 1;
+        if (res < s->tol_abs) { s->halt = 1; return; }
+        if (ladder_check(&s->lad, s->iter_base + j, res / s->bnorm)) { s->status = ST_ESCALATE; s->halt = 1; }
     }
 };
 
@@ -263,7 +265,8 @@ void launch_mdot(Ctx& ctx, int mode, int n, int nv, const double* V, long long l
 }  // namespace
 
 SolveResult fgmres_solve(Ctx& ctx, hamlss_mat* A, Prec* M, const double* b, double* x,
-                         double tol, int max_iter, int restart, Workspace& ws) {
+                         double tol, int max_iter, int restart, Workspace& ws,
+                         const LadderCfg* lad) {
     const int n = A->A.n;
     const int m = std::max(1, std::min(restart, n));
     if (m > 63) fail(HAMLSS_ERR_INVALID, "FGMRES restart length above 63 is not supported");
@@ -292,6 +295,7 @@ SolveResult fgmres_solve(Ctx& ctx, hamlss_mat* A, Prec* M, const double* b, doub
     GmState* s = reinterpret_cast<GmState*>(ws.state.p);
     GmState h0{};
     h0.m = m;
+    h0.lad = ladder_init(lad);
     HAMLSS_CUDA(cudaMemcpyAsync(s, &h0, sizeof(h0), cudaMemcpyHostToDevice, st));
     HAMLSS_CUDA(cudaEventRecord(ctx.ev0, st));
 
@@ -315,6 +319,7 @@ SolveResult fgmres_solve(Ctx& ctx, hamlss_mat* A, Prec* M, const double* b, doub
     while (total < max_iter) {
         const int cm = std::min(m, max_iter - total);
         HAMLSS_CUDA(cudaMemsetAsync(&s->halt, 0, sizeof(int), st));
+        HAMLSS_CUDA(cudaMemcpyAsync(&s->iter_base, &total, sizeof(int), cudaMemcpyHostToDevice, st));
         launch_spmv<double, 1>(sm, L, A->A.f64(), XVec<double>{x}, EpiRes{b, r}, FinCycleStart{s, a},
                                nullptr, "gmres_residual", 24.0 * n);
         launch_vec<0>(sm, L, n, BodyScaleV0{r, V, s, 0.0}, NoFin{}, &s->halt, "vec", 16.0 * n);
@@ -344,6 +349,11 @@ SolveResult fgmres_solve(Ctx& ctx, hamlss_mat* A, Prec* M, const double* b, doub
         if (h.status == ST_NONFINITE) { res.status = HAMLSS_ERR_NONFINITE; break; }
         total += h.jcount;
         ++cycles;
+        if (h.status == ST_ESCALATE) {       // device ladder test fired inside the cycle
+            res.escalate = h.lad.reason;
+            res.final_residual = h.res / h.bnorm;
+            break;
+        }
         double rel = h.res / h.bnorm;
         if (rel < tol || h.jcount == 0) {          // fgmres_solver.cpp:221-225
             res.converged = rel < tol;

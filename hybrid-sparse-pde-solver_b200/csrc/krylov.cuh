@@ -1,12 +1,14 @@
 // krylov.cuh -- device PCG and FGMRES(m) drivers.
 #pragma once
 
+#include "ladder.cuh"
 #include "precond.cuh"
 
 namespace hamlss {
 
 // Solve status codes kept in device state (polled by the host).
-enum : int { ST_RUN = 0, ST_CONV = 1, ST_MAXIT = 2, ST_RESTART = 3, ST_NONFINITE = 4 };
+enum : int { ST_RUN = 0, ST_CONV = 1, ST_MAXIT = 2, ST_RESTART = 3, ST_NONFINITE = 4,
+             ST_ESCALATE = 5 };
 
 struct SolveResult {
     int iterations = 0;
@@ -16,6 +18,7 @@ struct SolveResult {
     double initial_residual = 0.0;
     double final_residual = 0.0;
     double device_time_s = 0.0;
+    int escalate = 0;         // ESC_* when the device-side ladder test stopped the solve
 };
 
 // CGSolver::solve (cg_solver.cpp:37-191) on device vectors.  T = double runs the FP64
@@ -23,15 +26,17 @@ struct SolveResult {
 // entries of type T on the device.  `jac` (may be null) selects the fused Jacobi kernels.
 template <typename T>
 SolveResult cg_solve(Ctx& ctx, hamlss_mat* A, Prec* M, const T* b, T* x, double tol,
-                     int max_iter, int check_every, Workspace& ws);
+                     int max_iter, int check_every, Workspace& ws, const LadderCfg* lad = nullptr);
 
 // FGMRESSolver::solve (fgmres_solver.cpp:165-241) with CGS2 Arnoldi; FP64.
 SolveResult fgmres_solve(Ctx& ctx, hamlss_mat* A, Prec* M, const double* b, double* x,
-                         double tol, int max_iter, int restart, Workspace& ws);
+                         double tol, int max_iter, int restart, Workspace& ws,
+                         const LadderCfg* lad = nullptr);
 
 // Mixed precision: FP64 iterative refinement around an FP32 inner PCG / FGMRES.
 SolveResult mixed_solve(Ctx& ctx, int solver, hamlss_mat* A, Prec* M, const double* b,
-                        double* x, const hamlss_params& p, Workspace& ws, int* outer_iters);
+                        double* x, const hamlss_params& p, Workspace& ws, int* outer_iters,
+                        const LadderCfg* lad = nullptr);
 
 // ||b - A x|| / ||b|| in FP64 on the device (SolverBase::relative_residual,
 // solver_base.cpp:9-17).
@@ -39,5 +44,8 @@ double true_relative_residual(Ctx& ctx, hamlss_mat* A, const double* b, const do
                               Workspace& ws);
 
 inline Workspace& workspace_of(hamlss_mat* A) { return A->ws; }
+
+// AdaptiveSelector::extract_features + select_initial_state on the device.
+int extract_features(Ctx& ctx, hamlss_mat* A, double feat[24], int* initial_state);
 
 }  // namespace hamlss

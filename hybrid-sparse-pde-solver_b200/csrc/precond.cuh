@@ -37,6 +37,10 @@ std::unique_ptr<Prec> make_ilu0(Ctx& ctx, hamlss_mat* A);
 std::unique_ptr<Prec> make_amg(Ctx& ctx, hamlss_mat* A, const hamlss_params& p);
 
 int ilu_copy_factors(const Prec* M, double* out, cudaStream_t s);
+int amg_num_levels(const Prec* P, int* levels);
+int amg_level_matrix(const Prec* P, int level, int which, int* rows, int* cols, int* nnz, int* rp,
+                     int* ci, double* v, cudaStream_t s);
+int amg_aggregate_matrix(Ctx& ctx, hamlss_mat* A, double theta, int* agg_host, int* n_agg);
 int ilu_copy_levels(const Prec* M, int which, int* level, int* nlev, cudaStream_t s);
 
 // Extract a_ii into A->diag (once per value version).

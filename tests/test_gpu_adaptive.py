@@ -1,0 +1,120 @@
+"""Adaptive selector on the device against the reference (-m gpu).
+
+Features: same initial state; row statistics equal to 1e-12 relative, Lanczos-derived
+entries (condition, lambda bounds, energy proxies) to 1e-6 relative (dot products are
+summed in a different order).  Ladder (ladder_mode 0, the reference's rule): same
+initial state, same escalation sequence and final state, iterations within +-1.
+"""
+import numpy as np
+import pytest
+
+from gpu_util import need_gpu
+import hsps_b200 as H
+from hsps_b200 import problems as P
+from hsps_b200._abi import default_params
+
+pytestmark = pytest.mark.gpu
+
+LANCZOS = {6, 13, 14, 22, 23}   # cond, lambda_max, lambda_min, energy proxies
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _gpu():
+    need_gpu()
+
+
+def cases():
+    yield "poisson30", P.poisson_2d(30)
+    yield "varkappa33", P.varkappa_poisson_2d(33, 1.0, 9)
+    yield "varkappa_s15", P.varkappa_poisson_2d(28, 1.5, 2)
+    for pe in (1.0, 30.0, 300.0):
+        bx, by = P.convdiff_wind(26, pe)
+        yield f"convdiff26_pe{int(pe)}", P.convection_diffusion_2d(26, 1.0, bx, by)
+    yield "helmholtz20", P.helmholtz_2d(20, 0.3)
+
+
+CASES = list(cases())
+IDS = [c[0] for c in CASES]
+
+
+def dev(A):
+    n = len(A[0]) - 1
+    return H.SparseMatrix(n, n, *A)
+
+
+@pytest.mark.parametrize("name,A", CASES, ids=IDS)
+def test_features_match_reference(ref, name, A):
+    f_ref, s_ref = ref.features(*A)
+    f_dev, s_dev = H.AdaptiveSelector().extract_features(dev(A))
+    assert s_dev == s_ref
+    for k in range(24):
+        tol = 1e-6 if k in LANCZOS else 1e-12
+        assert f_dev[k] == pytest.approx(f_ref[k], rel=tol, abs=1e-300), (k, f_dev[k], f_ref[k])
+
+
+@pytest.mark.parametrize("name,A", CASES, ids=IDS)
+def test_ladder_matches_reference(ref, name, A):
+    n = len(A[0]) - 1
+    b = P.rhs(n, 23)
+    p = default_params(tol=1e-8, max_iter=120, restart_size=30, drop_tol=0.0)
+    rc, xo, so, log_ref = ref.solve_adaptive(*A, b, params=p)
+    sel = H.AdaptiveSelector(p)
+    x = np.zeros(n)
+    st = H.SolverStats()
+    ok = sel.solve(dev(A), b, x, st)
+    assert ok == bool(so.converged)
+    assert st.state_used == so.state_used
+    assert [(e.from_state, e.to_state) for e in sel.escalation_log()] == \
+           [(e.from_state, e.to_state) for e in log_ref]
+    assert abs(st.iterations - so.iterations) <= 1
+    if ok:
+        assert st.true_residual < 10 * p.tol
+
+
+def test_ladder_device_stall_escalates_early():
+    # Pe = 300 conv-diff: CG+Jacobi stalls; ladder_mode 1 escalates before max_iter
+    bx, by = P.convdiff_wind(40, 300.0)
+    A = P.convection_diffusion_2d(40, 1.0, bx, by)
+    n = 1600
+    b = P.rhs(n, 4)
+    M = dev(A)
+    p = default_params(tol=1e-8, max_iter=400, restart_size=30, drop_tol=0.0, ladder_mode=1)
+    sel = H.AdaptiveSelector(p)
+    f, s0 = sel.extract_features(M)
+    x = np.zeros(n)
+    st = H.SolverStats()
+    sel.solve(M, b, x, st)
+    log = sel.escalation_log()
+    if log:
+        assert all(e.reason in (1, 2, 3) for e in log)
+        assert log[0].at_iteration < p.max_iter
+
+
+def test_ladder_easy_poisson_no_escalation():
+    # test_adaptive.cpp:111-125 in the reference
+    p = default_params(tol=1e-9, max_iter=3000, restart_size=40, drop_tol=0.0)
+    A = H.SparseMatrix.poisson_2d(16)
+    sel = H.AdaptiveSelector(p)
+    x = np.zeros(256)
+    st = H.SolverStats()
+    assert sel.solve(A, np.ones(256), x, st)
+    assert sel.escalation_log() == [] and st.state_used == H.STATE_EASY
+
+
+def test_ladder_warm_start_reuses_x():
+    # test_adaptive.cpp:182-201: a converged x as the start needs no iterations
+    p = default_params(tol=1e-8, max_iter=2000, drop_tol=0.0)
+    A = H.SparseMatrix.poisson_2d(12)
+    b = np.ones(144)
+    sel = H.AdaptiveSelector(p)
+    x = np.zeros(144)
+    sel.solve(A, b, x)
+    st = H.SolverStats()
+    assert sel.solve(A, b, x, st) and st.iterations == 0
+
+
+def test_ladder_ilut_request_refused():
+    A = H.SparseMatrix.convection_diffusion_2d(16, 1.0, *P.convdiff_wind(16, 300.0))
+    sel = H.AdaptiveSelector(default_params(max_iter=5))   # default drop_tol = 1e-4
+    with pytest.raises(H.HamlssError):
+        sel.solve(A, np.ones(256), np.zeros(256))

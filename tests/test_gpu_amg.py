@@ -1,0 +1,179 @@
+"""SA-AMG on the device against the reference and the oracle (-m gpu).
+
+Bit-exact: aggregation (every level), P, R and A_c (structure and values), and the
+V-cycle output, against the reference where it can set up (<= 240^2 grids) and against
+the oracle beyond.  Solves: iteration count within +-1 of the reference (FP64), and the
+mixed-precision path reaches an FP64 true residual below tol.
+"""
+import numpy as np
+import pytest
+
+from gpu_util import need_gpu
+import hsps_b200 as H
+from hsps_b200 import problems as P
+from hsps_b200._abi import default_params
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _gpu():
+    need_gpu()
+
+
+def small_cases():
+    yield "poisson32", P.poisson_2d(32)
+    yield "varkappa40", P.varkappa_poisson_2d(40, 1.0, 8)
+    bx, by = P.convdiff_wind(30, 10.0)
+    yield "convdiff30_pe10", P.convection_diffusion_2d(30, 1.0, bx, by)
+    yield "helmholtz25", P.helmholtz_2d(25, 5.0)
+
+
+SMALL = list(small_cases())
+SIDS = [c[0] for c in SMALL]
+
+
+def dev(A):
+    n = len(A[0]) - 1
+    return H.SparseMatrix(n, n, *A)
+
+
+@pytest.mark.parametrize("name,A", SMALL, ids=SIDS)
+def test_aggregation_bitwise_vs_reference(ref, name, A):
+    M = dev(A)
+    for theta in (0.25, 0.1, 0.5):
+        m_ref, agg_ref = ref.aggregate(*A, theta)
+        m_dev, agg_dev = H.amg_aggregate(M, theta)
+        assert m_dev == m_ref
+        assert np.array_equal(agg_dev, agg_ref)
+
+
+@pytest.mark.parametrize("side,sigma", [(256, 1.0), (400, 0.5)])
+def test_aggregation_bitwise_large_vs_oracle(orc, side, sigma):
+    A = P.varkappa_poisson_2d(side, sigma, 3)
+    m_o, agg_o = orc.aggregate(*A, 0.25)
+    m_d, agg_d = H.amg_aggregate(dev(A), 0.25)
+    assert m_d == m_o and np.array_equal(agg_d, agg_o)
+    A = P.poisson_2d(side)
+    assert np.array_equal(H.amg_aggregate(dev(A), 0.25)[1], orc.aggregate(*A, 0.25)[1])
+
+
+def hierarchy(M):
+    out = []
+    for l in range(M.levels()):
+        d = {"A": M.level_matrix(l, 0)}
+        if l < M.levels() - 1:
+            d["P"] = M.level_matrix(l, 1)
+            d["R"] = M.level_matrix(l, 2)
+        out.append(d)
+    return out
+
+
+def assert_same_hierarchy(h_dev, h_ref):
+    assert len(h_dev) == len(h_ref)
+    for l, (a, b) in enumerate(zip(h_dev, h_ref)):
+        for k in ("A", "P", "R"):
+            if k not in b:
+                continue
+            assert a[k][:2] == b[k][:2], (l, k)
+            for x, y in zip(a[k][2:], b[k][2:]):
+                assert np.array_equal(x, y), (l, k)
+
+
+@pytest.mark.parametrize("name,A", SMALL, ids=SIDS)
+def test_hierarchy_bitwise_vs_reference(ref, name, A):
+    M = H.AMGPreconditioner()
+    M.setup(dev(A))
+    assert_same_hierarchy(hierarchy(M), ref.amg_hierarchy(*A))
+
+
+def test_hierarchy_bitwise_large_vs_oracle(orc):
+    # 384^2 is beyond what the reference can set up (dense n_f x n_c buffer)
+    A = P.varkappa_poisson_2d(384, 1.0, 2)
+    M = H.AMGPreconditioner()
+    M.setup(dev(A))
+    assert_same_hierarchy(hierarchy(M), orc.amg_hierarchy(*A))
+
+
+@pytest.mark.parametrize("name,A", SMALL, ids=SIDS)
+def test_vcycle_bitwise_vs_reference(ref, name, A):
+    n = len(A[0]) - 1
+    M = H.AMGPreconditioner()
+    M.setup(dev(A))
+    r = P.rhs(n, 17, -1.0, 1.0)
+    rc, z = ref.precond_apply(3, *A, r)
+    assert np.array_equal(M.apply(r), z)
+
+
+@pytest.mark.parametrize("name,A", SMALL, ids=SIDS)
+@pytest.mark.parametrize("solver", [H.SOLVER_CG, H.SOLVER_FGMRES])
+def test_amg_solve_parity(orc, ref, name, A, solver):
+    n = len(A[0]) - 1
+    b = P.rhs(n, 19)
+    p = default_params(tol=1e-8, max_iter=500, restart_size=30)
+    rc, xo, so = ref.solve(solver, 3, *A, b, params=p)
+    M = dev(A)
+    s, _ = H.SolverFactory.make(solver, H.PREC_AMG, M, p)
+    x = np.zeros(n)
+    st = H.SolverStats()
+    ok = s.solve(M, b, x, st)
+    assert ok == bool(so.converged)
+    assert abs(st.iterations - so.iterations) <= 1, (st.iterations, so.iterations)
+    if ok:
+        r = b - orc.spmv(*A, x)
+        assert np.linalg.norm(r) / np.linalg.norm(b) < 10 * p.tol
+
+
+@pytest.mark.parametrize("side", [64, 300])
+def test_mixed_precision_amg_pcg(orc, side):
+    A = P.varkappa_poisson_2d(side, 1.0, 5)
+    n = side * side
+    b = P.rhs(n, 5, -1.0, 1.0)
+    M = dev(A)
+    for omega, coarse in ((0.67, 50), (2.0 / 3.0, 512)):
+        p64 = default_params(tol=1e-10, max_iter=1000, amg_omega=omega, amg_coarse_limit=coarse,
+                             amg_levels=25)
+        pm = default_params(tol=1e-10, max_iter=1000, amg_omega=omega, amg_coarse_limit=coarse,
+                            amg_levels=25, precision=H._abi.MIXED)
+        s64, _ = H.SolverFactory.make("CG", "AMG", M, p64)
+        x64 = np.zeros(n)
+        st64 = H.SolverStats()
+        assert s64.solve(M, b, x64, st64)
+        sm, _ = H.SolverFactory.make("CG", "AMG", M, pm)
+        xm = np.zeros(n)
+        stm = H.SolverStats()
+        assert sm.solve(M, b, xm, stm)
+        r = b - orc.spmv(*A, xm)
+        assert np.linalg.norm(r) / np.linalg.norm(b) < 1e-10
+        assert stm.true_residual < 1e-10 and stm.outer_iterations >= 2
+        # error against the FP64 solve, relative to the solution size
+        assert np.max(np.abs(xm - x64)) <= 1e-6 * np.max(np.abs(x64))
+
+
+def test_mixed_precision_fgmres_ilu(orc):
+    bx, by = P.convdiff_wind(64, 10.0)
+    A = P.convection_diffusion_2d(64, 1.0, bx, by)
+    n = 64 * 64
+    b = P.rhs(n, 2)
+    M = dev(A)
+    p = default_params(tol=1e-10, max_iter=2000, restart_size=30, drop_tol=0.0, precision=H._abi.MIXED)
+    s, _ = H.SolverFactory.make("FGMRES", "ILU", M, p)
+    x = np.zeros(n)
+    st = H.SolverStats()
+    assert s.solve(M, b, x, st)
+    r = b - orc.spmv(*A, x)
+    assert np.linalg.norm(r) / np.linalg.norm(b) < 1e-9
+
+
+def test_amg_single_level_and_tiny():
+    # rows <= coarse_limit: the hierarchy is one level and the V-cycle is the dense solve
+    A = H.SparseMatrix.poisson_2d(5)
+    M = H.AMGPreconditioner()
+    M.setup(A)
+    assert M.levels() == 1
+    b = np.arange(25, dtype=float)
+    z = M.apply(b)
+    d = np.zeros((25, 25))
+    rp, ci, v = A.row_ptr(), A.col_idx(), A.values()
+    d[np.repeat(np.arange(25), np.diff(rp)), ci] = v
+    assert np.allclose(d @ z, b, atol=1e-12)
