@@ -27,8 +27,10 @@
 // restriction and the prolongation+correction are single fused SpMV passes.
 #include <cooperative_groups.h>
 
+#include <chrono>
 #include <climits>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 
 #include "krylov.cuh"
@@ -856,19 +858,38 @@ std::unique_ptr<Prec> make_amg(Ctx& ctx, hamlss_mat* A, const hamlss_params& p) 
         HAMLSS_LAUNCH_CHECK();
         M->lev.push_back(std::move(L0));
     }
+    // verbose >= 2: per-phase wall times of every level on stderr (SolverParams::verbose)
+    const bool trace = p.verbose >= 2;
+    auto tick = std::chrono::steady_clock::now();
+    auto phase = [&](int lv, const char* what) {
+        if (!trace) return;
+        HAMLSS_CUDA(cudaStreamSynchronize(s));
+        auto now = std::chrono::steady_clock::now();
+        std::fprintf(stderr, "[hamlss amg] level %d %-10s %9.3f ms\n", lv, what,
+                     std::chrono::duration<double, std::milli>(now - tick).count());
+        tick = now;
+    };
     for (int lv = 0; lv < max_levels - 1; ++lv) {
         AmgLevel& F = *M->lev.back();
         Csr<double> Af = M->Aview64(M->levels() - 1);
         if (Af.n <= p.amg_coarse_limit) break;
         DBuf<int> agg;
         int nc = aggregate_device(ctx, Af, p.amg_strong, agg);
+        phase(lv, "aggregate");
         if (nc >= Af.n) break;
         smooth_prolongation(ctx, Af, agg, nc, M->omega, F.P);
+        phase(lv, "prolong");
         transpose(ctx, F.P, F.R);
+        phase(lv, "transpose");
         DCsr AP;
         spgemm(ctx, Af, F.P.f64(), AP);
+        phase(lv, "A*P");
         auto C = std::make_unique<AmgLevel>();
         spgemm(ctx, F.R.f64(), AP.f64(), C->A);
+        phase(lv, "R*(AP)");
+        if (trace)
+            std::fprintf(stderr, "[hamlss amg] level %d n=%d nnz=%d -> n_c=%d nnz_c=%d nnz_P=%d\n", lv,
+                         Af.n, Af.nnz, C->A.n, C->A.nnz, F.P.nnz);
         C->n = C->A.n;
         C->dinv.ensure(std::max(C->n, 1));
         if (C->n) k_inv_diag<<<grid_for(ctx, C->n), 256, 0, s>>>(C->n, C->A.rp.p, C->A.ci.p, C->A.v.p, C->dinv.p);
@@ -899,6 +920,7 @@ std::unique_ptr<Prec> make_amg(Ctx& ctx, hamlss_mat* A, const hamlss_params& p) 
             k_dense_factor<<<1, 256, 0, s>>>(nc, M->Md.p, M->piv.p, M->skip.p);
             HAMLSS_LAUNCH_CHECK();
         }
+        phase(M->levels() - 1, "coarse LU");
         M->coarse_inverse = nc > 96;
         if (M->coarse_inverse) {
             M->Minv.ensure((size_t)nc * nc);
@@ -909,6 +931,7 @@ std::unique_ptr<Prec> make_amg(Ctx& ctx, hamlss_mat* A, const hamlss_params& p) 
         }
     }
     HAMLSS_CUDA(cudaStreamSynchronize(s));
+    phase(M->levels() - 1, "coarse inv");
     return M;
 }
 

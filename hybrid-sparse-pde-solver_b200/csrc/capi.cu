@@ -6,6 +6,7 @@
 #include <string>
 #include <vector>
 
+#include "batch.cuh"
 #include "krylov.cuh"
 #include "nvml_energy.cuh"
 
@@ -692,6 +693,130 @@ int hamlss_solve_adaptive(hamlss_ctx* ctx, const hamlss_mat* A, const double* b,
         if (n_log) *n_log = nlog;
         if (where == HAMLSS_HOST) Am->ws.d[7].download(x, A->A.n, s);
         HAMLSS_CUDA(cudaStreamSynchronize(s));
+        return HAMLSS_OK;
+    });
+}
+
+// ------------------------------------------------------------------ batched solves
+int hamlss_batch_create(hamlss_ctx* ctx, int32_t count, const int32_t* row_off,
+                        const int32_t* row_ptr, const int32_t* col_idx, const double* values,
+                        const int32_t* solver, const int32_t* precond, int where,
+                        const hamlss_params* params, hamlss_batch** out) {
+    return guarded([&]() -> int {
+        if (!ctx || !out) return set_err(HAMLSS_ERR_INVALID, "null argument");
+        hamlss_params p;
+        if (params) p = *params;
+        else hamlss_params_default(&p);
+        std::lock_guard<std::mutex> g(ctx->c.mu);
+        HAMLSS_CUDA(cudaSetDevice(ctx->c.device));
+        auto* h = new hamlss_batch();
+        h->ctx = ctx;
+        try {
+            h->b = batch_create(ctx->c, ctx, count, row_off, row_ptr, col_idx, values, solver, precond,
+                                where, p);
+        } catch (...) {
+            delete h;
+            throw;
+        }
+        *out = h;
+        return HAMLSS_OK;
+    });
+}
+
+int hamlss_batch_solve(hamlss_ctx* ctx, hamlss_batch* B, const double* b, double* x, int where,
+                       hamlss_batch_result* results, hamlss_stats* total) {
+    return guarded([&]() -> int {
+        if (!ctx || !B || !B->b || !b || !x) return set_err(HAMLSS_ERR_INVALID, "null argument");
+        if (B->ctx != ctx) return set_err(HAMLSS_ERR_INVALID, "batch belongs to another context");
+        std::lock_guard<std::mutex> g(ctx->c.mu);
+        HAMLSS_CUDA(cudaSetDevice(ctx->c.device));
+        Batch& Bt = *B->b;
+        cudaStream_t s = ctx->c.lane.stream;
+        const double t0 = now_s();
+        const double* db = b;
+        double* dx = x;
+        if (where == HAMLSS_HOST) {
+            Bt.bb.upload(b, Bt.N, s);
+            Bt.xb.upload(x, Bt.N, s);
+            db = Bt.bb.p;
+            dx = Bt.xb.p;
+        }
+        const double ms = batch_run(ctx->c, Bt, db, dx, 0xFu);
+        std::vector<hamlss_batch_result> res(Bt.count);
+        Bt.out.download(res.data(), Bt.count, s);
+        if (where == HAMLSS_HOST) Bt.xb.download(x, Bt.N, s);
+        HAMLSS_CUDA(cudaStreamSynchronize(s));
+        if (results) std::memcpy(results, res.data(), sizeof(hamlss_batch_result) * Bt.count);
+        if (total) {
+            hamlss_stats st;
+            std::memset(&st, 0, sizeof(st));
+            st.converged = 1;
+            st.outer_iterations = 0;
+            st.solver_used = -1;
+            st.precond_used = -1;
+            for (const auto& r : res) {
+                st.iterations += r.iterations;
+                st.outer_iterations = std::max(st.outer_iterations, r.outer_iterations);
+                st.converged &= r.converged;
+                st.final_residual = std::max(st.final_residual, r.final_residual);
+                st.initial_residual = std::max(st.initial_residual, r.initial_residual);
+                if (r.status != HAMLSS_OK && st.status == HAMLSS_OK) st.status = r.status;
+            }
+            st.true_residual = st.final_residual;
+            st.device_time_s = ms * 1e-3;
+            st.solve_time_s = now_s() - t0;
+            *total = st;
+        }
+        return HAMLSS_OK;
+    });
+}
+
+int hamlss_batch_set_widths(hamlss_batch* B, const int32_t widths[4]) {
+    return guarded([&]() -> int {
+        if (!B || !B->b || !widths) return set_err(HAMLSS_ERR_INVALID, "null argument");
+        for (int c = 0; c < kBatchClasses; ++c) {
+            bool ok = false;
+            for (int w : kBatchWidths) ok |= w == widths[c];
+            if (!ok) return set_err(HAMLSS_ERR_INVALID, "team width must be 32, 64, 128, 256 or 512");
+        }
+        for (int c = 0; c < kBatchClasses; ++c) B->b->width[c] = widths[c];
+        return HAMLSS_OK;
+    });
+}
+
+int hamlss_batch_get_widths(const hamlss_batch* B, int32_t widths[4]) {
+    return guarded([&]() -> int {
+        if (!B || !B->b || !widths) return set_err(HAMLSS_ERR_INVALID, "null argument");
+        for (int c = 0; c < kBatchClasses; ++c) widths[c] = B->b->width[c];
+        return HAMLSS_OK;
+    });
+}
+
+int hamlss_batch_autotune(hamlss_ctx* ctx, hamlss_batch* B, const double* b, int where,
+                          const char* cache_path, int32_t widths[4]) {
+    return guarded([&]() -> int {
+        if (!ctx || !B || !B->b || !b) return set_err(HAMLSS_ERR_INVALID, "null argument");
+        std::lock_guard<std::mutex> g(ctx->c.mu);
+        HAMLSS_CUDA(cudaSetDevice(ctx->c.device));
+        Batch& Bt = *B->b;
+        const double* db = b;
+        if (where == HAMLSS_HOST) {
+            Bt.bb.upload(b, Bt.N, ctx->c.lane.stream);
+            db = Bt.bb.p;
+        }
+        int w[kBatchClasses];
+        batch_autotune(ctx->c, Bt, db, cache_path, w);
+        if (widths)
+            for (int c = 0; c < kBatchClasses; ++c) widths[c] = w[c];
+        return HAMLSS_OK;
+    });
+}
+
+int hamlss_batch_release(hamlss_batch* B) {
+    return guarded([&]() -> int {
+        if (!B) return HAMLSS_OK;
+        if (B->ctx) HAMLSS_CUDA(cudaSetDevice(B->ctx->c.device));
+        delete B;
         return HAMLSS_OK;
     });
 }

@@ -21,7 +21,9 @@
 #include <cmath>
 #include <cstring>
 
+#include "ilu_row.cuh"
 #include "krylov.cuh"
+#include "scan.cuh"
 
 namespace cg = cooperative_groups;
 
@@ -122,30 +124,6 @@ __global__ void k_levels(int n, const int* __restrict__ trp, const int* __restri
         }
         start = next;
         grid.sync();
-    }
-}
-
-// IKJ elimination of the rows of one lower level (ilu.cpp:52-83), thread per row.
-// status[0] receives the smallest row whose pivot is tiny (ZERO_PIVOT).
-__device__ __forceinline__ void ilu_row(int i, const int* __restrict__ rp, const int* __restrict__ ci,
-                                        const int* __restrict__ dpos, double* lu, int* status) {
-    const int s = rp[i], e = rp[i + 1];
-    for (int p = s; p < e; ++p) {
-        const int k = ci[p];
-        if (k >= i) break;
-        const int dk = dpos[k];
-        const double ukk = dk >= 0 ? lu[dk] : 0.0;
-        if (fabs(ukk) < kEps) { atomicMin(status, k); return; }
-        const double lik = lu[p] / ukk;
-        lu[p] = lik;
-        int pi = p + 1;                          // merge pointer into row i (sorted)
-        for (int q = rp[k]; q < rp[k + 1]; ++q) {
-            const int j = ci[q];
-            if (j <= k) continue;
-            while (pi < e && ci[pi] < j) ++pi;
-            if (pi == e) break;
-            if (ci[pi] == j) lu[pi] = __dsub_rn(lu[pi], __dmul_rn(lik, lu[q]));
-        }
     }
 }
 
@@ -488,6 +466,45 @@ std::unique_ptr<Prec> make_ilu0(Ctx& ctx, hamlss_mat* A) {
     P->trow.release();
     P->indeg.release();
     return P;
+}
+
+// Level sets of the strictly lower and strictly upper dependency DAGs of a square CSR
+// pattern (the definitions make_ilu0 uses), without factorising.  The batched solver
+// calls this on its block-diagonal matrix: blocks never depend on one another, so every
+// row's level is its level inside its own system.
+void pattern_levels(Ctx& ctx, int n, int nnz, const int* rp, const int* ci, DBuf<int>& dpos,
+                    DBuf<int>& levelL, DBuf<int>& levelU, int* nlevL, int* nlevU) {
+    cudaStream_t s = ctx.lane.stream;
+    dpos.ensure(std::max(n, 1));
+    levelL.ensure(std::max(n, 1));
+    levelU.ensure(std::max(n, 1));
+    *nlevL = *nlevU = 0;
+    if (n == 0) return;
+    const int g = std::max(1, std::min(ceil_div(n, 256), ctx.sm_count * 8));
+    DBuf<int> lcnt(n), ucnt(n), trp(n + 1), trow(std::max(nnz, 1)), fill(n), indeg(n), cnt(n + 2),
+        order(n), lptr(n + 1), nl(2);
+    k_row_info<<<g, 256, 0, s>>>(n, rp, ci, dpos.p, lcnt.p, ucnt.p);
+    HAMLSS_CUDA(cudaMemsetAsync(trp.p, 0, sizeof(int) * (n + 1), s));
+    k_col_count<<<g, 256, 0, s>>>(n, rp, ci, trp.p);
+    HAMLSS_LAUNCH_CHECK();
+    exclusive_scan(ctx, trp.p, n + 1);
+    HAMLSS_CUDA(cudaMemcpyAsync(fill.p, trp.p, sizeof(int) * n, cudaMemcpyDeviceToDevice, s));
+    k_col_fill<<<g, 256, 0, s>>>(n, rp, ci, fill.p, trow.p);
+    HAMLSS_LAUNCH_CHECK();
+    const int lb = coop_blocks(ctx, k_levels<true>, 256);
+    HAMLSS_CUDA(cudaMemcpyAsync(indeg.p, lcnt.p, sizeof(int) * n, cudaMemcpyDeviceToDevice, s));
+    HAMLSS_CUDA(cudaMemsetAsync(cnt.p, 0, sizeof(int) * (n + 2), s));
+    coop_launch(ctx, k_levels<true>, lb, 256, n, (const int*)trp.p, (const int*)trow.p, indeg.p,
+                order.p, lptr.p, cnt.p, levelL.p, nl.p);
+    HAMLSS_CUDA(cudaMemcpyAsync(indeg.p, ucnt.p, sizeof(int) * n, cudaMemcpyDeviceToDevice, s));
+    HAMLSS_CUDA(cudaMemsetAsync(cnt.p, 0, sizeof(int) * (n + 2), s));
+    coop_launch(ctx, k_levels<false>, lb, 256, n, (const int*)trp.p, (const int*)trow.p, indeg.p,
+                order.p, lptr.p, cnt.p, levelU.p, nl.p + 1);
+    int h[2];
+    HAMLSS_CUDA(cudaMemcpyAsync(h, nl.p, sizeof(h), cudaMemcpyDeviceToHost, s));
+    HAMLSS_CUDA(cudaStreamSynchronize(s));
+    *nlevL = h[0];
+    *nlevU = h[1];
 }
 
 // Inspection entry points (hamlss.h).

@@ -42,6 +42,8 @@ int amg_level_matrix(const Prec* P, int level, int which, int* rows, int* cols, 
                      int* ci, double* v, cudaStream_t s);
 int amg_aggregate_matrix(Ctx& ctx, hamlss_mat* A, double theta, int* agg_host, int* n_agg);
 int ilu_copy_levels(const Prec* M, int which, int* level, int* nlev, cudaStream_t s);
+void pattern_levels(Ctx& ctx, int n, int nnz, const int* rp, const int* ci, DBuf<int>& dpos,
+                    DBuf<int>& levelL, DBuf<int>& levelU, int* nlevL, int* nlevU);
 
 // Extract a_ii into A->diag (once per value version).
 void ensure_diag(Ctx& ctx, hamlss_mat* A);

@@ -123,6 +123,19 @@ class Stats(C.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+class BatchResult(C.Structure):
+    """hamlss_batch_result: per-system outcome of a batched solve."""
+
+    _fields_ = [
+        ("iterations", C.c_int32),
+        ("outer_iterations", C.c_int32),
+        ("converged", C.c_int32),
+        ("status", C.c_int32),
+        ("initial_residual", C.c_double),
+        ("final_residual", C.c_double),
+    ]
+
+
 class Escalation(C.Structure):
     """hamlss_escalation: hsps::EscalationRecord (adaptive_selector.hpp:38-44)."""
 
@@ -186,12 +199,19 @@ def _declare(L: C.CDLL) -> None:
         "hamlss_solve_adaptive": (C.c_int, [P, P, V, V, C.c_int, C.POINTER(Params),
                                             C.POINTER(Stats), C.POINTER(Escalation), I32, pi,
                                             pi]),
-        "hamlss_extract_features": (C.c_int, [P, P, pd, pi]),
+        "hamlss_extract_features": (C.c_int, [P, P, P, pi]),
         "hamlss_amg_aggregate": (C.c_int, [P, P, D, V, pi]),
         "hamlss_amg_num_levels": (C.c_int, [P, pi]),
         "hamlss_amg_level_matrix": (C.c_int, [P, I32, I32, pi, pi, pi, V, V, V]),
         "hamlss_ilu_factors": (C.c_int, [P, V]),
         "hamlss_ilu_levels": (C.c_int, [P, I32, V, pi]),
+        "hamlss_batch_create": (C.c_int, [P, I32, V, V, V, V, V, V, C.c_int, C.POINTER(Params),
+                                          pp]),
+        "hamlss_batch_solve": (C.c_int, [P, P, V, V, C.c_int, V, C.POINTER(Stats)]),
+        "hamlss_batch_set_widths": (C.c_int, [P, V]),
+        "hamlss_batch_get_widths": (C.c_int, [P, V]),
+        "hamlss_batch_autotune": (C.c_int, [P, P, V, C.c_int, C.c_char_p, V]),
+        "hamlss_batch_release": (C.c_int, [P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name, None)

@@ -228,6 +228,53 @@ int hamlss_solve_adaptive(hamlss_ctx* ctx, const hamlss_mat* A, const double* b,
 int hamlss_extract_features(hamlss_ctx* ctx, const hamlss_mat* A, double features[24],
                             int32_t* initial_state);
 
+/* ------------------------------------------------------------ batched solves
+ * No counterpart in the reference, which solves one system per SolverBase::solve call
+ * (include/solvers/solver_base.hpp:32-35); each system of a batch runs the reference's
+ * algorithm for its method (CGSolver + JacobiPreconditioner, or FGMRESSolver +
+ * ILUPreconditioner with drop_tol 0), all of them inside one persistent kernel.
+ *
+ * The `count` systems form ONE block-diagonal CSR: system k owns rows
+ * [row_off[k], row_off[k+1]) and every entry of those rows has its column in the same
+ * range (global row_ptr of row_off[count] + 1 entries, global column indices).  row_off is
+ * host memory; row_ptr / col_idx / values follow `where`.  solver[k] is HAMLSS_SOLVER_CG
+ * or HAMLSS_SOLVER_FGMRES, precond[k] HAMLSS_PREC_NONE, _JACOBI or (FGMRES only) _ILU.
+ * Values are kept in FP64 and FP32: the systems are solved in FP32 inside an FP64
+ * iterative-refinement loop to params->tol FP64 relative residual (params->max_iter inner
+ * iterations, params->ir_max_outer refinement steps, params->restart_size <= 32).
+ * A setup failure of one system (zero diagonal, zero pivot) is reported in its result and
+ * does not stop the others. */
+typedef struct hamlss_batch hamlss_batch;
+typedef struct hamlss_batch_result {
+    int32_t iterations;        /* inner Krylov iterations over all refinement steps */
+    int32_t outer_iterations;  /* FP64 refinement steps                             */
+    int32_t converged;
+    int32_t status;            /* HAMLSS_OK or the HAMLSS_ERR_* of this system      */
+    double  initial_residual;  /* ||b - A x0||                                      */
+    double  final_residual;    /* FP64 ||b - A x|| / ||b||                          */
+} hamlss_batch_result;
+
+int hamlss_batch_create(hamlss_ctx* ctx, int32_t count, const int32_t* row_off,
+                        const int32_t* row_ptr, const int32_t* col_idx, const double* values,
+                        const int32_t* solver, const int32_t* precond, int where,
+                        const hamlss_params* params, hamlss_batch** out);
+/* b, x: row_off[count] entries each (x = initial guess on entry).  results: `count`
+ * entries (may be NULL); total (may be NULL): summed iterations, converged = all systems
+ * converged, final_residual = the largest, device_time_s = the kernel's event time. */
+int hamlss_batch_solve(hamlss_ctx* ctx, hamlss_batch* B, const double* b, double* x, int where,
+                       hamlss_batch_result* results, hamlss_stats* total);
+/* Team width (threads per system: 32, 64, 128, 256 or 512) of the four size classes
+ * n <= 1024, <= 4096, <= 16384 and larger.  Results depend on the width only through the
+ * order of the dot-product sums. */
+int hamlss_batch_set_widths(hamlss_batch* B, const int32_t widths[4]);
+int hamlss_batch_get_widths(const hamlss_batch* B, int32_t widths[4]);
+/* Time every width for every size class present (solves of the batch itself, x0 = 0, on
+ * internal buffers), keep the fastest, and record them in `cache_path` (may be NULL) keyed
+ * by device, class, method mix and restart length; a cached key is reused without timing. */
+int hamlss_batch_autotune(hamlss_ctx* ctx, hamlss_batch* B, const double* b, int where,
+                          const char* cache_path, int32_t widths[4]);
+int hamlss_batch_release(hamlss_batch* B);
+
 /* ------------------------------------------------------- inspection (parity)
  * Internals that the reference keeps private but that parity is checked on. */
 /* Greedy aggregation of one matrix (amg.cpp:30-67): agg[rows]; returns the count. */

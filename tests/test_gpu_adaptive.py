@@ -114,7 +114,9 @@ def test_ladder_warm_start_reuses_x():
 
 
 def test_ladder_ilut_request_refused():
-    A = H.SparseMatrix.convection_diffusion_2d(16, 1.0, *P.convdiff_wind(16, 300.0))
-    sel = H.AdaptiveSelector(default_params(max_iter=5))   # default drop_tol = 1e-4
+    # EASY (CG+Jacobi) cannot converge in 5 iterations, so the ladder escalates to
+    # MODERATE, which asks for ILUT under the default drop_tol = 1e-4
+    A = H.SparseMatrix.poisson_2d(16)
+    sel = H.AdaptiveSelector(default_params(max_iter=5))
     with pytest.raises(H.HamlssError):
         sel.solve(A, np.ones(256), np.zeros(256))

@@ -70,10 +70,13 @@ def hierarchy(M):
 
 
 def assert_same_hierarchy(h_dev, h_ref):
+    # The reference also stores, on each coarse level, a copy of the P and R that lead to
+    # it (amg.cpp:220-229); the coarsest level's copy is the previous level's operator, so
+    # P and R are compared on the levels that own them: every level but the coarsest.
     assert len(h_dev) == len(h_ref)
     for l, (a, b) in enumerate(zip(h_dev, h_ref)):
         for k in ("A", "P", "R"):
-            if k not in b:
+            if k not in b or (k != "A" and l == len(h_ref) - 1):
                 continue
             assert a[k][:2] == b[k][:2], (l, k)
             for x, y in zip(a[k][2:], b[k][2:]):
