@@ -748,8 +748,8 @@ int aggregate_device(Ctx& ctx, const Csr<double>& A, double theta, DBuf<int>& ag
     HAMLSS_CUDA(cudaMemsetAsync(status.p, 0, sizeof(int) * n, s));
     HAMLSS_CUDA(cudaMemsetAsync(cnt.p, 0, sizeof(int) * (n + 2), s));
     {
-        static int per = 0;
-        if (!per) per = std::min(occupancy_blocks(k_aggregate_levels, 256), 4);
+        // thread-safe one-time initialisation (contexts may be driven from several threads)
+        static const int per = std::min(occupancy_blocks(k_aggregate_levels, 256), 4);
         int blocks = std::max(1, std::min(per * ctx.sm_count, ceil_div(n, 256)));
         const int* rp = A.rp;
         const int* ci = A.ci;

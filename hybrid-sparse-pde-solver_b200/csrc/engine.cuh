@@ -116,9 +116,9 @@ void launch_spmv(int sm_count, const Lane& L, const Csr<T>& A, const XOp& xop, c
                  const Fin& fin = Fin{}, const int* gate = nullptr, const char* name = "spmv",
                  double vec_bytes = -1.0) {
     ProfScope ps(L, name, csr_bytes(A) + (vec_bytes >= 0 ? vec_bytes : 2.0 * sizeof(T) * A.n));
-    static int per_sm = 0;
     auto kern = k_spmv<T, NRED, XOp, Epi, Fin>;
-    if (!per_sm) per_sm = std::min(occupancy_blocks(kern, kSpmvThreads), kMaxBlocksPerSm);
+    // thread-safe one-time initialisation (contexts may be driven from several threads)
+    static const int per_sm = std::min(occupancy_blocks(kern, kSpmvThreads), kMaxBlocksPerSm);
     const int ntiles = ceil_div(A.n, 32);
     int blocks = std::max(1, std::min(ceil_div(ntiles, kSpmvWarps), sm_count * per_sm));
     kern<<<blocks, kSpmvThreads, 0, L.stream>>>(A.n, A.rp, A.ci, A.v, xop, epi, L.red(), fin, gate);

@@ -329,8 +329,7 @@ struct IluPrec : Prec {
             k_ilu_apply_block<T, 1024><<<1, 1024, 0, L.stream>>>(F, r, yb, z, gate);
             HAMLSS_LAUNCH_CHECK();
         } else {
-            static int blocks = 0;
-            if (!blocks) blocks = coop_blocks(ctx, k_ilu_apply_grid<T>, 256);
+            static const int blocks = coop_blocks(ctx, k_ilu_apply_grid<T>, 256);
             void* args[] = {(void*)&F, (void*)&r, (void*)&yb, (void*)&z, (void*)&gate};
             HAMLSS_CUDA(cudaLaunchCooperativeKernel((const void*)k_ilu_apply_grid<T>, dim3(blocks),
                                                     dim3(256), args, 0, L.stream));
