@@ -32,6 +32,14 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "hybrid-sparse-pde-solver_b200"))
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 
+_T0 = time.perf_counter()
+
+
+def log(msg):
+    """Progress on stderr (the JSON result alone goes to stdout)."""
+    print(f"[bench {time.perf_counter() - _T0:8.1f}s] {msg}", file=sys.stderr, flush=True)
+
+
 N_SIDE = 2048
 SIGMA = 1.0
 TOL = 1e-10
@@ -49,6 +57,9 @@ def parse():
     ap.add_argument("--n-side", type=int, default=N_SIDE)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample-iters", type=int, default=40)
+    ap.add_argument("--serving-requests", type=int, default=200,
+                    help="requests in the serving stream (0 skips the serving measurement)")
+    ap.add_argument("--serving-n-max", type=float, default=2.6e5)
     return ap.parse_args()
 
 
@@ -65,6 +76,31 @@ def problem(n_side, seed):
     rp, ci, v = P.varkappa_poisson_2d(n_side, SIGMA, seed)
     b = P.rhs(len(rp) - 1, seed, -1.0, 1.0)
     return rp, ci, v, b
+
+
+# ------------------------------------------------------------- replicas over ranks
+def max_over_ranks(v, device):
+    """The largest of every rank's `v` (the slowest replica sets the job's time).  Every
+    rank must call it the same number of times; with one process it returns `v`."""
+    import torch
+    import torch.distributed as dist
+
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(v)
+    t = torch.tensor([float(v)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(steps_per_rank, world, max_ms):
+    """Whole-job solves/s: every rank solved `steps_per_rank` systems of its own (weak
+    scaling, no collective on the data path) within the slowest rank's time."""
+    return world * steps_per_rank / (max_ms / 1e3)
+
+
+def replica_seed(rank):
+    """Each rank solves its own seeded instance of the workload."""
+    return 1000 + rank
 
 
 # ----------------------------------------------------------------- clocks sampling
@@ -205,7 +241,9 @@ def run_ours(args, rank, world, local):
     L = _abi.lib()
     solver = solver_choice(args.solver)
     params, stype, ptype = make_params(solver)
-    rp, ci, v, b = problem(args.n_side, 1000 + rank)
+    log(f"solver {solver}; generating the {args.n_side}^2 system")
+    rp, ci, v, b = problem(args.n_side, replica_seed(rank))
+    log(f"n={len(rp) - 1} nnz={len(v)}; uploading")
     n, nnz = len(rp) - 1, len(v)
     A = H.SparseMatrix(n, n, rp, ci, v, ctx)
     db = torch.from_numpy(b).cuda()
@@ -231,6 +269,8 @@ def run_ours(args, rank, world, local):
 
     for _ in range(args.warmup):
         st = one_solve()
+        log(f"warm-up solve: {st.iterations} iterations, {st.outer_iterations} outer, "
+            f"true rel {st.true_residual:.2e}, {st.solve_time_s:.3f} s")
     if not st.converged or st.true_residual > 1.5 * TOL:
         raise RuntimeError(f"warm-up solve did not reach tolerance: {st.as_dict()}")
 
@@ -253,6 +293,7 @@ def run_ours(args, rank, world, local):
     ev1.record(stream)
     torch.cuda.synchronize()
     dev_ms = ev0.elapsed_time(ev1)
+    log(f"timed {args.steps} solves: {dev_ms:.1f} ms")
     cap = 64
     names = C.create_string_buffer(32 * cap)
     launches = (C.c_int32 * cap)()
@@ -267,12 +308,8 @@ def run_ours(args, rank, world, local):
         nm = names.raw[32 * i:32 * i + 32].split(b"\0")[0].decode()
         fams.append((nm, launches[i], tms[i], tby[i]))
     total_launches = sum(f[1] for f in fams)
-    max_ms = dev_ms
-    if dist:
-        t = torch.tensor([dev_ms], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        max_ms = float(t.item())
-    value = world * args.steps / (max_ms / 1e3)
+    max_ms = max_over_ranks(dev_ms, "cuda")
+    value = replica_throughput(args.steps, world, max_ms)
 
     # ---- end to end through the C ABI with host buffers (pinned)
     hb = torch.from_numpy(b).pin_memory()
@@ -311,12 +348,9 @@ def run_ours(args, rank, world, local):
     for _ in range(e_steps):
         e2e_step()
     torch.cuda.synchronize()
-    e_dt = time.perf_counter() - t0
-    if dist:
-        t = torch.tensor([e_dt], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e_dt = float(t.item())
-    e2e_value = world * e_steps / e_dt
+    e_dt = max_over_ranks(time.perf_counter() - t0, "cuda")
+    e2e_value = replica_throughput(e_steps, world, e_dt * 1e3)
+    log(f"e2e {e_steps} solves: {e_dt:.3f} s")
     h2d = 4 * (n + 1) + 12 * nnz + 8 * n + 8 * n       # CSR + b + initial x
     d2h = 8 * n                                         # solution
 
@@ -427,6 +461,107 @@ def run_reference(args, rank, world):
                     "d2h_bytes_per_step": 0}}
 
 
+# ------------------------------------------------------------------ serving stream
+def serving_params():
+    import hsps_b200 as H
+
+    return H.SolverParams(tol=TOL, max_iter=4000, restart_size=30, drop_tol=0.0,
+                          precision=1, amg_omega=2.0 / 3.0, amg_coarse_limit=512, amg_levels=25)
+
+
+def _pct(lat, q):
+    lat = sorted(lat)
+    k = max(0, min(len(lat) - 1, int(np.ceil(q * len(lat))) - 1))
+    return lat[k]
+
+
+def serve_plain(reqs, params, device):
+    """One solve per call, in arrival order (the one-solve-per-launch path): upload, adaptive
+    ladder, download through the C ABI on one context.  Latency = completion - arrival."""
+    import ctypes as C
+
+    import hsps_b200 as H
+    from hsps_b200 import _abi
+
+    L = _abi.lib()
+    ctx = H.Context(device)
+    lat, res = [], []
+    t0 = time.perf_counter()
+    for rp, ci, v, b, arr, _ in reqs:
+        now = time.perf_counter() - t0
+        if now < arr:
+            time.sleep(arr - now)
+        x = np.zeros(len(b))
+        mh = C.c_void_p()
+        rc = L.hamlss_mat_upload(ctx.h, len(b), len(b), len(v), rp.ctypes.data, ci.ctypes.data,
+                                 v.ctypes.data, H.HOST, C.byref(mh))
+        st = _abi.Stats()
+        nlog, init = C.c_int32(), C.c_int32()
+        if rc == 0:
+            rc = L.hamlss_solve_adaptive(ctx.h, mh, b.ctypes.data, x.ctypes.data, H.HOST,
+                                         C.byref(params), C.byref(st), None, 0, C.byref(nlog),
+                                         C.byref(init))
+        L.hamlss_mat_release(mh)
+        if rc:
+            raise RuntimeError(L.hamlss_last_error())
+        lat.append(time.perf_counter() - t0 - arr)
+        res.append(st.true_residual if st.converged else float("inf"))
+    span = time.perf_counter() - t0 - reqs[0][4]
+    return {"solves_per_s": round(len(reqs) / span, 2), "p50_ms": round(1e3 * _pct(lat, 0.5), 2),
+            "p99_ms": round(1e3 * _pct(lat, 0.99), 2), "max_true_residual": max(res)}
+
+
+def serve_engine(reqs, params, device):
+    """The continuous-batching server: requests submitted at their arrival times."""
+    from hsps_b200.serve import Server
+
+    with Server(device=device, slots=4, batch_max_rows=16384) as srv:
+        hs = []
+        t0 = time.perf_counter()
+        for rp, ci, v, b, arr, _ in reqs:
+            now = time.perf_counter() - t0
+            if now < arr:
+                time.sleep(arr - now)
+            hs.append(srv.submit(rp, ci, v, b, params=params))
+        res = []
+        for h in hs:
+            _, st = h.wait(timeout=900)
+            res.append(st.true_residual if st.converged else float("inf"))
+        rep = srv.report()
+    return {"solves_per_s": round(rep["solves_per_s"], 2),
+            "p50_ms": round(1e3 * rep["p50_latency_s"], 2),
+            "p99_ms": round(1e3 * rep["p99_latency_s"], 2), "max_true_residual": max(res),
+            "coalesced": rep["coalesced"], "batches": rep["batches"],
+            "escalated": rep["escalated"], "peak_running": rep["peak_running"],
+            "peak_admitted_gb": round(rep["peak_admitted_bytes"] / 1e9, 3)}
+
+
+def run_serving(args, local):
+    """Serving stream: burst capacity of both paths, then Poisson arrivals at 90% of the
+    plain path's capacity, latencies measured from arrival."""
+    from hsps_b200 import problems as P
+
+    R = args.serving_requests
+    params = serving_params()
+    burst = P.serving_stream(R, 77, 1e3, args.serving_n_max, rate=0.0)
+    serve_plain(burst[:8], params, local)           # warm-up (module load, first contexts)
+    serve_engine(burst[:8], params, local)
+    log("serving: burst, plain path")
+    plain_b = serve_plain(burst, params, local)
+    log(f"serving: burst, server ({plain_b})")
+    eng_b = serve_engine(burst, params, local)
+    log(f"serving: arrivals ({eng_b})")
+    rate = 0.9 * plain_b["solves_per_s"]
+    timed = P.serving_stream(R, 77, 1e3, args.serving_n_max, rate=rate)
+    plain_r = serve_plain(timed, params, local)
+    eng_r = serve_engine(timed, params, local)
+    return {"requests": R, "n_range": [1e3, args.serving_n_max], "tol": TOL,
+            "mix": "50% var-kappa Poisson, 35% upwind conv-diff, 15% shifted Helmholtz",
+            "inner": "mixed precision (FP32 inner, FP64 refinement), adaptive ladder",
+            "burst": {"server": eng_b, "plain": plain_b},
+            "poisson_arrivals": {"rate_per_s": round(rate, 2), "server": eng_r, "plain": plain_r}}
+
+
 def main():
     args = parse()
     rank, world, local = dist_env()
@@ -446,7 +581,11 @@ def main():
     out, data = run_ours(args, rank, world, local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         iters_fp64 = out["iterations"] if out["config"]["solver"] == "cg_jacobi" else fp64_cg_iterations(data)
+        log(f"FP64 CG+Jacobi needs {iters_fp64} iterations; timing the reference sample")
         out["cpu_baseline"] = cpu_baseline(args, data, iters_fp64)
+        log("cpu baseline done")
+    if rank == 0 and world == 1 and args.serving_requests > 0:
+        out["serving"] = run_serving(args, local)
     if world > 1:
         import torch
 

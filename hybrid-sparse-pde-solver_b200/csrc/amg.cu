@@ -43,6 +43,13 @@ namespace hamlss {
 namespace {
 
 constexpr double kEps = 2.220446049250313e-16;
+constexpr int kLongRow = 32;            // rows longer than this are given a whole block
+constexpr int kSortMax = 8192;          // largest shared-memory sort (u64 keys)
+
+// Rows that the block-per-row kernels (smoothed P, transpose sort) take.
+__host__ __device__ __forceinline__ bool smooth_row_on_block(int len) {
+    return len > kLongRow && len + 1 <= kSortMax;
+}
 
 struct DCsr {
     int n = 0, m = 0, nnz = 0;
@@ -173,6 +180,7 @@ __global__ void k_smooth_p(int n, const int* __restrict__ rp, const int* __restr
                            int* pcnt, const int* __restrict__ prp, int* pci, double* pv) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const int s = rp[i], e = rp[i + 1];
+        if (smooth_row_on_block(e - s)) continue;       // k_smooth_p_rows takes it
         double id = 0.0;
         for (int k = s; k < e; ++k)
             if (ci[k] == i) { id = (fabs(v[k]) > kEps) ? omega / v[k] : 0.0; break; }
@@ -239,6 +247,7 @@ __global__ void k_t_fill(int n, const int* __restrict__ rp, const int* __restric
 __global__ void k_t_sort(int m, const int* __restrict__ trp, int* tci, double* tv) {
     for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < m; r += gridDim.x * blockDim.x) {
         const int s = trp[r], e = trp[r + 1];
+        if (smooth_row_on_block(e - s)) continue;       // k_t_sort_rows takes it
         for (int a = s + 1; a < e; ++a) {
             int c = tci[a];
             double x = tv[a];
@@ -262,8 +271,10 @@ template <bool FILL>
 __global__ void k_spgemm(int m, const int* __restrict__ arp, const int* __restrict__ aci,
                          const double* __restrict__ av, const int* __restrict__ brp,
                          const int* __restrict__ bci, const double* __restrict__ bv, int* ccnt,
-                         const int* __restrict__ crp, int* cci, double* cv, int* heads) {
+                         const int* __restrict__ crp, int* cci, double* cv, int* heads,
+                         const int* __restrict__ cls) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+        if (cls[i]) continue;                           // k_spgemm_rows takes it
         const int s = arp[i], k = arp[i + 1] - s;
         int lpos[kHeads], lend[kHeads], lcur[kHeads];
         int* pos = k <= kHeads ? lpos : heads + 3LL * s;
@@ -293,6 +304,247 @@ __global__ void k_spgemm(int m, const int* __restrict__ arp, const int* __restri
             }
         }
         if (!FILL) ccnt[i] = o;
+    }
+}
+
+// ------------------------------------------------- block-per-row setup kernels
+// Coarse AMG levels grow long rows (hundreds of entries); one thread per row is then
+// quadratic or worse.  These kernels give such a row a whole block and sort in shared
+// memory.  They produce exactly the same entries, values and order as the thread-per-row
+// kernels above: every value is still accumulated by one thread, in the same order.
+constexpr int kRowBlock = 256;
+constexpr unsigned long long kNoKey = ~0ull;
+
+// Ascending bitonic sort of N (a power of two) keys in shared memory by the whole block.
+__device__ void block_bitonic(unsigned long long* a, int N) {
+    __syncthreads();
+    for (int k = 2; k <= N; k <<= 1)
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int t = threadIdx.x; t < N; t += blockDim.x) {
+                const int p = t ^ j;
+                if (p > t) {
+                    const unsigned long long x = a[t], y = a[p];
+                    if ((x > y) == ((t & k) == 0)) { a[t] = y; a[p] = x; }
+                }
+            }
+            __syncthreads();
+        }
+}
+
+__device__ __forceinline__ int pow2_at_least(int v) {
+    int p = 1;
+    while (p < v) p <<= 1;
+    return p;
+}
+
+// Rows [0, n) with kLongRow < len and len + 1 <= kSortMax, appended to `list`.
+// count[1] receives the longest listed row.
+__global__ void k_long_rows(int n, const int* __restrict__ rp, int* list, int* count) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int len = rp[i + 1] - rp[i];
+        if (smooth_row_on_block(len)) {
+            list[atomicAdd(count, 1)] = i;
+            atomicMax(count + 1, len);
+        }
+    }
+}
+
+// Smoothed prolongation of the listed rows (amg.cpp:101-178), one block per row.  The
+// row's (agg(j), position) pairs are sorted, so each candidate column's contributions sit
+// together in row order; the first thread of each group computes the value with the same
+// operations as p_value().  Shared memory: pow2(len + 1) keys + as many doubles.
+template <bool FILL>
+__global__ void k_smooth_p_rows(const int* __restrict__ rows, int nrows, const int* __restrict__ rp,
+                                const int* __restrict__ ci, const double* __restrict__ v,
+                                const int* __restrict__ agg, double omega, int* pcnt,
+                                const int* __restrict__ prp, int* pci, double* pv) {
+    extern __shared__ unsigned long long sm_keys[];
+    __shared__ double s_id;
+    __shared__ int s_warp[kRowBlock / 32];
+    for (int r = blockIdx.x; r < nrows; r += gridDim.x) {
+        const int i = rows[r];
+        const int s = rp[i], e = rp[i + 1], len = e - s;
+        const int N = pow2_at_least(len + 1);
+        double* val = reinterpret_cast<double*>(sm_keys + N);
+        if (threadIdx.x == 0) {
+            double id = 0.0;
+            for (int k = s; k < e; ++k)
+                if (ci[k] == i) { id = (fabs(v[k]) > kEps) ? omega / v[k] : 0.0; break; }
+            s_id = id;
+        }
+        __syncthreads();
+        const double id = s_id;
+        const bool raw = fabs(id) < kEps;
+        const unsigned ai = (unsigned)agg[i];
+        for (int t = threadIdx.x; t < N; t += blockDim.x) {
+            unsigned long long key = kNoKey;
+            if (t == 0) key = (unsigned long long)ai << 32;             // the row's own aggregate
+            else if (t <= len && !raw) {
+                const int j = ci[s + t - 1];
+                if (j != i) key = ((unsigned long long)(unsigned)agg[j] << 32) | (unsigned)t;
+            }
+            sm_keys[t] = key;
+        }
+        block_bitonic(sm_keys, N);
+        // group leaders compute their candidate's value; survivors are flagged in val[]
+        int keep = 0;
+        for (int t = threadIdx.x; t < N; t += blockDim.x) {
+            const unsigned long long key = sm_keys[t];
+            bool lead = key != kNoKey && (t == 0 || (sm_keys[t - 1] >> 32) != (key >> 32));
+            double x = 0.0;
+            if (lead) {
+                const unsigned c = (unsigned)(key >> 32);
+                x = (c == ai) ? 1.0 : 0.0;
+                for (int u = t; u < N && (sm_keys[u] >> 32) == c && sm_keys[u] != kNoKey; ++u) {
+                    const int pos = (int)(sm_keys[u] & 0xffffffffu);
+                    if (pos == 0) continue;
+                    x = __dsub_rn(x, __dmul_rn(id, v[s + pos - 1]));
+                }
+                if (!(fabs(x) > 1e-14)) lead = false;
+            }
+            val[t] = lead ? x : __longlong_as_double(0x7ff8dead00000000ll);  // NaN marks "none"
+            keep += lead;
+        }
+        // block count of survivors
+        int w = keep;
+        for (int o = 16; o > 0; o >>= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
+        __syncthreads();
+        if ((threadIdx.x & 31) == 0) s_warp[threadIdx.x >> 5] = w;
+        __syncthreads();
+        if (!FILL) {
+            if (threadIdx.x == 0) {
+                int tot = 0;
+                for (int q = 0; q < (int)blockDim.x / 32; ++q) tot += s_warp[q];
+                pcnt[i] = tot;
+            }
+        } else if (threadIdx.x == 0) {
+            // survivors in ascending column order: one thread walks the sorted groups
+            int o = prp[i];
+            for (int t = 0; t < N; ++t) {
+                const double x = val[t];
+                if (x == x) {
+                    pci[o] = (int)(sm_keys[t] >> 32);
+                    pv[o] = x;
+                    ++o;
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// SpGEMM row classes: 0 thread-per-row merge (short rows, or rows too wide for shared
+// memory), 1 block-per-row hash accumulation.  `hmax` receives the widest class-1 table.
+constexpr int kHashMax = 4096;          // distinct output columns a shared table may hold
+
+__global__ void k_spgemm_classify(int m, const int* __restrict__ arp, const int* __restrict__ aci,
+                                  const int* __restrict__ brp, int bcols, int* cls, int* list,
+                                  int* count, int* hmax) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+        const int s = arp[i], k = arp[i + 1] - s;
+        long long u = 0;
+        for (int t = 0; t < k; ++t) {
+            const int j = aci[s + t];
+            u += brp[j + 1] - brp[j];
+        }
+        const long long h = u < bcols ? u : bcols;
+        const bool block = (k > kHeads || u > 512) && h <= kHashMax;
+        cls[i] = block ? 1 : 0;
+        if (block) {
+            list[atomicAdd(count, 1)] = i;
+            atomicMax(hmax, (int)h);
+        }
+    }
+}
+
+// Row i of C = A B for the listed rows, one block per row.  The products of left entry t
+// are added into a shared hash table (slot per output column) one t at a time, with a
+// barrier between t's, so every column's sum runs over t in row order from 0.0 with
+// separate multiply and add -- the same arithmetic as k_spgemm.  Survivors (|v| > eps^2)
+// are then sorted by column.  Shared memory: S ints + S doubles + S u64 (S = table size).
+template <bool FILL>
+__global__ void k_spgemm_rows(const int* __restrict__ rows, int nrows, int S,
+                              const int* __restrict__ arp, const int* __restrict__ aci,
+                              const double* __restrict__ av, const int* __restrict__ brp,
+                              const int* __restrict__ bci, const double* __restrict__ bv,
+                              int* ccnt, const int* __restrict__ crp, int* cci, double* cv) {
+    extern __shared__ unsigned long long sm_keys[];
+    double* vals = reinterpret_cast<double*>(sm_keys + S);
+    int* cols = reinterpret_cast<int*>(vals + S);
+    __shared__ int s_n;
+    for (int r = blockIdx.x; r < nrows; r += gridDim.x) {
+        const int i = rows[r];
+        const int s = arp[i], k = arp[i + 1] - s;
+        for (int t = threadIdx.x; t < S; t += blockDim.x) {
+            cols[t] = -1;
+            vals[t] = 0.0;
+        }
+        if (threadIdx.x == 0) s_n = 0;
+        __syncthreads();
+        for (int t = 0; t < k; ++t) {
+            const int j = aci[s + t];
+            const double a = av[s + t];
+            const int e1 = brp[j + 1];
+            for (int e = brp[j] + threadIdx.x; e < e1; e += blockDim.x) {
+                const int col = bci[e];
+                unsigned h = ((unsigned)col * 2654435761u) & (unsigned)(S - 1);
+                for (;;) {
+                    const int old = atomicCAS(&cols[h], -1, col);
+                    if (old == -1 || old == col) break;
+                    h = (h + 1) & (unsigned)(S - 1);
+                }
+                vals[h] = __dadd_rn(vals[h], __dmul_rn(a, bv[e]));
+            }
+            __syncthreads();
+        }
+        // compact the survivors (any order), then sort them by column
+        for (int t = threadIdx.x; t < S; t += blockDim.x)
+            if (cols[t] >= 0 && fabs(vals[t]) > kEps * kEps)
+                sm_keys[atomicAdd(&s_n, 1)] = ((unsigned long long)(unsigned)cols[t] << 32) | (unsigned)t;
+        __syncthreads();
+        const int cnt = s_n;
+        if (!FILL) {
+            if (threadIdx.x == 0) ccnt[i] = cnt;
+        } else {
+            const int N = pow2_at_least(cnt > 0 ? cnt : 1);
+            for (int t = cnt + threadIdx.x; t < N; t += blockDim.x) sm_keys[t] = kNoKey;
+            block_bitonic(sm_keys, N);
+            const int o = crp[i];
+            for (int t = threadIdx.x; t < cnt; t += blockDim.x) {
+                const unsigned long long key = sm_keys[t];
+                cci[o + t] = (int)(key >> 32);
+                cv[o + t] = vals[key & 0xffffffffu];
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// Sort the listed rows of a transpose (distinct columns per row) by column, one block per
+// row; the values move with their columns.  Shared memory: pow2(len) keys + len doubles.
+__global__ void k_t_sort_rows(const int* __restrict__ rows, int nrows, const int* __restrict__ trp,
+                              int* tci, double* tv) {
+    extern __shared__ unsigned long long sm_keys[];
+    for (int r = blockIdx.x; r < nrows; r += gridDim.x) {
+        const int row = rows[r];
+        const int s = trp[row], len = trp[row + 1] - s;
+        const int N = pow2_at_least(len);
+        double* val = reinterpret_cast<double*>(sm_keys + N);
+        for (int t = threadIdx.x; t < N; t += blockDim.x) {
+            if (t < len) {
+                sm_keys[t] = ((unsigned long long)(unsigned)tci[s + t] << 32) | (unsigned)t;
+                val[t] = tv[s + t];
+            } else {
+                sm_keys[t] = kNoKey;
+            }
+        }
+        block_bitonic(sm_keys, N);
+        for (int t = threadIdx.x; t < len; t += blockDim.x) {
+            const unsigned long long key = sm_keys[t];
+            tci[s + t] = (int)(key >> 32);
+            tv[s + t] = val[key & 0xffffffffu];
+        }
+        __syncthreads();
     }
 }
 
@@ -790,17 +1042,59 @@ void build_csr_counts(Ctx& ctx, DCsr& C, int rows, int cols, DBuf<int>& cnt) {
     C.v.ensure(std::max(C.nnz, 1));
 }
 
+// Rows of a CSR that a block-per-row kernel takes (smooth_row_on_block); returns their
+// count, the list in `list` and the shared memory the longest one needs, 16 bytes per slot
+// of its sort (synchronises).
+int long_rows(Ctx& ctx, int n, const int* rp, DBuf<int>& list, size_t* smem) {
+    cudaStream_t s = ctx.lane.stream;
+    list.ensure(std::max(n, 1));
+    DBuf<int> cnt(2);
+    cnt.zero(s);
+    if (n) k_long_rows<<<grid_for(ctx, n), 256, 0, s>>>(n, rp, list.p, cnt.p);
+    HAMLSS_LAUNCH_CHECK();
+    int h[2] = {0, 0};
+    cnt.download(h, 2, s);
+    HAMLSS_CUDA(cudaStreamSynchronize(s));
+    size_t N = 1;
+    while (N < (size_t)h[1] + 1) N <<= 1;
+    *smem = 16 * N;
+    return h[0];
+}
+
+// Grid and dynamic shared memory of a block-per-row kernel (shared bytes per block).
+template <typename K>
+int row_grid(Ctx& ctx, K kernel, size_t smem, int nrows) {
+    HAMLSS_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per = 0;
+    HAMLSS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, kRowBlock, smem));
+    return std::max(1, std::min(nrows, ctx.sm_count * std::max(per, 1)));
+}
+
 void smooth_prolongation(Ctx& ctx, const Csr<double>& A, const DBuf<int>& agg, int nc, double omega,
                          DCsr& P) {
     const int n = A.n;
     cudaStream_t s = ctx.lane.stream;
     const int g = grid_for(ctx, n);
-    DBuf<int> cnt(n);
+    DBuf<int> cnt(n), list;
+    size_t smem = 0;                                // keys + values of the longest row
+    const int nlong = long_rows(ctx, n, A.rp, list, &smem);
     k_smooth_p<false><<<g, 256, 0, s>>>(n, A.rp, A.ci, A.v, agg.p, omega, cnt.p, nullptr, nullptr, nullptr);
     HAMLSS_LAUNCH_CHECK();
+    if (nlong) {
+        const int gb = row_grid(ctx, k_smooth_p_rows<false>, smem, nlong);
+        k_smooth_p_rows<false><<<gb, kRowBlock, smem, s>>>(list.p, nlong, A.rp, A.ci, A.v, agg.p, omega,
+                                                           cnt.p, nullptr, nullptr, nullptr);
+        HAMLSS_LAUNCH_CHECK();
+    }
     build_csr_counts(ctx, P, n, nc, cnt);
     k_smooth_p<true><<<g, 256, 0, s>>>(n, A.rp, A.ci, A.v, agg.p, omega, nullptr, P.rp.p, P.ci.p, P.v.p);
     HAMLSS_LAUNCH_CHECK();
+    if (nlong) {
+        const int gb = row_grid(ctx, k_smooth_p_rows<true>, smem, nlong);
+        k_smooth_p_rows<true><<<gb, kRowBlock, smem, s>>>(list.p, nlong, A.rp, A.ci, A.v, agg.p, omega,
+                                                          nullptr, P.rp.p, P.ci.p, P.v.p);
+        HAMLSS_LAUNCH_CHECK();
+    }
 }
 
 void transpose(Ctx& ctx, const DCsr& P, DCsr& R) {
@@ -820,20 +1114,51 @@ void transpose(Ctx& ctx, const DCsr& P, DCsr& R) {
     k_t_fill<<<grid_for(ctx, P.n), 256, 0, s>>>(P.n, P.rp.p, P.ci.p, P.v.p, fill.p, R.ci.p, R.v.p);
     k_t_sort<<<grid_for(ctx, R.n), 256, 0, s>>>(R.n, R.rp.p, R.ci.p, R.v.p);
     HAMLSS_LAUNCH_CHECK();
+    DBuf<int> list;
+    size_t smem = 0;
+    const int nlong = long_rows(ctx, R.n, R.rp.p, list, &smem);
+    if (nlong) {
+        const int gb = row_grid(ctx, k_t_sort_rows, smem, nlong);
+        k_t_sort_rows<<<gb, kRowBlock, smem, s>>>(list.p, nlong, R.rp.p, R.ci.p, R.v.p);
+        HAMLSS_LAUNCH_CHECK();
+    }
 }
 
 void spgemm(Ctx& ctx, const Csr<double>& A, const Csr<double>& B, DCsr& C) {
     cudaStream_t s = ctx.lane.stream;
     const int g = grid_for(ctx, A.n);
     DBuf<int> heads(3LL * std::max(A.nnz, 1));
-    DBuf<int> cnt(std::max(A.n, 1));
-    k_spgemm<false><<<g, 256, 0, s>>>(A.n, A.rp, A.ci, A.v, B.rp, B.ci, B.v, cnt.p, nullptr, nullptr,
-                                      nullptr, heads.p);
+    DBuf<int> cnt(std::max(A.n, 1)), cls(std::max(A.n, 1)), list(std::max(A.n, 1)), meta(2);
+    meta.zero(s);
+    if (A.n)
+        k_spgemm_classify<<<g, 256, 0, s>>>(A.n, A.rp, A.ci, B.rp, B.m, cls.p, list.p, meta.p, meta.p + 1);
     HAMLSS_LAUNCH_CHECK();
+    int hm[2] = {0, 0};
+    meta.download(hm, 2, s);
+    HAMLSS_CUDA(cudaStreamSynchronize(s));
+    const int nlong = hm[0];
+    int S = 64;
+    while (S < 2 * hm[1]) S <<= 1;
+    const size_t smem = 20 * (size_t)S;                 // u64 keys + doubles + ints per slot
+    k_spgemm<false><<<g, 256, 0, s>>>(A.n, A.rp, A.ci, A.v, B.rp, B.ci, B.v, cnt.p, nullptr, nullptr,
+                                      nullptr, heads.p, cls.p);
+    HAMLSS_LAUNCH_CHECK();
+    if (nlong) {
+        const int gb = row_grid(ctx, k_spgemm_rows<false>, smem, nlong);
+        k_spgemm_rows<false><<<gb, kRowBlock, smem, s>>>(list.p, nlong, S, A.rp, A.ci, A.v, B.rp, B.ci, B.v,
+                                                         cnt.p, nullptr, nullptr, nullptr);
+        HAMLSS_LAUNCH_CHECK();
+    }
     build_csr_counts(ctx, C, A.n, B.m, cnt);
     k_spgemm<true><<<g, 256, 0, s>>>(A.n, A.rp, A.ci, A.v, B.rp, B.ci, B.v, nullptr, C.rp.p, C.ci.p,
-                                     C.v.p, heads.p);
+                                     C.v.p, heads.p, cls.p);
     HAMLSS_LAUNCH_CHECK();
+    if (nlong) {
+        const int gb = row_grid(ctx, k_spgemm_rows<true>, smem, nlong);
+        k_spgemm_rows<true><<<gb, kRowBlock, smem, s>>>(list.p, nlong, S, A.rp, A.ci, A.v, B.rp, B.ci, B.v,
+                                                        nullptr, C.rp.p, C.ci.p, C.v.p);
+        HAMLSS_LAUNCH_CHECK();
+    }
 }
 
 }  // namespace

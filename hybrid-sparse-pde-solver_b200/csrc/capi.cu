@@ -63,6 +63,10 @@ void fgmres_cost(long long n, long long nz, const SolveResult& r, long long* flo
 
 }  // namespace
 
+namespace hamlss {
+int set_last_error(int code, const std::string& msg) { return set_err(code, msg); }
+}  // namespace hamlss
+
 extern "C" {
 
 const char* hamlss_version(void) { return "hamlss-b200 0.1 (sm_100a)"; }

@@ -22,6 +22,9 @@ struct Error : std::runtime_error {
 
 [[noreturn]] inline void fail(int code, const std::string& msg) { throw Error(code, msg); }
 
+// Record the thread's hamlss_last_error() message; returns `code`.
+int set_last_error(int code, const std::string& msg);
+
 inline void cuda_check(cudaError_t e, const char* what, const char* file, int line) {
     if (e != cudaSuccess) {
         int code = (e == cudaErrorMemoryAllocation) ? HAMLSS_ERR_NOMEM : HAMLSS_ERR_CUDA;

@@ -148,6 +148,46 @@ class Escalation(C.Structure):
     ]
 
 
+class ServerConfig(C.Structure):
+    """hamlss_server_config: device, solve lanes, HBM budget, coalescing limits."""
+
+    _fields_ = [
+        ("device", C.c_int32),
+        ("slots", C.c_int32),
+        ("hbm_budget_bytes", C.c_int64),
+        ("batch_max_rows", C.c_int32),
+        ("batch_max_count", C.c_int32),
+    ]
+
+
+class ServerReport(C.Structure):
+    """hamlss_server_report: counters, latency percentiles and throughput of a server."""
+
+    _fields_ = [
+        ("submitted", C.c_int64),
+        ("completed", C.c_int64),
+        ("failed", C.c_int64),
+        ("cancelled", C.c_int64),
+        ("coalesced", C.c_int64),
+        ("batches", C.c_int64),
+        ("escalated", C.c_int64),
+        ("fallback", C.c_int64),
+        ("queued", C.c_int64),
+        ("running", C.c_int32),
+        ("peak_running", C.c_int32),
+        ("admitted_bytes", C.c_int64),
+        ("peak_admitted_bytes", C.c_int64),
+        ("p50_latency_s", C.c_double),
+        ("p99_latency_s", C.c_double),
+        ("mean_latency_s", C.c_double),
+        ("max_latency_s", C.c_double),
+        ("solves_per_s", C.c_double),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
 _lib = None
 
 
@@ -212,6 +252,16 @@ def _declare(L: C.CDLL) -> None:
         "hamlss_batch_get_widths": (C.c_int, [P, V]),
         "hamlss_batch_autotune": (C.c_int, [P, P, V, C.c_int, C.c_char_p, V]),
         "hamlss_batch_release": (C.c_int, [P]),
+        "hamlss_server_config_default": (None, [C.POINTER(ServerConfig)]),
+        "hamlss_server_create": (C.c_int, [C.POINTER(ServerConfig), pp]),
+        "hamlss_server_submit": (C.c_int, [P, I32, I32, V, V, V, V, V, C.POINTER(Params),
+                                           C.POINTER(C.c_int64)]),
+        "hamlss_server_wait": (C.c_int, [P, I64, D, C.POINTER(Stats)]),
+        "hamlss_server_test": (C.c_int, [P, I64, pi]),
+        "hamlss_server_cancel": (C.c_int, [P, I64]),
+        "hamlss_server_get_report": (C.c_int, [P, C.POINTER(ServerReport)]),
+        "hamlss_server_reset_report": (C.c_int, [P]),
+        "hamlss_server_destroy": (C.c_int, [P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name, None)

@@ -128,3 +128,32 @@ def helmholtz_2d(n: int, c: float):
 
 def rhs(n_rows: int, seed: int, lo: float = 0.0, hi: float = 1.0) -> np.ndarray:
     return uniform(seed, n_rows, lo, hi, offset=1 << 40)
+
+
+def serving_stream(count: int, seed: int, n_lo: float = 1e3, n_hi: float = 4.2e6,
+                   rate: float = 0.0):
+    """A serving workload: `count` requests (rp, ci, v, b, arrival_s, kind).
+
+    Sizes are log-uniform in [n_lo, n_hi] on square grids (side = round(sqrt(n))).  The mix
+    is 50% variable-kappa Poisson (sigma uniform in [0, 1.5]), 35% upwind
+    convection-diffusion (cell Peclet log-uniform in [1, 1000]) and 15% shifted Helmholtz
+    (c uniform in [0.1, 10]); rhs uniform [0, 1).  Arrivals form a Poisson process of
+    `rate` requests/s (exponential gaps); rate 0 puts every arrival at t = 0."""
+    u = uniform(seed, 6 * count).reshape(count, 6)
+    t = 0.0
+    out = []
+    for k in range(count):
+        n = math.exp(math.log(n_lo) + u[k, 0] * (math.log(n_hi) - math.log(n_lo)))
+        side = max(8, int(round(math.sqrt(n))))
+        rseed = seed * 1_000_003 + k
+        if u[k, 1] < 0.5:
+            A, kind = varkappa_poisson_2d(side, 1.5 * u[k, 2], rseed), "varkappa"
+        elif u[k, 1] < 0.85:
+            pe = math.exp(u[k, 3] * math.log(1000.0))
+            A, kind = convection_diffusion_2d(side, 1.0, *convdiff_wind(side, pe)), "convdiff"
+        else:
+            A, kind = helmholtz_2d(side, 0.1 + 9.9 * u[k, 4]), "helmholtz"
+        if rate > 0:
+            t += -math.log1p(-u[k, 5]) / rate
+        out.append((*A, rhs(side * side, rseed), t, kind))
+    return out

@@ -275,6 +275,74 @@ int hamlss_batch_autotune(hamlss_ctx* ctx, hamlss_batch* B, const double* b, int
                           const char* cache_path, int32_t widths[4]);
 int hamlss_batch_release(hamlss_batch* B);
 
+/* ------------------------------------------------------------------ serving
+ * No counterpart in the reference, which solves one system per synchronous
+ * AdaptiveSelector::solve call (src/adaptive/adaptive_selector.cpp:298-394).  A server keeps
+ * that per-request algorithm (the adaptive ladder; params->precision selects the FP64 or
+ * the mixed-precision inner path) and runs many requests at once on one device:
+ *   - admission: a request is admitted when its estimated device footprint fits
+ *     hbm_budget_bytes beside those already admitted; one that could never fit is refused
+ *     by submit with HAMLSS_ERR_BUDGET;
+ *   - `slots` solve lanes (a worker thread and CUDA stream each) run admitted requests
+ *     through the ladder concurrently, so their kernels overlap on the device;
+ *   - requests with n <= batch_max_rows are coalesced: whenever the batch lane is free it
+ *     solves every queued small request with the head's tolerance (up to batch_max_count)
+ *     in one persistent launch -- CG + Jacobi for symmetric systems with a positive
+ *     diagonal, FGMRES + ILU(0) for the rest, FP32 inside FP64 refinement.  A system that
+ *     fails there continues on a solve lane through the full ladder.
+ *   - when the ladder fails from the state the features chose, the rungs below it that it
+ *     skipped are tried too (FGMRES + ILU(0); CG + Jacobi for symmetric systems with a
+ *     positive diagonal), each from the request's initial guess.
+ * Requests that arrive while others run are admitted as lanes and budget free up.  A
+ * request's result does not depend on the other requests in flight.
+ *
+ * The caller's arrays (CSR, b, x) must stay valid and unmodified until the request is
+ * finished; x holds the initial guess on submit and the solution once it is done.
+ * Functions are thread-safe: any thread may submit, test, wait or cancel. */
+typedef struct hamlss_server hamlss_server;
+typedef struct hamlss_server_config {
+    int32_t device;            /* CUDA device (0)                                           */
+    int32_t slots;             /* concurrent solve lanes (4)                                */
+    int64_t hbm_budget_bytes;  /* admission budget for request state (150e9)                */
+    int32_t batch_max_rows;    /* coalesce requests with n <= this; 0 disables (16384)      */
+    int32_t batch_max_count;   /* systems per coalesced launch (2048)                       */
+} hamlss_server_config;
+
+typedef struct hamlss_server_report {
+    int64_t submitted, completed, failed, cancelled;
+    int64_t coalesced;         /* completed in the batch lane                               */
+    int64_t batches;           /* coalesced launches                                        */
+    int64_t escalated;         /* moved from the batch lane to a solve lane                 */
+    int64_t fallback;          /* solved by a rung below the ladder's failed start           */
+    int64_t queued;            /* waiting now                                               */
+    int32_t running, peak_running;
+    int64_t admitted_bytes, peak_admitted_bytes;
+    double  p50_latency_s, p99_latency_s, mean_latency_s, max_latency_s;  /* submit -> done */
+    double  solves_per_s;      /* completed / (last completion - first submit)              */
+} hamlss_server_report;
+
+void hamlss_server_config_default(hamlss_server_config* config);
+int hamlss_server_create(const hamlss_server_config* config, hamlss_server** out);
+/* Queue one solve A x = b (host CSR, host b and x).  *request_id identifies it. */
+int hamlss_server_submit(hamlss_server* server, int32_t n, int32_t nnz, const int32_t* row_ptr,
+                         const int32_t* col_idx, const double* values, const double* b, double* x,
+                         const hamlss_params* params, int64_t* request_id);
+/* Wait for a request (timeout_s < 0: no limit).  Returns its status (HAMLSS_OK or the error
+ * that ended it) and fills *stats; HAMLSS_ERR_TIMEOUT if it is still in flight.  A request
+ * that has been waited for successfully or with an error is forgotten. */
+int hamlss_server_wait(hamlss_server* server, int64_t request_id, double timeout_s,
+                       hamlss_stats* stats);
+/* *done = 1 once the request has finished (it can then be waited for without blocking). */
+int hamlss_server_test(hamlss_server* server, int64_t request_id, int32_t* done);
+/* Withdraw a request that has not started: its wait returns HAMLSS_ERR_CANCELLED. */
+int hamlss_server_cancel(hamlss_server* server, int64_t request_id);
+int hamlss_server_get_report(hamlss_server* server, hamlss_server_report* report);
+/* Clear the counters and latency record (e.g. after a warm-up stream). */
+int hamlss_server_reset_report(hamlss_server* server);
+/* Finish the requests in flight, cancel the queued ones, release the lanes.  No other call
+ * on this server may be in progress or follow. */
+int hamlss_server_destroy(hamlss_server* server);
+
 /* ------------------------------------------------------- inspection (parity)
  * Internals that the reference keeps private but that parity is checked on. */
 /* Greedy aggregation of one matrix (amg.cpp:30-67): agg[rows]; returns the count. */

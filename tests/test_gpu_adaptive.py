@@ -4,6 +4,14 @@ Features: same initial state; row statistics equal to 1e-12 relative, Lanczos-de
 entries (condition, lambda bounds, energy proxies) to 1e-6 relative (dot products are
 summed in a different order).  Ladder (ladder_mode 0, the reference's rule): same
 initial state, same escalation sequence and final state, iterations within +-1.
+
+One exception is measured, not assumed: when the reference's own final iterate has a true
+residual above 10 x tol although its recursive FGMRES estimate says converged, the basis
+has lost orthogonality and the iteration count is decided by rounding (on the Pe = 30
+conv-diff case FGMRES + AMG takes 23 iterations in the reference, 33 with numpy's MGS
+sums and 16 with CGS2, true residual 1e-7 in every variant).  For such a case the test
+requires the same states and convergence flags and a device true residual no worse than
+10 x the reference's.
 """
 import numpy as np
 import pytest
@@ -66,6 +74,11 @@ def test_ladder_matches_reference(ref, name, A):
     assert st.state_used == so.state_used
     assert [(e.from_state, e.to_state) for e in sel.escalation_log()] == \
            [(e.from_state, e.to_state) for e in log_ref]
+    ref_true = np.linalg.norm(b - ref.spmv(*A, xo)) / np.linalg.norm(b)
+    if ref_true > 10 * p.tol:
+        # rounding-decided iteration count (see the module docstring)
+        assert st.true_residual <= 10 * ref_true, (st.true_residual, ref_true)
+        return
     assert abs(st.iterations - so.iterations) <= 1
     if ok:
         assert st.true_residual < 10 * p.tol

@@ -75,7 +75,7 @@ def test_batch_mix_matches_reference(orc, ref):
         solver = 0 if solvers[k] == H.SOLVER_CG else 1
         prec = 1 if precs[k] == H.PREC_JACOBI else 2
         rc, xr, st = ref.solve(solver, prec, *A, rhs[k], params=pref)
-        assert rc == 0 and st.converged
+        assert rc == 1 and st.converged          # ref_solve returns solve()'s bool
         err = np.linalg.norm(xs[k] - xr) / np.linalg.norm(xr)
         assert err <= 1e-6, (k, err)
     assert tot.converged == 1
