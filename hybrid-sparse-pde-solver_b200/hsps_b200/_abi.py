@@ -230,6 +230,7 @@ def _declare(L: C.CDLL) -> None:
         "hamlss_axpy": (C.c_int, [P, I32, D, V, V]),
         "hamlss_axpby": (C.c_int, [P, I32, D, V, D, V]),
         "hamlss_scale": (C.c_int, [P, I32, D, V]),
+        "hamlss_dot_noalloc": (C.c_int, [I32, V, V, pd, V]),
         "hamlss_precond_setup": (C.c_int, [P, P, C.c_int, C.POINTER(Params), pp, pd]),
         "hamlss_precond_apply": (C.c_int, [P, P, V, V, C.c_int]),
         "hamlss_precond_type": (C.c_int, [P, pi]),

@@ -193,6 +193,22 @@ int hamlss_axpy(hamlss_ctx* ctx, int32_t n, double alpha, const double* x, doubl
 int hamlss_axpby(hamlss_ctx* ctx, int32_t n, double a, const double* x, double b, double* y);
 int hamlss_scale(hamlss_ctx* ctx, int32_t n, double alpha, double* x);
 
+/* x . y for callers that cannot let a library allocate device memory: an application that
+ * reserves the GPU's memory for its own pool, or a latency-critical loop where cudaMalloc /
+ * cudaFree would stall the whole device.  No counterpart in the reference (it has no
+ * device memory); same kernel and same result as hamlss_dot, but no context and no
+ * allocation of any kind.
+ *   x, y    device pointers on the CURRENT device; result: host pointer (one double).
+ *   stream  a cudaStream_t (NULL: the default stream); the call waits for it to finish.
+ * The scratch (2048 partial sums, the result slot and a ticket: 16 KiB) is a fixed array
+ * compiled into the library, which every GPU that loads the library holds until exit.
+ * The first call on each device looks up that array's device address (make that first
+ * call before any stream capture).  All calls on a device share the array: calls whose
+ * work may overlap on the GPU (other streams, other host threads) race; serialise them.
+ * A launch that would need more than 2048 partial sums (a GPU with more than 256 SMs) is
+ * refused with HAMLSS_ERR_SIZE. */
+int hamlss_dot_noalloc(int32_t n, const double* x, const double* y, double* result, void* stream);
+
 /* ------------------------------------------------------------ preconditioners
  * Replaces SolverFactory::make_precond (solver_factory.cpp:54-97) followed by
  * PreconditionerBase::setup.  kind = HAMLSS_PREC_*; HAMLSS_PREC_NONE yields *out == NULL
