@@ -8,9 +8,9 @@
 //                 seed(i)  <=>  no seed in IN(i) = { s < i : s -> i strong }
 //                 agg(i)    =  number of seeds before i            (seed)
 //                           =  agg(min seed in IN(i))              (otherwise)
-//               IN(i) only holds lower indices, so the decisions follow the DAG's
-//               topological levels: one cooperative kernel pops each level's frontier
-//               (Kahn order), one grid barrier per level, then a scan numbers the seeds.
+//               IN(i) only holds lower indices, so one cooperative kernel decides the
+//               nodes in index order, warp by warp, each node as soon as its IN nodes are
+//               decided (no grid barriers), then a scan numbers the seeds.
 //   prolong     Jacobi-smoothed tentative prolongation (amg.cpp:101-178) computed
 //               sparsely: row i starts at e_agg(i) and subtracts (omega/a_ii) a_ij at column
 //               agg(j) in row order, then drops |v| <= 1e-14.  Same operations in the same
@@ -34,6 +34,7 @@
 #include <cstring>
 
 #include "krylov.cuh"
+#include "dense_lu.cuh"
 #include "scan.cuh"
 
 namespace cg = cooperative_groups;
@@ -45,6 +46,8 @@ namespace {
 constexpr double kEps = 2.220446049250313e-16;
 constexpr int kLongRow = 32;            // rows longer than this are given a whole block
 constexpr int kSortMax = 8192;          // largest shared-memory sort (u64 keys)
+constexpr int kBlockedCoarse = 1024;    // coarsest levels above this use the blocked LU
+constexpr int kStallDenseMax = 8192;    // largest level the stall rule makes the coarsest
 
 // Rows that the block-per-row kernels (smoothed P, transpose sort) take.
 __host__ __device__ __forceinline__ bool smooth_row_on_block(int len) {
@@ -100,42 +103,70 @@ __global__ void k_in_fill(int n, const int* __restrict__ rp, const int* __restri
     }
 }
 
-// Decide seed / non-seed in the topological order of the IN-DAG.
-// status: 1 seed, 2 non-seed.  indeg starts at |IN(i)|; order/cnt are frontier storage.
-__global__ void k_aggregate_levels(int n, const int* __restrict__ rp, const int* __restrict__ ci,
-                                   const double* __restrict__ v, const double* __restrict__ rmax,
-                                   double theta, const int* __restrict__ in_rp,
-                                   const int* __restrict__ in_src, int* indeg, int* status,
-                                   int* order, int* cnt, int* nlev) {
-    cg::grid_group grid = cg::this_grid();
-    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
-    const int nth = gridDim.x * blockDim.x;
-    for (int i = tid; i < n; i += nth)
-        if (indeg[i] == 0) order[atomicAdd(&cnt[0], 1)] = i;
-    grid.sync();
-    int start = 0;
-    for (int l = 0;; ++l) {
-        const int c = *(volatile int*)&cnt[l];
-        if (c == 0) {
-            if (tid == 0) *nlev = l;
-            break;
-        }
-        const int next = start + c;
-        for (int t = tid; t < c; t += nth) {
-            const int i = order[start + t];
-            bool captured = false;
-            for (int k = in_rp[i]; k < in_rp[i + 1]; ++k)
-                if (status[in_src[k]] == 1) { captured = true; break; }
-            status[i] = captured ? 2 : 1;
-            const double th = theta * rmax[i];
-            for (int k = rp[i]; k < rp[i + 1]; ++k) {
-                const int d = ci[k];
-                if (d > i && fabs(v[k]) >= th)
-                    if (atomicSub(&indeg[d], 1) == 1) order[next + atomicAdd(&cnt[l + 1], 1)] = d;
+// Decide seed / non-seed for every node: seed(i) <=> no seed in IN(i).  IN(i) holds only
+// lower indices, so node i can be decided as soon as its IN nodes are.  Persistent warps
+// claim chunks of 32 consecutive nodes in increasing order (atomic ticket).  For a chunk,
+// the warp first reads the decided status of every IN node outside the chunk, all loads
+// in flight together (waiting for any not yet decided), and notes which IN nodes lie
+// inside the chunk; it then decides the 32 nodes in order from registers alone and
+// publishes them with one store.  Every claimed chunk belongs to a running warp
+// (cooperative launch: all blocks resident) and a chunk only waits on earlier chunks, so
+// the waits end.  Each wait is bounded (about a second): past that the kernel records
+// *err and moves on, and the host reports HAMLSS_ERR_TIMEOUT.
+// status: 0 undecided (zeroed before the launch), 1 seed, 2 non-seed.
+constexpr long long kWaitCycles = 2000000000LL;
+
+__device__ __forceinline__ int wait_status(const int* status, int src, int* err) {
+    const volatile int* vs = status + src;
+    int st = *vs;
+    if (st == 0) {
+        const long long t0 = clock64();
+        while ((st = *vs) == 0) {
+            if (clock64() - t0 > kWaitCycles) {
+                atomicExch(err, 1);
+                return 2;
             }
         }
-        start = next;
-        grid.sync();
+    }
+    return st;
+}
+
+__global__ void k_aggregate_wave(int n, const int* __restrict__ in_rp, const int* __restrict__ in_src,
+                                 int* status, int* ticket, int* err) {
+    const int lane = threadIdx.x & 31;
+    for (;;) {
+        int base = 0;
+        if (lane == 0) base = atomicAdd(ticket, 32);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= n) break;
+        const int cnt = min(32, n - base);
+        // pass 1: outside seeds (bit q of `outside`) and in-chunk IN nodes of node q (`inmask`,
+        // held by lane q)
+        unsigned outside = 0u, inmask = 0u;
+        for (int q = 0; q < cnt; ++q) {
+            const int i = base + q;
+            const int s0 = in_rp[i], s1 = in_rp[i + 1];
+            unsigned local_bits = 0u;
+            bool cap = false;
+            for (int k = s0 + lane; k < s1; k += 32) {
+                const int src = in_src[k];
+                if (src >= base) local_bits |= 1u << (src - base);
+                else cap |= wait_status(status, src, err) == 1;
+            }
+            if (__any_sync(0xffffffffu, cap)) outside |= 1u << q;
+            for (int o = 16; o > 0; o >>= 1) local_bits |= __shfl_xor_sync(0xffffffffu, local_bits, o);
+            if (lane == q) inmask = local_bits;
+        }
+        // pass 2: decide in order (seeds: bit q of `seeds`), registers only
+        unsigned seeds = 0u;
+        for (int q = 0; q < cnt; ++q) {
+            const unsigned mq = __shfl_sync(0xffffffffu, inmask, q);
+            const bool captured = ((outside >> q) & 1u) || (mq & seeds);
+            if (!captured) seeds |= 1u << q;
+        }
+        // publish
+        __threadfence();
+        if (lane < cnt) *(volatile int*)(status + base + lane) = ((seeds >> lane) & 1u) ? 1 : 2;
     }
 }
 
@@ -433,13 +464,20 @@ __global__ void k_smooth_p_rows(const int* __restrict__ rows, int nrows, const i
     }
 }
 
-// SpGEMM row classes: 0 thread-per-row merge (short rows, or rows too wide for shared
-// memory), 1 block-per-row hash accumulation.  `hmax` receives the widest class-1 table.
+// SpGEMM row classes: 0 thread-per-row merge (short rows, or rows too long for the rest),
+// 1 block-per-row hash accumulation, 2 block-per-row dense accumulation (the right operand
+// has at most kDenseCols columns), 3 warp-per-row merge (left rows of kHeads+1 to
+// kWarpHeads entries).  count[0] / list: class-1 rows, count[1] the widest class-1 table,
+// count[2] / list + m: class-2 rows, count[3] / list + 2m: class-3 rows, count[4] their
+// longest left row.
 constexpr int kHashMax = 4096;          // distinct output columns a shared table may hold
+constexpr int kDenseCols = 16384;       // columns a shared dense accumulator may hold
+constexpr int kWarpHeads = 2048;        // merge heads a warp keeps in shared memory
+constexpr int kMergeWarps = 4;          // warps (rows) per block of k_spgemm_warp
 
 __global__ void k_spgemm_classify(int m, const int* __restrict__ arp, const int* __restrict__ aci,
                                   const int* __restrict__ brp, int bcols, int* cls, int* list,
-                                  int* count, int* hmax) {
+                                  int* count) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
         const int s = arp[i], k = arp[i + 1] - s;
         long long u = 0;
@@ -448,12 +486,160 @@ __global__ void k_spgemm_classify(int m, const int* __restrict__ arp, const int*
             u += brp[j + 1] - brp[j];
         }
         const long long h = u < bcols ? u : bcols;
-        const bool block = (k > kHeads || u > 512) && h <= kHashMax;
-        cls[i] = block ? 1 : 0;
-        if (block) {
+        const bool lng = k > kHeads || u > 512;
+        int c = 0;
+        if (lng && bcols <= kDenseCols && h > kHashMax / 4) c = 2;
+        else if (lng && h <= kHashMax) c = 1;
+        else if (k > kHeads && k <= kWarpHeads) c = 3;
+        cls[i] = c;
+        if (c == 1) {
             list[atomicAdd(count, 1)] = i;
-            atomicMax(hmax, (int)h);
+            atomicMax(count + 1, (int)h);
+        } else if (c == 2) {
+            list[m + atomicAdd(count + 2, 1)] = i;
+        } else if (c == 3) {
+            list[2LL * m + atomicAdd(count + 3, 1)] = i;
+            atomicMax(count + 4, k);
         }
+    }
+}
+
+// Row i of C = A B for the listed rows, one warp per row: a k-way merge of the selected
+// rows of B with the k merge heads in shared memory (lane l owns heads l, l+32, ...).  Each
+// output column is the warp-wide minimum of the heads; its products are added in the
+// order of the left row (groups of 32 in turn, lanes in order within a group) from 0.0 with
+// separate multiply and add -- the arithmetic of k_spgemm.  Shared memory: 3 * KH ints per
+// warp (KH >= the longest listed left row).
+template <bool FILL>
+__global__ void k_spgemm_warp(const int* __restrict__ rows, int nrows, int KH,
+                              const int* __restrict__ arp, const int* __restrict__ aci,
+                              const double* __restrict__ av, const int* __restrict__ brp,
+                              const int* __restrict__ bci, const double* __restrict__ bv,
+                              int* ccnt, const int* __restrict__ crp, int* cci, double* cv) {
+    extern __shared__ int sm_heads[];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int* pos = sm_heads + (size_t)wid * 3 * KH;
+    int* end = pos + KH;
+    int* cur = end + KH;
+    const int nwarps = gridDim.x * (blockDim.x >> 5);
+    for (int r = blockIdx.x * (blockDim.x >> 5) + wid; r < nrows; r += nwarps) {
+        const int i = rows[r];
+        const int s = arp[i], k = arp[i + 1] - s;
+        for (int t = lane; t < k; t += 32) {
+            const int j = aci[s + t];
+            const int p0 = brp[j], p1 = brp[j + 1];
+            pos[t] = p0;
+            end[t] = p1;
+            cur[t] = p0 < p1 ? bci[p0] : INT_MAX;
+        }
+        int o = FILL ? crp[i] : 0;
+        const int groups = (k + 31) >> 5;
+        for (;;) {
+            int m = INT_MAX;
+            for (int t = lane; t < k; t += 32) m = min(m, cur[t]);
+            for (int q = 16; q > 0; q >>= 1) m = min(m, __shfl_xor_sync(0xffffffffu, m, q));
+            if (m == INT_MAX) break;
+            double sum = 0.0;
+            for (int g = 0; g < groups; ++g) {
+                const int t = (g << 5) + lane;
+                const bool hit = t < k && cur[t] == m;
+                double prod = 0.0;
+                if (hit) {
+                    const int p = pos[t];
+                    prod = __dmul_rn(av[s + t], bv[p]);
+                    pos[t] = p + 1;
+                    cur[t] = p + 1 < end[t] ? bci[p + 1] : INT_MAX;
+                }
+                unsigned mask = __ballot_sync(0xffffffffu, hit);
+                while (mask) {
+                    const int l = __ffs(mask) - 1;
+                    sum = __dadd_rn(sum, __shfl_sync(0xffffffffu, prod, l));
+                    mask &= mask - 1;
+                }
+            }
+            if (fabs(sum) > kEps * kEps) {
+                if (FILL && lane == 0) {
+                    cci[o] = m;
+                    cv[o] = sum;
+                }
+                ++o;
+            }
+        }
+        if (!FILL && lane == 0) ccnt[i] = o;
+        __syncwarp();
+    }
+}
+
+// Row i of C = A B for the listed rows, one block per row, with a dense accumulator of
+// all B.m columns in shared memory: the products of left entry t are added one t at a time
+// (barrier between t's), so each column sums over t in row order from 0.0 with separate
+// multiply and add -- the arithmetic of k_spgemm.  Survivors (|v| > eps^2) come out in
+// column order from a chunked block scan, which also clears the accumulator for the next
+// row.  Shared memory: B.m doubles + B.m flag bytes.
+template <bool FILL>
+__global__ void k_spgemm_dense(const int* __restrict__ rows, int nrows, int bcols,
+                               const int* __restrict__ arp, const int* __restrict__ aci,
+                               const double* __restrict__ av, const int* __restrict__ brp,
+                               const int* __restrict__ bci, const double* __restrict__ bv,
+                               int* ccnt, const int* __restrict__ crp, int* cci, double* cv) {
+    extern __shared__ double acc[];
+    unsigned char* hit = reinterpret_cast<unsigned char*>(acc + bcols);
+    __shared__ int s_warp[kRowBlock / 32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int chunk = (bcols + blockDim.x - 1) / blockDim.x;
+    const int c0 = threadIdx.x * chunk, c1 = min(bcols, c0 + chunk);
+    for (int c = c0; c < c1; ++c) {
+        acc[c] = 0.0;
+        hit[c] = 0;
+    }
+    __syncthreads();
+    for (int r = blockIdx.x; r < nrows; r += gridDim.x) {
+        const int i = rows[r];
+        const int s = arp[i], k = arp[i + 1] - s;
+        for (int t = 0; t < k; ++t) {
+            const int j = aci[s + t];
+            const double a = av[s + t];
+            const int e1 = brp[j + 1];
+            for (int e = brp[j] + threadIdx.x; e < e1; e += blockDim.x) {
+                const int col = bci[e];
+                acc[col] = __dadd_rn(acc[col], __dmul_rn(a, bv[e]));
+                hit[col] = 1;
+            }
+            __syncthreads();
+        }
+        // survivors of this thread's column chunk
+        int mine = 0;
+        for (int c = c0; c < c1; ++c) mine += (hit[c] && fabs(acc[c]) > kEps * kEps) ? 1 : 0;
+        // block exclusive scan of `mine`
+        int incl = mine;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        if (lane == 31) s_warp[wid] = incl;
+        __syncthreads();
+        int before = 0, total = 0;
+        for (int w = 0; w < nw; ++w) {
+            if (w < wid) before += s_warp[w];
+            total += s_warp[w];
+        }
+        before += incl - mine;
+        if (!FILL) {
+            if (threadIdx.x == 0) ccnt[i] = total;
+        } else {
+            int o = crp[i] + before;
+            for (int c = c0; c < c1; ++c)
+                if (hit[c] && fabs(acc[c]) > kEps * kEps) {
+                    cci[o] = c;
+                    cv[o] = acc[c];
+                    ++o;
+                }
+        }
+        for (int c = c0; c < c1; ++c) {
+            acc[c] = 0.0;
+            hit[c] = 0;
+        }
+        __syncthreads();
     }
 }
 
@@ -985,39 +1171,30 @@ int aggregate_device(Ctx& ctx, const Csr<double>& A, double theta, DBuf<int>& ag
     if (n == 0) return 0;
     ProfScope ps(ctx.lane, "setup", 0.0);
     DBuf<double> rmax(n);
-    DBuf<int> in_rp(n + 1), fill(n), status(n), order(n), cnt(n + 2), nlev(1), flag(n + 1);
+    DBuf<int> in_rp(n + 1), fill(n), status(n), cnt(2), flag(n + 1);
     k_rowmax<<<g, 256, 0, s>>>(n, A.rp, A.ci, A.v, rmax.p);
     HAMLSS_CUDA(cudaMemsetAsync(in_rp.p, 0, sizeof(int) * (n + 1), s));
     k_in_count<<<g, 256, 0, s>>>(n, A.rp, A.ci, A.v, rmax.p, theta, in_rp.p);
     HAMLSS_LAUNCH_CHECK();
-    DBuf<int> indeg(n);
-    HAMLSS_CUDA(cudaMemcpyAsync(indeg.p, in_rp.p, sizeof(int) * n, cudaMemcpyDeviceToDevice, s));
     long long tot = exclusive_scan(ctx, in_rp.p, n + 1);
     DBuf<int> in_src(std::max<long long>(tot, 1));
     HAMLSS_CUDA(cudaMemcpyAsync(fill.p, in_rp.p, sizeof(int) * n, cudaMemcpyDeviceToDevice, s));
     k_in_fill<<<g, 256, 0, s>>>(n, A.rp, A.ci, A.v, rmax.p, theta, fill.p, in_src.p);
     HAMLSS_LAUNCH_CHECK();
     HAMLSS_CUDA(cudaMemsetAsync(status.p, 0, sizeof(int) * n, s));
-    HAMLSS_CUDA(cudaMemsetAsync(cnt.p, 0, sizeof(int) * (n + 2), s));
+    HAMLSS_CUDA(cudaMemsetAsync(cnt.p, 0, sizeof(int) * 2, s));
     {
         // thread-safe one-time initialisation (contexts may be driven from several threads)
-        static const int per = std::min(occupancy_blocks(k_aggregate_levels, 256), 4);
-        int blocks = std::max(1, std::min(per * ctx.sm_count, ceil_div(n, 256)));
-        const int* rp = A.rp;
-        const int* ci = A.ci;
-        const double* v = A.v;
-        const double* rm = rmax.p;
+        // a few warps per SM: enough chunks in flight for the wavefront, few spinning loads
+        int blocks = std::max(1, std::min(2 * ctx.sm_count, ceil_div(n, 128)));
         const int* irp = in_rp.p;
         const int* isrc = in_src.p;
-        int* ideg = indeg.p;
         int* st = status.p;
-        int* ord = order.p;
-        int* cn = cnt.p;
-        int* nl = nlev.p;
+        int* tk = cnt.p;
+        int* er = cnt.p + 1;
         int nn = n;
-        double th = theta;
-        void* args[] = {&nn, &rp, &ci, &v, &rm, &th, &irp, &isrc, &ideg, &st, &ord, &cn, &nl};
-        HAMLSS_CUDA(cudaLaunchCooperativeKernel((const void*)k_aggregate_levels, dim3(blocks), dim3(256),
+        void* args[] = {&nn, &irp, &isrc, &st, &tk, &er};
+        HAMLSS_CUDA(cudaLaunchCooperativeKernel((const void*)k_aggregate_wave, dim3(blocks), dim3(128),
                                                 args, 0, s));
     }
     k_seed_flags<<<g, 256, 0, s>>>(n, status.p, flag.p);
@@ -1025,7 +1202,10 @@ int aggregate_device(Ctx& ctx, const Csr<double>& A, double theta, DBuf<int>& ag
     long long nseed = exclusive_scan(ctx, flag.p, n + 1);
     k_assign<<<g, 256, 0, s>>>(n, status.p, flag.p, in_rp.p, in_src.p, agg.p);
     HAMLSS_LAUNCH_CHECK();
+    int err = 0;
+    HAMLSS_CUDA(cudaMemcpyAsync(&err, cnt.p + 1, sizeof(int), cudaMemcpyDeviceToHost, s));
     HAMLSS_CUDA(cudaStreamSynchronize(s));
+    if (err) fail(HAMLSS_ERR_TIMEOUT, "AMG aggregation: a bounded wait ran out");
     return (int)nseed;
 }
 
@@ -1061,10 +1241,46 @@ int long_rows(Ctx& ctx, int n, const int* rp, DBuf<int>& list, size_t* smem) {
     return h[0];
 }
 
-// Grid and dynamic shared memory of a block-per-row kernel (shared bytes per block).
+// Grid of a block-per-row kernel for `smem` dynamic shared bytes per block.  The kernel's
+// dynamic shared-memory limit is raised once, to the largest any launch of it asks for
+// (kMaxRowSmem), and never lowered: contexts on other threads launch it concurrently.
+constexpr size_t kMaxRowSmem = 20 * (size_t)kSortMax;   // hash table of kSortMax slots
+static_assert(kMaxRowSmem >= 9 * (size_t)kDenseCols && kMaxRowSmem >= 16 * (size_t)kSortMax &&
+                  kMaxRowSmem >= 12 * (size_t)kWarpHeads * kMergeWarps,
+              "row kernels' shared memory");
+
+template <typename K>
+void raise_smem_limit(K kernel) {
+    HAMLSS_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxRowSmem));
+}
+
+bool raise_row_kernel_limits() {
+    raise_smem_limit(k_smooth_p_rows<false>);
+    raise_smem_limit(k_smooth_p_rows<true>);
+    raise_smem_limit(k_spgemm_rows<false>);
+    raise_smem_limit(k_spgemm_rows<true>);
+    raise_smem_limit(k_spgemm_dense<false>);
+    raise_smem_limit(k_spgemm_dense<true>);
+    raise_smem_limit(k_t_sort_rows);
+    raise_smem_limit(k_spgemm_warp<false>);
+    raise_smem_limit(k_spgemm_warp<true>);
+    return true;
+}
+
+// Grid of k_spgemm_warp (kMergeWarps rows per block).
+template <typename K>
+int merge_grid(Ctx& ctx, K kernel, size_t smem, int nrows) {
+    static const bool raised = raise_row_kernel_limits();   // once per process, thread-safe
+    (void)raised;
+    int per = 0;
+    HAMLSS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, 32 * kMergeWarps, smem));
+    return std::max(1, std::min(ceil_div(nrows, kMergeWarps), ctx.sm_count * std::max(per, 1)));
+}
+
 template <typename K>
 int row_grid(Ctx& ctx, K kernel, size_t smem, int nrows) {
-    HAMLSS_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    static const bool raised = raise_row_kernel_limits();   // once per process, thread-safe
+    (void)raised;
     int per = 0;
     HAMLSS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, kRowBlock, smem));
     return std::max(1, std::min(nrows, ctx.sm_count * std::max(per, 1)));
@@ -1128,18 +1344,24 @@ void spgemm(Ctx& ctx, const Csr<double>& A, const Csr<double>& B, DCsr& C) {
     cudaStream_t s = ctx.lane.stream;
     const int g = grid_for(ctx, A.n);
     DBuf<int> heads(3LL * std::max(A.nnz, 1));
-    DBuf<int> cnt(std::max(A.n, 1)), cls(std::max(A.n, 1)), list(std::max(A.n, 1)), meta(2);
+    DBuf<int> cnt(std::max(A.n, 1)), cls(std::max(A.n, 1)), list(3LL * std::max(A.n, 1)), meta(5);
     meta.zero(s);
     if (A.n)
-        k_spgemm_classify<<<g, 256, 0, s>>>(A.n, A.rp, A.ci, B.rp, B.m, cls.p, list.p, meta.p, meta.p + 1);
+        k_spgemm_classify<<<g, 256, 0, s>>>(A.n, A.rp, A.ci, B.rp, B.m, cls.p, list.p, meta.p);
     HAMLSS_LAUNCH_CHECK();
-    int hm[2] = {0, 0};
-    meta.download(hm, 2, s);
+    int hm[5] = {0, 0, 0, 0, 0};
+    meta.download(hm, 5, s);
     HAMLSS_CUDA(cudaStreamSynchronize(s));
-    const int nlong = hm[0];
+    const int nlong = hm[0], ndense = hm[2], nwarp = hm[3];
+    int KH = 32;
+    while (KH < hm[4]) KH <<= 1;
+    const size_t wsmem = sizeof(int) * 3 * (size_t)KH * kMergeWarps;
+    const int* wlist = list.p + 2LL * A.n;
     int S = 64;
     while (S < 2 * hm[1]) S <<= 1;
     const size_t smem = 20 * (size_t)S;                 // u64 keys + doubles + ints per slot
+    const size_t dsmem = 9 * (size_t)std::max(B.m, 1);   // dense accumulator + hit flags
+    const int* dlist = list.p + A.n;
     k_spgemm<false><<<g, 256, 0, s>>>(A.n, A.rp, A.ci, A.v, B.rp, B.ci, B.v, cnt.p, nullptr, nullptr,
                                       nullptr, heads.p, cls.p);
     HAMLSS_LAUNCH_CHECK();
@@ -1147,6 +1369,18 @@ void spgemm(Ctx& ctx, const Csr<double>& A, const Csr<double>& B, DCsr& C) {
         const int gb = row_grid(ctx, k_spgemm_rows<false>, smem, nlong);
         k_spgemm_rows<false><<<gb, kRowBlock, smem, s>>>(list.p, nlong, S, A.rp, A.ci, A.v, B.rp, B.ci, B.v,
                                                          cnt.p, nullptr, nullptr, nullptr);
+        HAMLSS_LAUNCH_CHECK();
+    }
+    if (nwarp) {
+        const int gb = merge_grid(ctx, k_spgemm_warp<false>, wsmem, nwarp);
+        k_spgemm_warp<false><<<gb, 32 * kMergeWarps, wsmem, s>>>(wlist, nwarp, KH, A.rp, A.ci, A.v, B.rp,
+                                                                  B.ci, B.v, cnt.p, nullptr, nullptr, nullptr);
+        HAMLSS_LAUNCH_CHECK();
+    }
+    if (ndense) {
+        const int gb = row_grid(ctx, k_spgemm_dense<false>, dsmem, ndense);
+        k_spgemm_dense<false><<<gb, kRowBlock, dsmem, s>>>(dlist, ndense, B.m, A.rp, A.ci, A.v, B.rp, B.ci,
+                                                           B.v, cnt.p, nullptr, nullptr, nullptr);
         HAMLSS_LAUNCH_CHECK();
     }
     build_csr_counts(ctx, C, A.n, B.m, cnt);
@@ -1157,6 +1391,18 @@ void spgemm(Ctx& ctx, const Csr<double>& A, const Csr<double>& B, DCsr& C) {
         const int gb = row_grid(ctx, k_spgemm_rows<true>, smem, nlong);
         k_spgemm_rows<true><<<gb, kRowBlock, smem, s>>>(list.p, nlong, S, A.rp, A.ci, A.v, B.rp, B.ci, B.v,
                                                         nullptr, C.rp.p, C.ci.p, C.v.p);
+        HAMLSS_LAUNCH_CHECK();
+    }
+    if (nwarp) {
+        const int gb = merge_grid(ctx, k_spgemm_warp<true>, wsmem, nwarp);
+        k_spgemm_warp<true><<<gb, 32 * kMergeWarps, wsmem, s>>>(wlist, nwarp, KH, A.rp, A.ci, A.v, B.rp,
+                                                                 B.ci, B.v, nullptr, C.rp.p, C.ci.p, C.v.p);
+        HAMLSS_LAUNCH_CHECK();
+    }
+    if (ndense) {
+        const int gb = row_grid(ctx, k_spgemm_dense<true>, dsmem, ndense);
+        k_spgemm_dense<true><<<gb, kRowBlock, dsmem, s>>>(dlist, ndense, B.m, A.rp, A.ci, A.v, B.rp, B.ci,
+                                                          B.v, nullptr, C.rp.p, C.ci.p, C.v.p);
         HAMLSS_LAUNCH_CHECK();
     }
 }
@@ -1174,6 +1420,7 @@ std::unique_ptr<Prec> make_amg(Ctx& ctx, hamlss_mat* A, const hamlss_params& p) 
     M->post = p.amg_smooth_post;
     cudaStream_t s = ctx.lane.stream;
     ProfScope ps(ctx.lane, "setup", 0.0);
+    AllocScope scope(s);                 // setup buffers from the stream-ordered pool
     const int max_levels = std::max(1, p.amg_levels);
     {
         auto L0 = std::make_unique<AmgLevel>();
@@ -1186,13 +1433,16 @@ std::unique_ptr<Prec> make_amg(Ctx& ctx, hamlss_mat* A, const hamlss_params& p) 
     // verbose >= 2: per-phase wall times of every level on stderr (SolverParams::verbose)
     const bool trace = p.verbose >= 2;
     auto tick = std::chrono::steady_clock::now();
+    long long alloc0 = alloc_ns().load();
     auto phase = [&](int lv, const char* what) {
         if (!trace) return;
         HAMLSS_CUDA(cudaStreamSynchronize(s));
         auto now = std::chrono::steady_clock::now();
-        std::fprintf(stderr, "[hamlss amg] level %d %-10s %9.3f ms\n", lv, what,
-                     std::chrono::duration<double, std::milli>(now - tick).count());
+        const long long a = alloc_ns().load();
+        std::fprintf(stderr, "[hamlss amg] level %d %-10s %9.3f ms (alloc/free %7.3f ms)\n", lv, what,
+                     std::chrono::duration<double, std::milli>(now - tick).count(), (a - alloc0) * 1e-6);
         tick = now;
+        alloc0 = a;
     };
     for (int lv = 0; lv < max_levels - 1; ++lv) {
         AmgLevel& F = *M->lev.back();
@@ -1202,6 +1452,11 @@ std::unique_ptr<Prec> make_amg(Ctx& ctx, hamlss_mat* A, const hamlss_params& p) 
         int nc = aggregate_device(ctx, Af, p.amg_strong, agg);
         phase(lv, "aggregate");
         if (nc >= Af.n) break;
+        // engine option: a level that barely coarsens becomes the (dense) coarsest one,
+        // when it is small enough for the dense factorisation
+        if (p.amg_stall_ratio > 0.0 && (double)nc > p.amg_stall_ratio * (double)Af.n &&
+            Af.n <= kStallDenseMax)
+            break;
         smooth_prolongation(ctx, Af, agg, nc, M->omega, F.P);
         phase(lv, "prolong");
         transpose(ctx, F.P, F.R);
@@ -1242,6 +1497,18 @@ std::unique_ptr<Prec> make_amg(Ctx& ctx, hamlss_mat* A, const hamlss_params& p) 
         HAMLSS_CUDA(cudaMemsetAsync(M->Md.p, 0, sizeof(double) * (size_t)nc * nc, s));
         if (nc) {
             k_csr_to_dense<<<grid_for(ctx, nc), 256, 0, s>>>(nc, C.rp, C.ci, C.v, M->Md.p);
+            HAMLSS_LAUNCH_CHECK();
+        }
+        if (nc > kBlockedCoarse) {
+            // large coarsest level: blocked LU with partial pivoting + explicit inverse
+            M->coarse_inverse = true;
+            M->Minv.ensure((size_t)nc * nc);
+            dense_lu_inverse(ctx, nc, M->Md.p, M->Minv.p, M->piv.p);
+            M->Md.release();
+            phase(M->levels() - 1, "blocked LU");
+            return M;
+        }
+        if (nc) {
             k_dense_factor<<<1, 256, 0, s>>>(nc, M->Md.p, M->piv.p, M->skip.p);
             HAMLSS_LAUNCH_CHECK();
         }

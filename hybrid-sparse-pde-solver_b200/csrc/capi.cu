@@ -7,6 +7,7 @@
 #include <vector>
 
 #include "batch.cuh"
+#include "dense_lu.cuh"
 #include "krylov.cuh"
 #include "nvml_energy.cuh"
 
@@ -112,6 +113,7 @@ int hamlss_ctx_create(int device, hamlss_ctx** out) {
         auto* c = new hamlss_ctx();
         c->c.device = device;
         HAMLSS_CUDA(cudaDeviceGetAttribute(&c->c.sm_count, cudaDevAttrMultiProcessorCount, device));
+        pool_keep_memory(device);
         lane_init(c->c.lane, c->c.sm_count);
         c->c.lane.prof = &c->c.prof;
         HAMLSS_CUDA(cudaEventCreate(&c->c.ev0));
@@ -126,6 +128,7 @@ int hamlss_ctx_destroy(hamlss_ctx* ctx) {
     return guarded([&]() -> int {
         if (!ctx) return HAMLSS_OK;
         cudaSetDevice(ctx->c.device);
+        blas_destroy(ctx->c.blas);
         lane_destroy(ctx->c.lane);
         for (auto e : ctx->c.prof.ev) cudaEventDestroy(e);
         if (ctx->c.ev0) cudaEventDestroy(ctx->c.ev0);
@@ -819,7 +822,10 @@ int hamlss_batch_autotune(hamlss_ctx* ctx, hamlss_batch* B, const double* b, int
 int hamlss_batch_release(hamlss_batch* B) {
     return guarded([&]() -> int {
         if (!B) return HAMLSS_OK;
-        if (B->ctx) HAMLSS_CUDA(cudaSetDevice(B->ctx->c.device));
+        if (B->ctx) {
+            HAMLSS_CUDA(cudaSetDevice(B->ctx->c.device));
+            cudaStreamSynchronize(B->ctx->c.lane.stream);
+        }
         delete B;
         return HAMLSS_OK;
     });

@@ -3,6 +3,8 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
+#include <chrono>
 #include <cstdint>
 #include <cstdio>
 #include <stdexcept>
@@ -35,18 +37,60 @@ inline void cuda_check(cudaError_t e, const char* what, const char* file, int li
 #define HAMLSS_CUDA(call) ::hamlss::cuda_check((call), #call, __FILE__, __LINE__)
 #define HAMLSS_LAUNCH_CHECK() ::hamlss::cuda_check(cudaGetLastError(), "kernel launch", __FILE__, __LINE__)
 
-// Owning device allocation (cudaMalloc at setup time; the solve loops allocate nothing).
+// Nanoseconds spent in device allocation and release calls, process-wide (the setup trace
+// at verbose >= 2 reports it per phase).
+inline std::atomic<long long>& alloc_ns() {
+    static std::atomic<long long> ns{0};
+    return ns;
+}
+struct AllocTimer {
+    std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+    ~AllocTimer() {
+        alloc_ns() += std::chrono::duration_cast<std::chrono::nanoseconds>(
+                          std::chrono::steady_clock::now() - t0).count();
+    }
+};
+
+// Stream of the enclosing setup scope on this thread (null: none).  Inside a scope, device
+// buffers come from the device's stream-ordered memory pool on that stream, so the many
+// temporaries of a preconditioner setup neither map fresh memory nor synchronise the
+// device when freed (cudaFree does both).
+inline cudaStream_t& alloc_scope_stream() {
+    static thread_local cudaStream_t s = nullptr;
+    return s;
+}
+// Keep freed pool memory cached in the process (once per device).
+void pool_keep_memory(int device);
+
+struct AllocScope {
+    cudaStream_t prev;
+    explicit AllocScope(cudaStream_t s) : prev(alloc_scope_stream()) { alloc_scope_stream() = s; }
+    ~AllocScope() { alloc_scope_stream() = prev; }
+    AllocScope(const AllocScope&) = delete;
+    AllocScope& operator=(const AllocScope&) = delete;
+};
+
+// Owning device allocation (at setup time; the solve loops allocate nothing).  A buffer
+// allocated inside an AllocScope is freed in stream order: on the scope's stream when
+// released inside a scope (temporaries whose kernels may still be queued there), else on
+// the legacy stream -- by then the engine has synchronised the stream that used it (every
+// solve call and every release entry point synchronises its context's stream).
 template <typename T>
 struct DBuf {
     T* p = nullptr;
     size_t n = 0;
+    bool pooled = false;
     DBuf() = default;
     explicit DBuf(size_t count) { alloc(count); }
     DBuf(const DBuf&) = delete;
     DBuf& operator=(const DBuf&) = delete;
-    DBuf(DBuf&& o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
+    DBuf(DBuf&& o) noexcept : p(o.p), n(o.n), pooled(o.pooled) { o.p = nullptr; o.n = 0; o.pooled = false; }
     DBuf& operator=(DBuf&& o) noexcept {
-        if (this != &o) { release(); p = o.p; n = o.n; o.p = nullptr; o.n = 0; }
+        if (this != &o) {
+            release();
+            p = o.p; n = o.n; pooled = o.pooled;
+            o.p = nullptr; o.n = 0; o.pooled = false;
+        }
         return *this;
     }
     ~DBuf() { release(); }
@@ -56,10 +100,31 @@ struct DBuf {
         // pad to a 256-byte multiple plus one line: vector loads and bulk copies may touch
         // the tail of the last row tile
         size_t bytes = ((count * sizeof(T) + 255) / 256 + 1) * 256;
-        HAMLSS_CUDA(cudaMalloc(&p, bytes));
+        AllocTimer at;
+        cudaStream_t s = alloc_scope_stream();
+        if (s) {
+            HAMLSS_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&p), bytes, s));
+            pooled = true;
+        } else {
+            HAMLSS_CUDA(cudaMalloc(&p, bytes));
+            pooled = false;
+        }
     }
     void ensure(size_t count) { if (count > n || !p) alloc(count); }
-    void release() { if (p) { cudaFree(p); p = nullptr; n = 0; } }
+    void release() {
+        if (p) {
+            AllocTimer at;
+            if (pooled) {
+                cudaStream_t s = alloc_scope_stream();
+                cudaFreeAsync(p, s ? s : cudaStreamLegacy);
+            } else {
+                cudaFree(p);
+            }
+            p = nullptr;
+            n = 0;
+            pooled = false;
+        }
+    }
     void zero(cudaStream_t s) { if (p) HAMLSS_CUDA(cudaMemsetAsync(p, 0, n * sizeof(T), s)); }
     void upload(const T* h, size_t count, cudaStream_t s) {
         ensure(count);

@@ -1,0 +1,437 @@
+// dense_lu.cu -- blocked LU with partial pivoting and the explicit inverse, for the
+// coarsest AMG level when it is too large for the one-block elimination in amg.cu.
+//
+// The reference solves its coarsest level by dense Gaussian elimination with partial
+// pivoting (amg.cpp:260-291).  Coarse operators of the smoothed-aggregation hierarchy
+// become dense, and when the hierarchy is cut where coarsening stalls the coarsest level
+// can hold thousands of rows.  Blocked for the GPU (row-major n x n, nb = 64), first
+// without interchanges -- diagonal block in shared memory, L21 and U12 by triangular
+// solves, A22 by DGEMM, no grid-wide synchronisation -- and, if a pivot falls below 1e-10
+// of the largest entry, again with partial pivoting as the reference does:
+//   panel     columns [k0, k0+nb): one cooperative kernel over all SMs, one column at a
+//             time -- pivot search (largest |a_ij|, first index on ties, like the
+//             reference), row swap inside the panel, multipliers l = a_ij * (1/a_jj),
+//             rank-1 update of the panel's remaining columns; two grid barriers a column
+//   swaps     the panel's row interchanges applied to every other column
+//   U12       L11^-1 A12, one thread per column (unit lower triangular solve)
+//   trailing  A22 -= L21 U12, a library DGEMM (cuBLAS)
+// The inverse solves A X = I: X = P I, then L Y = X and U X = Y, blocked the same way
+// (triangular solve of a 64-row block per column, DGEMM update of the rest).
+#include <cooperative_groups.h>
+#include <cublas_v2.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+
+#include "dense_lu.cuh"
+
+namespace cg = cooperative_groups;
+
+namespace hamlss {
+
+namespace {
+
+constexpr int kNb = 64;
+constexpr int kPanelThreads = 256;
+
+__device__ __forceinline__ bool better(double v, int i, double bv, int bi) {
+    return v > bv || (v == bv && i < bi);
+}
+
+// Panel factorisation, cooperative.  Rows [k0, n) go to warps round-robin; lane c holds
+// panel columns c and c + 32 of its row.  cand_v / cand_i: one slot per block.
+__global__ void __launch_bounds__(kPanelThreads)
+k_lu_panel(int n, int k0, int kb, double* M, int* piv, double* cand_v, int* cand_i, int* singular) {
+    cg::grid_group grid = cg::this_grid();
+    __shared__ double prow[kNb], jrow[kNb];
+    __shared__ double wv[kPanelThreads / 32];
+    __shared__ int wi[kPanelThreads / 32];
+    __shared__ int s_p;
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, nwb = blockDim.x >> 5;
+    const int gw = blockIdx.x * nwb + wib, W = gridDim.x * nwb;
+    // candidate for column k0 (before any update of this panel)
+    auto block_candidate = [&](double v, int idx) {
+        for (int o = 16; o > 0; o >>= 1) {
+            const double ov = __shfl_xor_sync(0xffffffffu, v, o);
+            const int oi = __shfl_xor_sync(0xffffffffu, idx, o);
+            if (better(ov, oi, v, idx)) { v = ov; idx = oi; }
+        }
+        if (lane == 0) { wv[wib] = v; wi[wib] = idx; }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double bv = -1.0;
+            int bi = INT_MAX;
+            for (int w = 0; w < nwb; ++w)
+                if (better(wv[w], wi[w], bv, bi)) { bv = wv[w]; bi = wi[w]; }
+            cand_v[blockIdx.x] = bv;
+            cand_i[blockIdx.x] = bi;
+        }
+        __syncthreads();
+    };
+    {
+        double v = -1.0;
+        int idx = INT_MAX;
+        for (int i = k0 + gw; i < n; i += W)
+            if (lane == 0) {
+                const double a = fabs(M[(size_t)i * n + k0]);
+                if (better(a, i, v, idx)) { v = a; idx = i; }
+            }
+        block_candidate(v, idx);
+    }
+    grid.sync();
+    for (int jj = 0; jj < kb; ++jj) {
+        const int j = k0 + jj;
+        // every block reduces the candidates the same way: the same pivot row p (the order
+        // of the reduction does not matter: "better" is a strict total order)
+        if (wib == 0) {
+            double bv = -1.0;
+            int bi = INT_MAX;
+            for (int b = lane; b < (int)gridDim.x; b += 32) {
+                const double v = __ldcg(&cand_v[b]);
+                const int i = __ldcg(&cand_i[b]);
+                if (better(v, i, bv, bi)) { bv = v; bi = i; }
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+                const double ov = __shfl_xor_sync(0xffffffffu, bv, o);
+                const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+                if (better(ov, oi, bv, bi)) { bv = ov; bi = oi; }
+            }
+            if (lane == 0) {
+                s_p = bi;
+                if (blockIdx.x == 0) {
+                    piv[j] = bi;
+                    if (!(bv > 0.0)) *singular = 1;
+                }
+            }
+        }
+        __syncthreads();
+        const int p = s_p;
+        for (int c = threadIdx.x; c < kb; c += blockDim.x) {
+            prow[c] = __ldcg(&M[(size_t)p * n + k0 + c]);
+            jrow[c] = __ldcg(&M[(size_t)j * n + k0 + c]);
+        }
+        __syncthreads();
+        grid.sync();                       // rows j and p read by everyone before writes
+        const double d = prow[jj];
+        const double inv = (d != 0.0) ? 1.0 / d : 0.0;
+        double v = -1.0;
+        int idx = INT_MAX;
+        for (int i = k0 + gw; i < n; i += W) {
+            if (i < j) continue;
+            double* row = M + (size_t)i * n + k0;
+            const int c0 = lane, c1 = lane + 32;
+            if (i == j) {
+                if (c0 < kb) row[c0] = prow[c0];
+                if (c1 < kb) row[c1] = prow[c1];
+                continue;
+            }
+            double r0 = 0.0, r1 = 0.0;
+            if (i == p) {
+                r0 = c0 < kb ? jrow[c0] : 0.0;
+                r1 = c1 < kb ? jrow[c1] : 0.0;
+            } else {
+                r0 = c0 < kb ? row[c0] : 0.0;
+                r1 = c1 < kb ? row[c1] : 0.0;
+            }
+            // multiplier l = a_ij * (1/a_jj), then a_ic -= l * a_pc for c > j
+            const double aij = __shfl_sync(0xffffffffu, jj < 32 ? r0 : r1, jj & 31);
+            const double l = __dmul_rn(aij, inv);
+            if (c0 < kb) {
+                if (c0 == jj) r0 = l;
+                else if (c0 > jj) r0 = __dsub_rn(r0, __dmul_rn(l, prow[c0]));
+                row[c0] = r0;
+            }
+            if (c1 < kb) {
+                if (c1 == jj) r1 = l;
+                else if (c1 > jj) r1 = __dsub_rn(r1, __dmul_rn(l, prow[c1]));
+                row[c1] = r1;
+            }
+            // candidate for the next column (j + 1) from the updated row
+            if (jj + 1 < kb) {
+                const int nc = jj + 1;
+                const double a = fabs(__shfl_sync(0xffffffffu, nc < 32 ? r0 : r1, nc & 31));
+                if (better(a, i, v, idx)) { v = a; idx = i; }
+            }
+        }
+        if (jj + 1 < kb) block_candidate(v, idx);
+        grid.sync();
+    }
+}
+
+// ------------------------------------------------------------ without pivoting
+// Diagonal block A11 (rows / columns [k0, k0+kb)) factored in shared memory by one block:
+// l = a_rj * (1/a_jj), a_rc -= l * a_jc.  *tiny is set when a pivot's magnitude falls
+// below `floor` (the caller then redoes the whole factorisation with partial pivoting).
+__global__ void k_lu_diag_nopiv(int n, int k0, int kb, double* M, double floor, int* tiny) {
+    __shared__ double a[kNb][kNb + 1];
+    for (int t = threadIdx.x; t < kb * kb; t += blockDim.x) {
+        const int r = t / kb, c = t - r * kb;
+        a[r][c] = M[(size_t)(k0 + r) * n + k0 + c];
+    }
+    __syncthreads();
+    for (int j = 0; j < kb; ++j) {
+        const double d = a[j][j];
+        if (threadIdx.x == 0 && !(fabs(d) > floor)) *tiny = 1;
+        const double inv = (d != 0.0) ? 1.0 / d : 0.0;
+        __syncthreads();
+        for (int t = threadIdx.x; t < (kb - j - 1) * (kb - j); t += blockDim.x) {
+            const int r = j + 1 + t / (kb - j), c = j + t % (kb - j);
+            const double l = __dmul_rn(a[r][j], inv);
+            if (c == j) continue;
+            a[r][c] = __dsub_rn(a[r][c], __dmul_rn(l, a[j][c]));
+        }
+        __syncthreads();
+        for (int r = j + 1 + threadIdx.x; r < kb; r += blockDim.x) a[r][j] = __dmul_rn(a[r][j], inv);
+        __syncthreads();
+    }
+    for (int t = threadIdx.x; t < kb * kb; t += blockDim.x) {
+        const int r = t / kb, c = t - r * kb;
+        M[(size_t)(k0 + r) * n + k0 + c] = a[r][c];
+    }
+}
+
+// L21 = A21 U11^-1 for rows [k0+kb, n), one thread per row (U11 in shared memory).
+__global__ void k_lu_l21(int n, int k0, int kb, double* M) {
+    __shared__ double u[kNb][kNb + 1];
+    for (int t = threadIdx.x; t < kb * kb; t += blockDim.x) {
+        const int r = t / kb, c = t - r * kb;
+        u[r][c] = M[(size_t)(k0 + r) * n + k0 + c];
+    }
+    __syncthreads();
+    for (int r = k0 + kb + blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+        double* row = M + (size_t)r * n + k0;
+        for (int j = 0; j < kb; ++j) {
+            double acc = row[j];
+            for (int q = 0; q < j; ++q) acc = __dsub_rn(acc, __dmul_rn(row[q], u[q][j]));
+            const double d = u[j][j];
+            row[j] = __dmul_rn(acc, (d != 0.0) ? 1.0 / d : 0.0);
+        }
+    }
+}
+
+__global__ void k_abs_max(long long count, const double* __restrict__ a, unsigned long long* out) {
+    double m = 0.0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < count;
+         i += (long long)gridDim.x * blockDim.x)
+        m = fmax(m, fabs(a[i]));
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    // non-negative doubles order like their bit patterns
+    if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
+}
+
+// Apply the panel's interchanges (rows k0 + jj <-> piv[k0 + jj], in order) to the columns
+// outside the panel.
+__global__ void k_lu_swap(int n, int k0, int kb, double* M, const int* __restrict__ piv) {
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+        if (c >= k0 && c < k0 + kb) continue;
+        for (int jj = 0; jj < kb; ++jj) {
+            const int j = k0 + jj, p = piv[j];
+            if (p == j) continue;
+            const double t = M[(size_t)j * n + c];
+            M[(size_t)j * n + c] = M[(size_t)p * n + c];
+            M[(size_t)p * n + c] = t;
+        }
+    }
+}
+
+// B[r][c] for r in [k0, k0+kb): B := L11^-1 B (unit lower L11 = L[k0.., k0..]), columns
+// [c0, c1) of B, one thread per column.  L and B may be the same matrix.
+__global__ void k_trsm_lower_unit(int n, int k0, int kb, const double* __restrict__ L, int ldl,
+                                  double* B, int ldb, int c0, int c1) {
+    __shared__ double sl[kNb][kNb];
+    for (int t = threadIdx.x; t < kb * kb; t += blockDim.x) {
+        const int r = t / kb, q = t - r * kb;
+        sl[r][q] = L[(size_t)(k0 + r) * ldl + k0 + q];
+    }
+    __syncthreads();
+    for (int c = c0 + blockIdx.x * blockDim.x + threadIdx.x; c < c1; c += gridDim.x * blockDim.x) {
+        for (int r = 1; r < kb; ++r) {
+            double acc = B[(size_t)(k0 + r) * ldb + c];
+            for (int q = 0; q < r; ++q)
+                acc = __dsub_rn(acc, __dmul_rn(sl[r][q], B[(size_t)(k0 + q) * ldb + c]));
+            B[(size_t)(k0 + r) * ldb + c] = acc;
+        }
+    }
+}
+
+// B := U11^-1 B for rows [k0, k0+kb) (upper U11 = U[k0.., k0..] with its diagonal).
+__global__ void k_trsm_upper(int n, int k0, int kb, const double* __restrict__ U, int ldu, double* B,
+                             int ldb, int c0, int c1) {
+    __shared__ double su[kNb][kNb];
+    for (int t = threadIdx.x; t < kb * kb; t += blockDim.x) {
+        const int r = t / kb, q = t - r * kb;
+        su[r][q] = U[(size_t)(k0 + r) * ldu + k0 + q];
+    }
+    __syncthreads();
+    for (int c = c0 + blockIdx.x * blockDim.x + threadIdx.x; c < c1; c += gridDim.x * blockDim.x) {
+        for (int r = kb - 1; r >= 0; --r) {
+            double acc = B[(size_t)(k0 + r) * ldb + c];
+            for (int q = r + 1; q < kb; ++q)
+                acc = __dsub_rn(acc, __dmul_rn(su[r][q], B[(size_t)(k0 + q) * ldb + c]));
+            B[(size_t)(k0 + r) * ldb + c] = acc / su[r][r];
+        }
+    }
+}
+
+// X = P I: the identity with the factorisation's row interchanges applied in order.
+__global__ void k_perm_identity(int n, const int* __restrict__ piv, double* X) {
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+        for (int r = 0; r < n; ++r) X[(size_t)r * n + c] = (r == c) ? 1.0 : 0.0;
+        for (int j = 0; j < n; ++j) {
+            const int p = piv[j];
+            if (p == j) continue;
+            const double t = X[(size_t)j * n + c];
+            X[(size_t)j * n + c] = X[(size_t)p * n + c];
+            X[(size_t)p * n + c] = t;
+        }
+    }
+}
+
+void cublas_check(cublasStatus_t s, const char* what) {
+    if (s != CUBLAS_STATUS_SUCCESS) fail(HAMLSS_ERR_CUDA, std::string("cuBLAS ") + what + " failed");
+}
+
+// Row-major C (m x p, ld n) -= A (m x k, ld n) * B (k x p, ld n).
+void gemm_sub(cublasHandle_t h, int n, int m, int p, int k, const double* A, const double* B, double* C) {
+    if (m <= 0 || p <= 0 || k <= 0) return;
+    const double minus1 = -1.0, one = 1.0;
+    cublas_check(cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, p, m, k, &minus1, B, n, A, n, &one, C, n),
+                 "dgemm");
+}
+
+int col_grid(Ctx& ctx, int cols) {
+    return std::max(1, std::min(ceil_div(cols, 128), ctx.sm_count * 4));
+}
+
+
+__global__ void k_iota(int n, int* piv) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) piv[i] = i;
+}
+
+cublasHandle_t blas_of(Ctx& ctx) {
+    if (!ctx.blas) {
+        cublasHandle_t h = nullptr;
+        cublas_check(cublasCreate(&h), "create");
+        ctx.blas = h;
+    }
+    cublasHandle_t h = static_cast<cublasHandle_t>(ctx.blas);
+    cublas_check(cublasSetStream(h, ctx.lane.stream), "set stream");
+    cublas_check(cublasSetMathMode(h, CUBLAS_DEFAULT_MATH), "math mode");
+    return h;
+}
+
+// Blocked LU without row interchanges; false when a pivot falls below `floor`.
+bool factor_nopivot(Ctx& ctx, cublasHandle_t h, int n, double* M, double floor) {
+    cudaStream_t s = ctx.lane.stream;
+    DBuf<int> tiny(1);
+    tiny.zero(s);
+    for (int k0 = 0; k0 < n; k0 += kNb) {
+        const int kb = std::min(kNb, n - k0);
+        k_lu_diag_nopiv<<<1, 256, 0, s>>>(n, k0, kb, M, floor, tiny.p);
+        HAMLSS_LAUNCH_CHECK();
+        const int rest = n - k0 - kb;
+        if (rest > 0) {
+            k_lu_l21<<<col_grid(ctx, rest), 128, 0, s>>>(n, k0, kb, M);
+            k_trsm_lower_unit<<<col_grid(ctx, rest), 128, 0, s>>>(n, k0, kb, M, n, M, n, k0 + kb, n);
+            HAMLSS_LAUNCH_CHECK();
+            gemm_sub(h, n, rest, rest, kb, M + (size_t)(k0 + kb) * n + k0, M + (size_t)k0 * n + k0 + kb,
+                     M + (size_t)(k0 + kb) * n + k0 + kb);
+        }
+    }
+    int t = 0;
+    tiny.download(&t, 1, s);
+    HAMLSS_CUDA(cudaStreamSynchronize(s));
+    return t == 0;
+}
+
+// Blocked LU with partial pivoting (cooperative panels).
+void factor_pivot(Ctx& ctx, cublasHandle_t h, int n, double* M, int* piv) {
+    cudaStream_t s = ctx.lane.stream;
+    DBuf<double> cand_v(ctx.sm_count);
+    DBuf<int> cand_i(ctx.sm_count), singular(1);
+    singular.zero(s);
+    const int pblocks = ctx.sm_count;               // one block per SM: few candidates
+    const int cg_ = col_grid(ctx, n);
+    for (int k0 = 0; k0 < n; k0 += kNb) {
+        const int kb = std::min(kNb, n - k0);
+        int nn = n, kk0 = k0, kkb = kb;
+        double* Mp = M;
+        int* pp = piv;
+        double* cv = cand_v.p;
+        int* ci = cand_i.p;
+        int* sg = singular.p;
+        void* args[] = {&nn, &kk0, &kkb, &Mp, &pp, &cv, &ci, &sg};
+        HAMLSS_CUDA(cudaLaunchCooperativeKernel((const void*)k_lu_panel, dim3(pblocks), dim3(kPanelThreads),
+                                                args, 0, s));
+        k_lu_swap<<<cg_, 128, 0, s>>>(n, k0, kb, M, piv);
+        HAMLSS_LAUNCH_CHECK();
+        const int rest = n - k0 - kb;
+        if (rest > 0) {
+            k_trsm_lower_unit<<<col_grid(ctx, rest), 128, 0, s>>>(n, k0, kb, M, n, M, n, k0 + kb, n);
+            HAMLSS_LAUNCH_CHECK();
+            gemm_sub(h, n, rest, rest, kb, M + (size_t)(k0 + kb) * n + k0, M + (size_t)k0 * n + k0 + kb,
+                     M + (size_t)(k0 + kb) * n + k0 + kb);
+        }
+    }
+    int sing = 0;
+    singular.download(&sing, 1, s);
+    HAMLSS_CUDA(cudaStreamSynchronize(s));
+    if (sing) fail(HAMLSS_ERR_ZERO_PIVOT, "coarsest AMG level is singular (zero pivot in its dense LU)");
+}
+
+}  // namespace
+
+void dense_lu_inverse(Ctx& ctx, int n, double* M, double* Minv, int* piv) {
+    cudaStream_t s = ctx.lane.stream;
+    if (n <= 0) return;
+    cublasHandle_t h = blas_of(ctx);
+    const int cg_ = col_grid(ctx, n);
+    const size_t bytes = sizeof(double) * (size_t)n * n;
+    // First without interchanges (the coarse operators here are symmetric positive definite
+    // or close to diagonally dominant, where that is stable); if a pivot falls below
+    // 1e-10 of the largest entry, start over with partial pivoting.
+    DBuf<unsigned long long> amax(1);
+    amax.zero(s);
+    k_abs_max<<<col_grid(ctx, (int)std::min<size_t>((size_t)n * n / 8 + 1, 1u << 30)), 128, 0, s>>>(
+        (long long)n * n, M, amax.p);
+    HAMLSS_LAUNCH_CHECK();
+    unsigned long long bits = 0;
+    amax.download(&bits, 1, s);
+    HAMLSS_CUDA(cudaMemcpyAsync(Minv, M, bytes, cudaMemcpyDeviceToDevice, s));   // backup
+    HAMLSS_CUDA(cudaStreamSynchronize(s));
+    double big = 0.0;
+    std::memcpy(&big, &bits, sizeof big);
+    if (factor_nopivot(ctx, h, n, M, 1e-10 * big)) {
+        k_iota<<<cg_, 128, 0, s>>>(n, piv);
+        HAMLSS_LAUNCH_CHECK();
+    } else {
+        HAMLSS_CUDA(cudaMemcpyAsync(M, Minv, bytes, cudaMemcpyDeviceToDevice, s));
+        factor_pivot(ctx, h, n, M, piv);
+    }
+    // X = P I; L Y = X (forward, unit lower); U X = Y (backward)
+    k_perm_identity<<<cg_, 128, 0, s>>>(n, piv, Minv);
+    HAMLSS_LAUNCH_CHECK();
+    for (int k0 = 0; k0 < n; k0 += kNb) {
+        const int kb = std::min(kNb, n - k0);
+        k_trsm_lower_unit<<<cg_, 128, 0, s>>>(n, k0, kb, M, n, Minv, n, 0, n);
+        HAMLSS_LAUNCH_CHECK();
+        const int rest = n - k0 - kb;
+        gemm_sub(h, n, rest, n, kb, M + (size_t)(k0 + kb) * n + k0, Minv + (size_t)k0 * n,
+                 Minv + (size_t)(k0 + kb) * n);
+    }
+    const int last = ((n - 1) / kNb) * kNb;
+    for (int k0 = last; k0 >= 0; k0 -= kNb) {
+        const int kb = std::min(kNb, n - k0);
+        k_trsm_upper<<<cg_, 128, 0, s>>>(n, k0, kb, M, n, Minv, n, 0, n);
+        HAMLSS_LAUNCH_CHECK();
+        gemm_sub(h, n, k0, n, kb, M + k0, Minv + (size_t)k0 * n, Minv);
+    }
+    HAMLSS_CUDA(cudaStreamSynchronize(s));
+}
+
+void blas_destroy(void* h) {
+    if (h) cublasDestroy(static_cast<cublasHandle_t>(h));
+}
+
+}  // namespace hamlss

@@ -1,10 +1,23 @@
 // engine.cu -- context / lane setup, device CSR helpers, Jacobi, residual check.
+#include <mutex>
 #include <cmath>
 #include <cstring>
 
 #include "krylov.cuh"
 
 namespace hamlss {
+
+void pool_keep_memory(int device) {
+    static std::mutex mu;
+    static bool done[64] = {};
+    std::lock_guard<std::mutex> g(mu);
+    if (device < 0 || device >= 64 || done[device]) return;
+    cudaMemPool_t pool;
+    HAMLSS_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
+    uint64_t keep = UINT64_MAX;
+    HAMLSS_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    done[device] = true;
+}
 
 void lane_init(Lane& L, int sm_count) {
     (void)sm_count;

@@ -66,6 +66,7 @@ struct Ctx {
     Profiler prof;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     HBuf<char> host_poll;      // pinned landing zone for polled device state
+    void* blas = nullptr;      // cuBLAS handle, created on first use (dense coarse LU)
     std::mutex mu;
 };
 
@@ -111,6 +112,20 @@ double csr_bytes(const Csr<T>& A) {
     return 4.0 * (A.n + 1) + (4.0 + sizeof(T)) * (double)A.nnz;
 }
 
+// Lanes per row of an SpMV: 1 (the 32-row tiles, the reference's summation order) for FP64
+// operands and for short rows; for FP32 operands a group sized to the average row length
+// (the mixed-precision inner solves and V-cycles carry no bit-exactness requirement).
+template <typename T>
+int spmv_group_size(const Csr<T>& A) {
+    if (sizeof(T) != sizeof(float) || A.n == 0) return 1;
+    const double avg = (double)A.nnz / A.n;
+    if (avg < 8.0) return 1;
+    if (avg < 16.0) return 4;
+    if (avg < 32.0) return 8;
+    if (avg < 64.0) return 16;
+    return 32;
+}
+
 template <typename T, int NRED, typename XOp, typename Epi, typename Fin = NoFin>
 void launch_spmv(int sm_count, const Lane& L, const Csr<T>& A, const XOp& xop, const Epi& epi,
                  const Fin& fin = Fin{}, const int* gate = nullptr, const char* name = "spmv",
@@ -119,9 +134,11 @@ void launch_spmv(int sm_count, const Lane& L, const Csr<T>& A, const XOp& xop, c
     auto kern = k_spmv<T, NRED, XOp, Epi, Fin>;
     // thread-safe one-time initialisation (contexts may be driven from several threads)
     static const int per_sm = std::min(occupancy_blocks(kern, kSpmvThreads), kMaxBlocksPerSm);
-    const int ntiles = ceil_div(A.n, 32);
-    int blocks = std::max(1, std::min(ceil_div(ntiles, kSpmvWarps), sm_count * per_sm));
-    kern<<<blocks, kSpmvThreads, 0, L.stream>>>(A.n, A.rp, A.ci, A.v, xop, epi, L.red(), fin, gate);
+    const int gsz = spmv_group_size(A);
+    const int rows_per_warp = gsz > 1 ? 32 / gsz : 32;
+    const int nwork = ceil_div(A.n, rows_per_warp);
+    int blocks = std::max(1, std::min(ceil_div(nwork, kSpmvWarps), sm_count * per_sm));
+    kern<<<blocks, kSpmvThreads, 0, L.stream>>>(A.n, A.rp, A.ci, A.v, xop, epi, L.red(), fin, gate, gsz);
     HAMLSS_LAUNCH_CHECK();
 }
 

@@ -211,9 +211,17 @@ void hamlss_server::solve_lane(hamlss_ctx* ctx) {
             rc = hamlss_solve_adaptive(ctx, A, r->b, r->x, HAMLSS_HOST, &r->p, &st, nullptr, 0,
                                        &nlog, &init);
         }
-        // The ladder climbs from the state the features pick; when it fails at the top,
-        // try the rungs below that it skipped (FGMRES + ILU(0), then CG + Jacobi for
-        // symmetric systems with a positive diagonal), each from the original x0.
+        // The ladder climbs from the state the features pick; when it fails at the top (no
+        // convergence, or a preconditioner that could not be set up), try the rungs below
+        // that it skipped (FGMRES + ILU(0), then CG + Jacobi for symmetric systems with a
+        // positive diagonal), each from the original x0.
+        const bool setup_failed = A && (rc == HAMLSS_ERR_NOMEM || rc == HAMLSS_ERR_ZERO_PIVOT ||
+                                        rc == HAMLSS_ERR_TIMEOUT || rc == HAMLSS_ERR_ZERO_DIAG);
+        if (setup_failed) {
+            rc = HAMLSS_OK;
+            st.converged = 0;
+            std::memcpy(r->x, x0.data(), sizeof(double) * r->n);
+        }
         for (int state = init - 1; rc == HAMLSS_OK && !st.converged && state >= 0; --state) {
             if (state == HAMLSS_STATE_EASY && !spd_like(r->n, r->rp, r->ci, r->v)) continue;
             const int kind = state == HAMLSS_STATE_EASY ? HAMLSS_PREC_JACOBI : HAMLSS_PREC_ILU;

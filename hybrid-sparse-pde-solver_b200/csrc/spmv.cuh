@@ -4,7 +4,9 @@
 // row.  Scheduling: one warp owns a tile of 32 consecutive rows; it stages the tile's
 // nonzeros (values + column indices) into shared memory with fully coalesced loads
 // (256 B / 128 B per warp instruction) in chunks of kChunk entries, then lane l sums row
-// tile+l from shared memory in column order.  A persistent grid walks the tiles.
+// tile+l from shared memory in column order.  Tiles of long rows (more than kLongTile
+// nonzeros: the dense-ish coarse AMG operators) skip the staging and each lane reads its
+// own row from global memory.  A persistent grid walks the tiles.
 //
 // Fusion: the kernel is parameterised by
 //   XOp  x(j)            -> value of the multiplied vector at column j (may be computed on
@@ -24,6 +26,7 @@ namespace hamlss {
 constexpr int kSpmvThreads = 256;             // 8 warps per block
 constexpr int kSpmvWarps = kSpmvThreads / 32;
 constexpr int kChunk = 256;                   // staged nonzeros per warp and round
+constexpr int kLongTile = 4 * kChunk;         // tiles with more nonzeros read rows directly
 
 template <typename T>
 __device__ __forceinline__ double mul_add(double acc, T a, double x) {
@@ -47,6 +50,12 @@ __device__ __forceinline__ double warp_tile_rows(int row0, int n, const int* __r
     const int ts = __shfl_sync(0xffffffffu, rs, 0);
     const int te = __shfl_sync(0xffffffffu, re, 31);
     double sum = 0.0;
+    if (te - ts > kLongTile) {
+        // long rows (coarse AMG levels): staging would leave one lane working per chunk, so
+        // every lane walks its own row straight from global memory -- same order, same sum
+        for (int k = rs; k < re; ++k) sum = mul_add<T>(sum, __ldg(&v[k]), x(__ldg(&ci[k])));
+        return sum;
+    }
     for (int base = ts; base < te; base += kChunk) {
         const int cnt = min(kChunk, te - base);
 #pragma unroll 4
@@ -69,10 +78,13 @@ struct NoFin {
 
 // gate: when non-null and *gate != 0 the whole launch is a no-op (the solve it belongs
 // to has stopped; the flag is only written by earlier kernels on the same stream).
+// gsz > 1 (FP32 operands only, see spmv_group_size): groups of gsz lanes share a row,
+// stride over its nonzeros and add their partial sums with shuffles -- coalesced loads for
+// rows of 8 and more nonzeros, at the price of the reference's summation order.
 template <typename T, int NRED, typename XOp, typename Epi, typename Fin>
 __global__ void __launch_bounds__(kSpmvThreads)
 k_spmv(int n, const int* __restrict__ rp, const int* __restrict__ ci, const T* __restrict__ v,
-       XOp xop, Epi epi, Reducer red, Fin fin, const int* gate) {
+       XOp xop, Epi epi, Reducer red, Fin fin, const int* gate, int gsz) {
     __shared__ T sv[kSpmvWarps][kChunk];
     __shared__ int sc[kSpmvWarps][kChunk];
     __shared__ double rsh[kSpmvWarps * (NRED > 0 ? NRED : 1)];
@@ -87,11 +99,26 @@ k_spmv(int n, const int* __restrict__ rp, const int* __restrict__ ci, const T* _
     double acc[NRED > 0 ? NRED : 1];
 #pragma unroll
     for (int k = 0; k < (NRED > 0 ? NRED : 1); ++k) acc[k] = 0.0;
-    for (int t = blockIdx.x * kSpmvWarps + wid; t < ntiles; t += gridDim.x * kSpmvWarps) {
-        const int row0 = t << 5;
-        double ax = warp_tile_rows<T>(row0, n, rp, ci, v, xop_l, sv[wid], sc[wid]);
-        const int row = row0 + lane;
-        if (row < n) epi_l(row, ax, acc);
+    if (gsz > 1) {
+        const int per_warp = 32 / gsz, sub = lane / gsz, gl = lane - sub * gsz;
+        const int stride = gridDim.x * kSpmvWarps * per_warp;
+        for (int base = (blockIdx.x * kSpmvWarps + wid) * per_warp; base < n; base += stride) {
+            const int row = base + sub;
+            double sum = 0.0;
+            if (row < n) {
+                const int rs = __ldg(&rp[row]), re = __ldg(&rp[row + 1]);
+                for (int k = rs + gl; k < re; k += gsz) sum = mul_add<T>(sum, __ldg(&v[k]), xop_l(__ldg(&ci[k])));
+            }
+            for (int o = gsz >> 1; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+            if (row < n && gl == 0) epi_l(row, sum, acc);
+        }
+    } else {
+        for (int t = blockIdx.x * kSpmvWarps + wid; t < ntiles; t += gridDim.x * kSpmvWarps) {
+            const int row0 = t << 5;
+            double ax = warp_tile_rows<T>(row0, n, rp, ci, v, xop_l, sv[wid], sc[wid]);
+            const int row = row0 + lane;
+            if (row < n) epi_l(row, ax, acc);
+        }
     }
     if constexpr (NRED > 0) {
         double tot[NRED];

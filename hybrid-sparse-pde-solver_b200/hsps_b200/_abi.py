@@ -68,6 +68,7 @@ class Params(C.Structure):
         ("jacobi_omega", C.c_double),
         ("ladder_mode", C.c_int32),
         ("check_every", C.c_int32),
+        ("amg_stall_ratio", C.c_double),
     ]
 
 
@@ -80,7 +81,7 @@ def default_params(**over) -> Params:
         sstep_cond_tol=1e12, async_enabled=0, async_max_stale=3, fill_per_row=0,
         block_size=1, record_hw_energy=0, precision=FP64, ir_inner_tol=1e-5,
         ir_max_outer=30, amg_omega=0.67, amg_coarse_limit=50, jacobi_omega=1.0,
-        ladder_mode=0, check_every=8,
+        ladder_mode=0, check_every=8, amg_stall_ratio=0.0,
     )
     for k, v in over.items():
         if not hasattr(p, k):

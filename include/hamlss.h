@@ -99,6 +99,9 @@ typedef struct hamlss_params {
     int32_t ladder_mode;      /* 0: escalate when an attempt exhausts max_iter (reference)   */
                               /* 1: also escalate on the device-side stall / budget checks   */
     int32_t check_every;      /* iterations between device->host convergence polls (8)      */
+    double  amg_stall_ratio;  /* 0: coarsen until amg_coarse_limit / amg_levels / no progress */
+                              /* (reference); r in (0,1): also stop when n_c > r * n_f, the  */
+                              /* coarsening having stalled, and solve that level densely     */
 } hamlss_params;
 
 /* ----------------------------------------------------------------- statistics

@@ -180,3 +180,76 @@ def test_amg_single_level_and_tiny():
     rp, ci, v = A.row_ptr(), A.col_idx(), A.values()
     d[np.repeat(np.arange(25), np.diff(rp)), ci] = v
     assert np.allclose(d @ z, b, atol=1e-12)
+
+
+@pytest.mark.parametrize("kind", ["varkappa", "convdiff"])
+def test_blocked_coarse_lu_inverse(kind):
+    # a one-level hierarchy of 2025 rows (> 1024): the V-cycle is the blocked dense LU's
+    # explicit inverse; compare with numpy's dense solve.  Bound: 1e-10 relative, the
+    # condition numbers here are below 1e4.
+    side = 45
+    if kind == "varkappa":
+        A = P.varkappa_poisson_2d(side, 1.0, 3)
+    else:
+        A = P.convection_diffusion_2d(side, 1.0, *P.convdiff_wind(side, 30.0))
+    n = side * side
+    M = H.AMGPreconditioner()
+    M.set_coarse_limit(3000)
+    M.setup(dev(A))
+    assert M.levels() == 1
+    r = P.rhs(n, 8, -1.0, 1.0)
+    z = M.apply(r)
+    d = np.zeros((n, n))
+    rp, ci, v = A
+    d[np.repeat(np.arange(n), np.diff(rp)), ci] = v
+    want = np.linalg.solve(d, r)
+    assert np.max(np.abs(z - want)) <= 1e-10 * np.max(np.abs(want))
+
+
+def test_stall_ratio_cuts_hierarchy(orc):
+    # amg_stall_ratio: the first level that keeps more than 70% of its rows becomes the
+    # dense coarsest level (here above 1024 rows, so the blocked LU runs); PCG still
+    # converges to the FP64 tolerance, in FP64 and in mixed precision
+    A = P.varkappa_poisson_2d(128, 1.0, 4)
+    n = 128 * 128
+    b = P.rhs(n, 4, -1.0, 1.0)
+    M = dev(A)
+    full = H.AMGPreconditioner(amg_omega=2.0 / 3.0, amg_coarse_limit=512, amg_levels=25)
+    full.setup(M)
+    cut = H.AMGPreconditioner(amg_omega=2.0 / 3.0, amg_coarse_limit=512, amg_levels=25,
+                              amg_stall_ratio=0.7)
+    cut.setup(M)
+    assert cut.levels() <= full.levels()
+    for prec in (0, H._abi.MIXED):
+        p = default_params(tol=1e-10, max_iter=500, amg_omega=2.0 / 3.0, amg_coarse_limit=512,
+                           amg_levels=25, amg_stall_ratio=0.7, precision=prec)
+        s, _ = H.SolverFactory.make("CG", "AMG", M, p)
+        x = np.zeros(n)
+        st = H.SolverStats()
+        assert s.solve(M, b, x, st)
+        assert np.linalg.norm(b - orc.spmv(*A, x)) / np.linalg.norm(b) < 1.5e-10
+
+
+def test_blocked_coarse_lu_pivoting():
+    # rows of a Poisson matrix shifted cyclically: most diagonal entries are zero, so the
+    # blocked LU must fall back to partial pivoting; the one-level V-cycle is then the
+    # explicit inverse, compared with numpy's dense solve to 1e-10 relative
+    side = 45
+    n = side * side
+    rp0, ci0, v0 = P.poisson_2d(side)
+    order = (np.arange(n) + 7) % n
+    lens = np.diff(rp0)[order]
+    rp = np.zeros(n + 1, np.int32)
+    np.cumsum(lens, out=rp[1:])
+    ci = np.concatenate([ci0[rp0[i]:rp0[i + 1]] for i in order]).astype(np.int32)
+    v = np.concatenate([v0[rp0[i]:rp0[i + 1]] for i in order])
+    M = H.AMGPreconditioner()
+    M.set_coarse_limit(3000)
+    M.setup(H.SparseMatrix(n, n, rp, ci, v))
+    assert M.levels() == 1
+    r = P.rhs(n, 9, -1.0, 1.0)
+    z = M.apply(r)
+    d = np.zeros((n, n))
+    d[np.repeat(np.arange(n), np.diff(rp)), ci] = v
+    want = np.linalg.solve(d, r)
+    assert np.max(np.abs(z - want)) <= 1e-10 * np.max(np.abs(want))
