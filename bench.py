@@ -172,15 +172,17 @@ def peaks():
 
 
 def ncu_traffic(kernel_family):
-    """Per-launch DRAM bytes of the dominant kernel from the committed ncu summary."""
+    """DRAM bytes per launch of the family's largest launch, from the committed ncu
+    summary (profiles/traffic.json): (bytes, which launch, its algorithmic bytes)."""
     path = os.path.join(ROOT, "profiles", "traffic.json")
     if not os.path.exists(path):
-        return None
+        return None, None, None
     try:
-        d = json.load(open(path))
-        return d.get(kernel_family, {}).get("dram_bytes_per_launch")
+        d = json.load(open(path)).get(kernel_family, {})
+        return (d.get("dram_bytes_per_launch"), d.get("launch"),
+                d.get("algorithmic_bytes_per_launch"))
     except (ValueError, OSError):
-        return None
+        return None, None, None
 
 
 # ------------------------------------------------------------------ CPU reference
@@ -379,7 +381,7 @@ def run_ours(args, rank, world, local):
     solve_fams = [f for f in fams if f[0] != "setup" and f[3] > 0]
     dom = max(solve_fams, key=lambda f: f[2]) if solve_fams else ("none", 0, 0.0, 0.0)
     achieved = (dom[3] / (dom[2] / 1e3)) / 1e9 if dom[2] > 0 else 0.0
-    traffic = ncu_traffic(dom[0])
+    traffic, traffic_launch, traffic_alg = ncu_traffic(dom[0])
     setup_ms = sum(f[2] for f in fams if f[0] == "setup")
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "traffic": traffic,
@@ -387,6 +389,7 @@ def run_ours(args, rank, world, local):
                 "bytes_per_launch": dom[3] / max(dom[1], 1),
                 "share_of_device_time": round(dom[2] / dev_total, 4),
                 "setup_share_of_device_time": round(setup_ms / dev_total, 4),
+                "traffic_launch": traffic_launch, "traffic_launch_algorithmic_bytes": traffic_alg,
                 "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs, of measured)"
                 if peak_kind == "measured" else "fallback 6.65 TB/s (of fallback)"}
 

@@ -106,10 +106,10 @@ __global__ void k_in_fill(int n, const int* __restrict__ rp, const int* __restri
 // Decide seed / non-seed for every node: seed(i) <=> no seed in IN(i).  IN(i) holds only
 // lower indices, so node i can be decided as soon as its IN nodes are.  Persistent warps
 // claim chunks of 32 consecutive nodes in increasing order (atomic ticket).  For a chunk,
-// the warp first reads the decided status of every IN node outside the chunk, all loads
-// in flight together (waiting for any not yet decided), and notes which IN nodes lie
-// inside the chunk; it then decides the 32 nodes in order from registers alone and
-// publishes them with one store.  Every claimed chunk belongs to a running warp
+// each lane first reads, for its own node, the decided status of the IN nodes outside the
+// chunk (waiting for any not yet decided) and notes which IN nodes lie inside the chunk;
+// the warp then decides the 32 nodes in order from registers alone and publishes them
+// with one store.  Every claimed chunk belongs to a running warp
 // (cooperative launch: all blocks resident) and a chunk only waits on earlier chunks, so
 // the waits end.  Each wait is bounded (about a second): past that the kernel records
 // *err and moves on, and the host reports HAMLSS_ERR_TIMEOUT.
@@ -126,6 +126,7 @@ __device__ __forceinline__ int wait_status(const int* status, int src, int* err)
                 atomicExch(err, 1);
                 return 2;
             }
+            __nanosleep(32);                 // poll gently: the producer needs the memory system
         }
     }
     return st;
@@ -140,23 +141,20 @@ __global__ void k_aggregate_wave(int n, const int* __restrict__ in_rp, const int
         base = __shfl_sync(0xffffffffu, base, 0);
         if (base >= n) break;
         const int cnt = min(32, n - base);
-        // pass 1: outside seeds (bit q of `outside`) and in-chunk IN nodes of node q (`inmask`,
-        // held by lane q)
-        unsigned outside = 0u, inmask = 0u;
-        for (int q = 0; q < cnt; ++q) {
-            const int i = base + q;
+        // pass 1, lane q for node base + q: whether an IN node outside the chunk is a seed
+        // (bit q of `outside`) and which IN nodes lie inside the chunk (`inmask`)
+        unsigned inmask = 0u;
+        bool cap = false;
+        if (lane < cnt) {
+            const int i = base + lane;
             const int s0 = in_rp[i], s1 = in_rp[i + 1];
-            unsigned local_bits = 0u;
-            bool cap = false;
-            for (int k = s0 + lane; k < s1; k += 32) {
+            for (int k = s0; k < s1; ++k) {
                 const int src = in_src[k];
-                if (src >= base) local_bits |= 1u << (src - base);
-                else cap |= wait_status(status, src, err) == 1;
+                if (src >= base) inmask |= 1u << (src - base);
+                else if (!cap) cap = wait_status(status, src, err) == 1;
             }
-            if (__any_sync(0xffffffffu, cap)) outside |= 1u << q;
-            for (int o = 16; o > 0; o >>= 1) local_bits |= __shfl_xor_sync(0xffffffffu, local_bits, o);
-            if (lane == q) inmask = local_bits;
         }
+        const unsigned outside = __ballot_sync(0xffffffffu, cap);
         // pass 2: decide in order (seeds: bit q of `seeds`), registers only
         unsigned seeds = 0u;
         for (int q = 0; q < cnt; ++q) {
@@ -473,6 +471,7 @@ __global__ void k_smooth_p_rows(const int* __restrict__ rows, int nrows, const i
 constexpr int kHashMax = 4096;          // distinct output columns a shared table may hold
 constexpr int kDenseCols = 16384;       // columns a shared dense accumulator may hold
 constexpr int kWarpHeads = 2048;        // merge heads a warp keeps in shared memory
+constexpr int kWarpMergeK = 128;        // long rows with at most this many left entries merge
 constexpr int kMergeWarps = 4;          // warps (rows) per block of k_spgemm_warp
 
 __global__ void k_spgemm_classify(int m, const int* __restrict__ arp, const int* __restrict__ aci,
@@ -488,7 +487,8 @@ __global__ void k_spgemm_classify(int m, const int* __restrict__ arp, const int*
         const long long h = u < bcols ? u : bcols;
         const bool lng = k > kHeads || u > 512;
         int c = 0;
-        if (lng && bcols <= kDenseCols && h > kHashMax / 4) c = 2;
+        if (lng && k <= kWarpMergeK) c = 3;
+        else if (lng && bcols <= kDenseCols && h > kHashMax / 4) c = 2;
         else if (lng && h <= kHashMax) c = 1;
         else if (k > kHeads && k <= kWarpHeads) c = 3;
         cls[i] = c;
@@ -1144,6 +1144,7 @@ Csr<float> AmgPrec::Rmat<float>(int l) { return lev[l]->R.f32(); }
 void AmgPrec::prepare32(Ctx& ctx) {
     if (f32_ready) return;
     cudaStream_t s = ctx.lane.stream;
+    AllocScope scope(s);                 // FP32 copies from the stream-ordered pool
     auto conv = [&](const DBuf<double>& a, DBuf<float>& b, long long n) {
         b.ensure(n);
         if (n) k_d2f<<<grid_for(ctx, n), 256, 0, s>>>(a.p, b.p, n);

@@ -14,6 +14,7 @@ namespace hamlss {
 // bytes it must move.  Used by bench.py for the live roofline figure.
 struct Profiler {
     bool on = false;
+    int depth = 0;            // open ProfScopes on the lane
     std::vector<cudaEvent_t> ev;
     size_t next = 0;
     struct Mark { const char* name; double bytes; size_t e0; };
@@ -49,14 +50,20 @@ struct Lane {
     Reducer red() const { return Reducer{partials.p, ticket.p}; }
 };
 
+// Only the outermost scope on a lane is recorded: a setup phase that launches many
+// kernels (or calls helpers with scopes of their own) counts once, under its own name.
 struct ProfScope {
     const Lane& L;
     long slot;
     const char* name;
     double bytes;
     ProfScope(const Lane& l, const char* nm, double b)
-        : L(l), slot(l.prof ? l.prof->begin(l.stream) : -1), name(nm), bytes(b) {}
-    ~ProfScope() { if (L.prof) L.prof->end(L.stream, slot, name, bytes); }
+        : L(l), slot(l.prof && l.prof->depth++ == 0 ? l.prof->begin(l.stream) : -1), name(nm), bytes(b) {}
+    ~ProfScope() {
+        if (!L.prof) return;
+        L.prof->end(L.stream, slot, name, bytes);
+        --L.prof->depth;
+    }
 };
 
 struct Ctx {

@@ -368,6 +368,7 @@ std::unique_ptr<Prec> make_ilu0(Ctx& ctx, hamlss_mat* A) {
     P->n = n;
     if (A->A.n != A->A.m) fail(HAMLSS_ERR_SIZE, "ILU needs a square matrix");
     cudaStream_t s = ctx.lane.stream;
+    AllocScope scope(s);                 // setup buffers from the stream-ordered pool
     const int g = std::max(1, std::min(ceil_div(n, 256), ctx.sm_count * 8));
     const int* rp = A->A.rp.p;
     const int* ci = A->A.ci.p;
