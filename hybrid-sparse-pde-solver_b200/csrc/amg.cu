@@ -48,6 +48,7 @@ constexpr int kLongRow = 32;            // rows longer than this are given a who
 constexpr int kSortMax = 8192;          // largest shared-memory sort (u64 keys)
 constexpr int kBlockedCoarse = 1024;    // coarsest levels above this use the blocked LU
 constexpr int kStallDenseMax = 8192;    // largest level the stall rule makes the coarsest
+constexpr int kMaxLevels = 64;          // hierarchy depth cap (amg_levels above it is clamped)
 
 // Rows that the block-per-row kernels (smoothed P, transpose sort) take.
 __host__ __device__ __forceinline__ bool smooth_row_on_block(int len) {
@@ -960,6 +961,19 @@ struct EpiProlong {
     }
 };
 
+// x_out = x_in + P e (prolongation and correction into the other Jacobi buffer)
+template <typename T>
+struct EpiProlongTo {
+    const T* xin;
+    T* xout;
+    HAMLSS_NO_LOAD
+    template <int NV>
+    __device__ __forceinline__ void operator()(int i, double ax, double (&)[NV]) const {
+        if constexpr (sizeof(T) == 8) xout[i] = __dadd_rn((double)xin[i], ax);
+        else xout[i] = (T)((double)xin[i] + ax);
+    }
+};
+
 template <typename T>
 struct BodyFirstSmooth {
     const T* b;
@@ -1051,7 +1065,10 @@ struct AmgPrec : Prec {
             coarse_solve<T>(ctx, L, rhs0, z, gate);
             return;
         }
-        // level 0: first pre-smoothing sweep from 0 (fused when pre >= 1)
+        // Jacobi sweeps alternate between a level's x and x2 buffers (no copies); cur[l] is
+        // the buffer that holds level l's iterate.  With the usual pre = post = 2 every level
+        // ends in its own x, else one copy puts level 0's result in z.
+        T* cur[kMaxLevels];
         for (int l = 0; l < nl - 1; ++l) {
             LevelVecs<T> V = vecs<T>(l);
             const T* b = l == 0 ? rhs0 : V.b;
@@ -1066,12 +1083,15 @@ struct AmgPrec : Prec {
             } else if (l == 0) {
                 HAMLSS_CUDA(cudaMemsetAsync(x, 0, sizeof(T) * n, L.stream));
             }
+            T* c = x;
             for (int s = done_sweeps; s < pre; ++s) {
-                launch_spmv<T, 0>(sm, L, A, XVec<T>{x}, EpiSmooth<T>{b, x, V.x2, V.dinv, om}, NoFin{}, gate,
+                T* o = (c == x) ? V.x2 : x;
+                launch_spmv<T, 0>(sm, L, A, XVec<T>{c}, EpiSmooth<T>{b, c, o, V.dinv, om}, NoFin{}, gate,
                                   "amg_smooth", 4.0 * w * n);
-                launch_vec<0>(sm, L, n, BodyCopy<T>{V.x2, x}, NoFin{}, gate, "vec", 2.0 * w * n);
+                c = o;
             }
-            launch_spmv<T, 0>(sm, L, A, XVec<T>{x}, EpiResid<T>{b, V.r}, NoFin{}, gate, "amg_resid",
+            cur[l] = c;
+            launch_spmv<T, 0>(sm, L, A, XVec<T>{c}, EpiResid<T>{b, V.r}, NoFin{}, gate, "amg_resid",
                               3.0 * w * n);
             LevelVecs<T> C = vecs<T>(l + 1);
             const bool coarse_smooth = (l + 1 < nl - 1) && pre >= 1;
@@ -1083,6 +1103,7 @@ struct AmgPrec : Prec {
         {
             LevelVecs<T> C = vecs<T>(nl - 1);
             coarse_solve<T>(ctx, L, C.b, C.x, gate);
+            cur[nl - 1] = C.x;
         }
         for (int l = nl - 2; l >= 0; --l) {
             LevelVecs<T> V = vecs<T>(l);
@@ -1090,20 +1111,27 @@ struct AmgPrec : Prec {
             T* x = l == 0 ? z : V.x;
             const int n = lev[l]->n;
             Csr<T> A = Amat<T>(ctx, l);
-            LevelVecs<T> C = vecs<T>(l + 1);
-            launch_spmv<T, 0>(sm, L, Pmat<T>(l), XVec<T>{C.x}, EpiProlong<T>{x}, NoFin{}, gate,
+            T* c = cur[l];
+            T* o = (c == x) ? V.x2 : x;
+            // prolongation + correction into the other buffer: o = c + P e
+            launch_spmv<T, 0>(sm, L, Pmat<T>(l), XVec<T>{cur[l + 1]}, EpiProlongTo<T>{c, o}, NoFin{}, gate,
                               "amg_prolong", w * lev[l + 1]->n + 2.0 * w * n);
+            c = o;
             for (int s = 0; s < post; ++s) {
                 const bool last = (l == 0 && s == post - 1);
+                o = (c == x) ? V.x2 : x;
                 if (last && with_dot) {
-                    launch_spmv<T, 1>(sm, L, A, XVec<T>{x}, EpiSmoothDot<T>{EpiSmooth<T>{b, x, V.x2, V.dinv, om}},
+                    launch_spmv<T, 1>(sm, L, A, XVec<T>{c}, EpiSmoothDot<T>{EpiSmooth<T>{b, c, o, V.dinv, om}},
                                       fin, gate, "amg_smooth", 4.0 * w * n);
                 } else {
-                    launch_spmv<T, 0>(sm, L, A, XVec<T>{x}, EpiSmooth<T>{b, x, V.x2, V.dinv, om}, NoFin{}, gate,
+                    launch_spmv<T, 0>(sm, L, A, XVec<T>{c}, EpiSmooth<T>{b, c, o, V.dinv, om}, NoFin{}, gate,
                                       "amg_smooth", 4.0 * w * n);
                 }
-                launch_vec<0>(sm, L, n, BodyCopy<T>{V.x2, x}, NoFin{}, gate, "vec", 2.0 * w * n);
+                c = o;
             }
+            if (c != x && l == 0)
+                launch_vec<0>(sm, L, n, BodyCopy<T>{c, x}, NoFin{}, gate, "vec", 2.0 * w * n);
+            cur[l] = c;
         }
     }
 
@@ -1422,7 +1450,7 @@ std::unique_ptr<Prec> make_amg(Ctx& ctx, hamlss_mat* A, const hamlss_params& p) 
     cudaStream_t s = ctx.lane.stream;
     ProfScope ps(ctx.lane, "setup", 0.0);
     AllocScope scope(s);                 // setup buffers from the stream-ordered pool
-    const int max_levels = std::max(1, p.amg_levels);
+    const int max_levels = std::min(kMaxLevels, std::max(1, p.amg_levels));
     {
         auto L0 = std::make_unique<AmgLevel>();
         L0->n = A->A.n;

@@ -667,7 +667,9 @@ int hamlss_solve_adaptive(hamlss_ctx* ctx, const hamlss_mat* A, const double* b,
             HAMLSS_CUDA(cudaStreamSynchronize(s));
             double setup = now_s() - t0;
             LadderCfg lad;
-            lad.on = p.ladder_mode == 1 && state != HAMLSS_STATE_HARD;
+            // mode 1: the device-side checks escalate the lower rungs; mode 2: they also end
+            // the top rung early on a stall or divergence (its caller then decides)
+            lad.on = (p.ladder_mode == 1 && state != HAMLSS_STATE_HARD) || p.ladder_mode == 2;
             lad.state = state;
             lad.window = p.stall_window;
             lad.threshold = p.stall_threshold;

@@ -1,12 +1,12 @@
 // spmv.cuh -- the CSR SpMV kernel template every solver kernel is built from.
 //
 // Layout: CSR, int32 row_ptr / col_idx, values in T (double or float), columns sorted per
-// row.  Scheduling: one warp owns a tile of 32 consecutive rows; it stages the tile's
-// nonzeros (values + column indices) into shared memory with fully coalesced loads
-// (256 B / 128 B per warp instruction) in chunks of kChunk entries, then lane l sums row
-// tile+l from shared memory in column order.  Tiles of long rows (more than kLongTile
-// nonzeros: the dense-ish coarse AMG operators) skip the staging and each lane reads its
-// own row from global memory.  A persistent grid walks the tiles.
+// row.  Scheduling: one warp owns a tile of 32 consecutive rows and lane l sums row
+// tile+l in column order, reading it straight from global memory four entries at a time
+// (consecutive rows are contiguous, so a warp's loads cover whole cache lines that L1
+// keeps for the next entries; measured 1.5x faster than staging the tile through shared
+// memory on the 5-point operator).  A persistent grid walks the tiles.  For FP32 operands
+// with longer rows, groups of lanes share a row instead (gsz below).
 //
 // Fusion: the kernel is parameterised by
 //   XOp  x(j)            -> value of the multiplied vector at column j (may be computed on
@@ -25,8 +25,6 @@ namespace hamlss {
 
 constexpr int kSpmvThreads = 256;             // 8 warps per block
 constexpr int kSpmvWarps = kSpmvThreads / 32;
-constexpr int kChunk = 256;                   // staged nonzeros per warp and round
-constexpr int kLongTile = 4 * kChunk;         // tiles with more nonzeros read rows directly
 
 template <typename T>
 __device__ __forceinline__ double mul_add(double acc, T a, double x) {
@@ -37,37 +35,25 @@ __device__ __forceinline__ double mul_add<double>(double acc, double a, double x
     return __dadd_rn(acc, __dmul_rn(a, x));
 }
 
-// Sum of row (row0 + lane) of A against x(); every lane of the warp must call it.
+// Sum of row `row` of A against x(), by one lane: the row's loads are issued four at a
+// time, then summed in column order -- the reference's order (sparse_matrix.cpp:80-86).
 template <typename T, typename XOp>
-__device__ __forceinline__ double warp_tile_rows(int row0, int n, const int* __restrict__ rp,
-                                                 const int* __restrict__ ci,
-                                                 const T* __restrict__ v, const XOp& x,
-                                                 T* sv, int* sc) {
-    const int lane = threadIdx.x & 31;
-    const int row = row0 + lane;
-    const int rs = __ldg(&rp[row < n ? row : n]);
-    const int re = row < n ? __ldg(&rp[row + 1]) : rs;
-    const int ts = __shfl_sync(0xffffffffu, rs, 0);
-    const int te = __shfl_sync(0xffffffffu, re, 31);
+__device__ __forceinline__ double lane_row_sum(int row, const int* __restrict__ rp,
+                                               const int* __restrict__ ci, const T* __restrict__ v,
+                                               const XOp& x) {
+    const int rs = __ldg(&rp[row]), re = __ldg(&rp[row + 1]);
     double sum = 0.0;
-    if (te - ts > kLongTile) {
-        // long rows (coarse AMG levels): staging would leave one lane working per chunk, so
-        // every lane walks its own row straight from global memory -- same order, same sum
-        for (int k = rs; k < re; ++k) sum = mul_add<T>(sum, __ldg(&v[k]), x(__ldg(&ci[k])));
-        return sum;
+    int k = rs;
+    for (; k + 4 <= re; k += 4) {
+        const T a0 = __ldg(&v[k]), a1 = __ldg(&v[k + 1]), a2 = __ldg(&v[k + 2]), a3 = __ldg(&v[k + 3]);
+        const int c0 = __ldg(&ci[k]), c1 = __ldg(&ci[k + 1]), c2 = __ldg(&ci[k + 2]), c3 = __ldg(&ci[k + 3]);
+        const double x0 = x(c0), x1 = x(c1), x2 = x(c2), x3 = x(c3);
+        sum = mul_add<T>(sum, a0, x0);
+        sum = mul_add<T>(sum, a1, x1);
+        sum = mul_add<T>(sum, a2, x2);
+        sum = mul_add<T>(sum, a3, x3);
     }
-    for (int base = ts; base < te; base += kChunk) {
-        const int cnt = min(kChunk, te - base);
-#pragma unroll 4
-        for (int k = lane; k < cnt; k += 32) {
-            sv[k] = __ldg(&v[base + k]);
-            sc[k] = __ldg(&ci[base + k]);
-        }
-        __syncwarp();
-        const int lo = max(rs, base), hi = min(re, base + cnt);
-        for (int k = lo; k < hi; ++k) sum = mul_add<T>(sum, sv[k - base], x(sc[k - base]));
-        __syncwarp();
-    }
+    for (; k < re; ++k) sum = mul_add<T>(sum, __ldg(&v[k]), x(__ldg(&ci[k])));
     return sum;
 }
 
@@ -85,8 +71,6 @@ template <typename T, int NRED, typename XOp, typename Epi, typename Fin>
 __global__ void __launch_bounds__(kSpmvThreads)
 k_spmv(int n, const int* __restrict__ rp, const int* __restrict__ ci, const T* __restrict__ v,
        XOp xop, Epi epi, Reducer red, Fin fin, const int* gate, int gsz) {
-    __shared__ T sv[kSpmvWarps][kChunk];
-    __shared__ int sc[kSpmvWarps][kChunk];
     __shared__ double rsh[kSpmvWarps * (NRED > 0 ? NRED : 1)];
     if (gate && *(volatile const int*)gate) return;
     XOp xop_l = xop;
@@ -114,10 +98,8 @@ k_spmv(int n, const int* __restrict__ rp, const int* __restrict__ ci, const T* _
         }
     } else {
         for (int t = blockIdx.x * kSpmvWarps + wid; t < ntiles; t += gridDim.x * kSpmvWarps) {
-            const int row0 = t << 5;
-            double ax = warp_tile_rows<T>(row0, n, rp, ci, v, xop_l, sv[wid], sc[wid]);
-            const int row = row0 + lane;
-            if (row < n) epi_l(row, ax, acc);
+            const int row = (t << 5) + lane;
+            if (row < n) epi_l(row, lane_row_sum<T>(row, rp, ci, v, xop_l), acc);
         }
     }
     if constexpr (NRED > 0) {

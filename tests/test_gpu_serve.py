@@ -39,7 +39,8 @@ def _gpu():
 
 def params(**over):
     kw = dict(tol=TOL, max_iter=4000, restart_size=30, drop_tol=0.0, precision=_abi.MIXED,
-              amg_omega=2.0 / 3.0, amg_coarse_limit=512, amg_levels=25)
+              amg_omega=2.0 / 3.0, amg_coarse_limit=512, amg_levels=25, amg_stall_ratio=0.75,
+              ladder_mode=2)
     kw.update(over)
     return default_params(**kw)
 
@@ -118,7 +119,8 @@ def test_batch_failure_escalates():
     A = P.convection_diffusion_2d(side, 1.0, *P.convdiff_wind(side, 300.0))
     b = P.rhs(side * side, 5)
     with Server(slots=2, batch_max_rows=16384) as srv:
-        x, st = srv.submit(*A, b, params=params(max_iter=3, ir_max_outer=1)).wait(timeout=600)
+        x, st = srv.submit(*A, b, params=params(max_iter=3, ir_max_outer=1,
+                                                amg_stall_ratio=0.0)).wait(timeout=600)
         rep = srv.report()
     assert rep["escalated"] == 1 and rep["coalesced"] == 0, rep
     assert st.state_used == H.STATE_HARD and not st.converged
