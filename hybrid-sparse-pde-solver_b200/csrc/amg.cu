@@ -472,7 +472,7 @@ __global__ void k_smooth_p_rows(const int* __restrict__ rows, int nrows, const i
 constexpr int kHashMax = 4096;          // distinct output columns a shared table may hold
 constexpr int kDenseCols = 16384;       // columns a shared dense accumulator may hold
 constexpr int kWarpHeads = 2048;        // merge heads a warp keeps in shared memory
-constexpr int kWarpMergeK = 128;        // long rows with at most this many left entries merge
+constexpr int kWarpMergeK = 512;        // long rows with at most this many left entries merge
 constexpr int kMergeWarps = 4;          // warps (rows) per block of k_spgemm_warp
 
 __global__ void k_spgemm_classify(int m, const int* __restrict__ arp, const int* __restrict__ aci,
@@ -487,9 +487,13 @@ __global__ void k_spgemm_classify(int m, const int* __restrict__ arp, const int*
         }
         const long long h = u < bcols ? u : bcols;
         const bool lng = k > kHeads || u > 512;
+        // dense accumulation pays one barrier per left entry: worth it when the right rows
+        // are long (>= 64 products a step); the warp merge pays per output column
+        const bool dense_ok = bcols <= kDenseCols && h > kHashMax / 4;
         int c = 0;
-        if (lng && k <= kWarpMergeK) c = 3;
-        else if (lng && bcols <= kDenseCols && h > kHashMax / 4) c = 2;
+        if (lng && dense_ok && u >= 64LL * k) c = 2;
+        else if (lng && k <= kWarpMergeK) c = 3;
+        else if (lng && dense_ok) c = 2;
         else if (lng && h <= kHashMax) c = 1;
         else if (k > kHeads && k <= kWarpHeads) c = 3;
         cls[i] = c;
@@ -526,24 +530,46 @@ __global__ void k_spgemm_warp(const int* __restrict__ rows, int nrows, int KH,
     for (int r = blockIdx.x * (blockDim.x >> 5) + wid; r < nrows; r += nwarps) {
         const int i = rows[r];
         const int s = arp[i], k = arp[i + 1] - s;
+        // lane-local minimum over the lane's own heads (t = lane, lane + 32, ...)
+        int lmin = INT_MAX;
         for (int t = lane; t < k; t += 32) {
             const int j = aci[s + t];
             const int p0 = brp[j], p1 = brp[j + 1];
             pos[t] = p0;
             end[t] = p1;
-            cur[t] = p0 < p1 ? bci[p0] : INT_MAX;
+            const int c = p0 < p1 ? bci[p0] : INT_MAX;
+            cur[t] = c;
+            lmin = min(lmin, c);
         }
         int o = FILL ? crp[i] : 0;
         const int groups = (k + 31) >> 5;
         for (;;) {
-            int m = INT_MAX;
-            for (int t = lane; t < k; t += 32) m = min(m, cur[t]);
+            int m = lmin;
             for (int q = 16; q > 0; q >>= 1) m = min(m, __shfl_xor_sync(0xffffffffu, m, q));
             if (m == INT_MAX) break;
+            // groups (t / 32) that hold a head at column m: every group when there are few,
+            // else only those some lane finds (only lanes whose minimum is m look)
+            unsigned long long gm;
+            if (groups <= 4) {
+                gm = (1ull << groups) - 1ull;
+            } else {
+                unsigned long long mine = 0ull;
+                if (lmin == m)
+                    for (int t = lane, g = 0; t < k; t += 32, ++g)
+                        if (cur[t] == m) mine |= 1ull << g;
+                unsigned lo = (unsigned)mine, hi = (unsigned)(mine >> 32);
+                for (int q = 16; q > 0; q >>= 1) lo |= __shfl_xor_sync(0xffffffffu, lo, q);
+                if (groups > 32)
+                    for (int q = 16; q > 0; q >>= 1) hi |= __shfl_xor_sync(0xffffffffu, hi, q);
+                gm = ((unsigned long long)hi << 32) | lo;
+            }
+            // products in the order of the left row: groups in turn, lanes in order inside
             double sum = 0.0;
-            for (int g = 0; g < groups; ++g) {
+            while (gm) {
+                const int g = __ffsll((long long)gm) - 1;
+                gm &= gm - 1;
                 const int t = (g << 5) + lane;
-                const bool hit = t < k && cur[t] == m;
+                const bool hit = t < k && lmin == m && cur[t] == m;
                 double prod = 0.0;
                 if (hit) {
                     const int p = pos[t];
@@ -557,6 +583,10 @@ __global__ void k_spgemm_warp(const int* __restrict__ rows, int nrows, int KH,
                     sum = __dadd_rn(sum, __shfl_sync(0xffffffffu, prod, l));
                     mask &= mask - 1;
                 }
+            }
+            if (lmin == m) {
+                lmin = INT_MAX;
+                for (int t = lane; t < k; t += 32) lmin = min(lmin, cur[t]);
             }
             if (fabs(sum) > kEps * kEps) {
                 if (FILL && lane == 0) {
