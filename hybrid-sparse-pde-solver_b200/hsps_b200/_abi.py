@@ -254,6 +254,13 @@ def _declare(L: C.CDLL) -> None:
         "hamlss_batch_get_widths": (C.c_int, [P, V]),
         "hamlss_batch_autotune": (C.c_int, [P, P, V, C.c_int, C.c_char_p, V]),
         "hamlss_batch_release": (C.c_int, [P]),
+        "hamlss_mtx_read_header": (C.c_int, [C.c_char_p, pi, pi, pi, C.POINTER(C.c_int64),
+                                             C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+        "hamlss_mtx_read_matrix": (C.c_int, [C.c_char_p, pi, pi, pi, V, V, V]),
+        "hamlss_mtx_read_vector": (C.c_int, [C.c_char_p, I32, V, pi]),
+        "hamlss_mtx_write_vector": (C.c_int, [C.c_char_p, I32, V, C.c_char_p]),
+        "hamlss_mtx_write_matrix": (C.c_int, [C.c_char_p, I32, I32, I32, V, V, V, C.c_char_p]),
+        "hamlss_mat_load_mtx": (C.c_int, [P, C.c_char_p, pp]),
         "hamlss_server_config_default": (None, [C.POINTER(ServerConfig)]),
         "hamlss_server_create": (C.c_int, [C.POINTER(ServerConfig), pp]),
         "hamlss_server_submit": (C.c_int, [P, I32, I32, V, V, V, V, V, C.POINTER(Params),

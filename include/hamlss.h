@@ -363,6 +363,34 @@ int hamlss_server_reset_report(hamlss_server* server);
  * on this server may be in progress or follow. */
 int hamlss_server_destroy(hamlss_server* server);
 
+/* ------------------------------------------------------------- MatrixMarket
+ * The .mtx files that feed the engine; same accepted formats and conversions as the
+ * reference's MatrixMarketIO (include/utils/matrix_market_io.hpp:80-130,
+ * src/utils/matrix_market_io.cpp): coordinate real / integer / pattern matrices,
+ * symmetric and skew-symmetric storage expanded, entries sorted by (row, column) with
+ * duplicates summed (SparseMatrix::from_coo, sparse_matrix.cpp:242-282); array or
+ * coordinate vectors.  Host code; no device involved except in hamlss_mat_load_mtx. */
+enum { HAMLSS_MTX_COORDINATE = 0, HAMLSS_MTX_ARRAY = 1 };
+enum { HAMLSS_MTX_REAL = 0, HAMLSS_MTX_INTEGER = 1, HAMLSS_MTX_COMPLEX = 2, HAMLSS_MTX_PATTERN = 3 };
+enum { HAMLSS_MTX_GENERAL = 0, HAMLSS_MTX_SYMMETRIC = 1, HAMLSS_MTX_SKEW = 2, HAMLSS_MTX_HERMITIAN = 3 };
+/* MatrixMarketIO::read_header: banner and size line; entries = stored entries (array:
+ * rows * cols).  Any output pointer may be NULL. */
+int hamlss_mtx_read_header(const char* path, int32_t* format, int32_t* field, int32_t* symmetry,
+                           int64_t* rows, int64_t* cols, int64_t* entries);
+/* MatrixMarketIO::load_matrix into CSR.  Pass NULL arrays to learn rows / cols / nnz first
+ * (the file is parsed again by the second call). */
+int hamlss_mtx_read_matrix(const char* path, int32_t* rows, int32_t* cols, int32_t* nnz,
+                           int32_t* row_ptr, int32_t* col_idx, double* values);
+/* MatrixMarketIO::load_vector(path, expected_n): *n values (values may be NULL to query). */
+int hamlss_mtx_read_vector(const char* path, int32_t expected_n, double* values, int32_t* n);
+/* MatrixMarketIO::save_vector / save_matrix ("%.15e" values; comment may be NULL). */
+int hamlss_mtx_write_vector(const char* path, int32_t n, const double* values, const char* comment);
+int hamlss_mtx_write_matrix(const char* path, int32_t rows, int32_t cols, int32_t nnz,
+                            const int32_t* row_ptr, const int32_t* col_idx, const double* values,
+                            const char* comment);
+/* Parse a .mtx matrix and upload it to the context's device (hamlss_mat_upload). */
+int hamlss_mat_load_mtx(hamlss_ctx* ctx, const char* path, hamlss_mat** out);
+
 /* ------------------------------------------------------- inspection (parity)
  * Internals that the reference keeps private but that parity is checked on. */
 /* Greedy aggregation of one matrix (amg.cpp:30-67): agg[rows]; returns the count. */

@@ -213,6 +213,27 @@ class Oracle:
         self.L.orc_extract_features(*A.args(), _p(f), C.byref(s))
         return f, s.value
 
+    def mtx_load_matrix(self, path):
+        """MatrixMarketIO::load_matrix: (rows, cols, rp, ci, v), or None on an exception."""
+        r, c, nz = C.c_int32(), C.c_int32(), C.c_int32()
+        p = os.fsencode(path)
+        if self.L.ref_mtx_load_matrix(p, C.byref(r), C.byref(c), C.byref(nz), None, None, None):
+            return None
+        rp = np.empty(r.value + 1, _i32)
+        ci = np.empty(max(nz.value, 1), _i32)
+        v = np.empty(max(nz.value, 1), _f64)
+        self.L.ref_mtx_load_matrix(p, C.byref(r), C.byref(c), C.byref(nz), _p(rp), _p(ci), _p(v))
+        return r.value, c.value, rp, ci[:nz.value], v[:nz.value]
+
+    def mtx_load_vector(self, path, expected_n=0):
+        n = C.c_int32()
+        p = os.fsencode(path)
+        if self.L.ref_mtx_load_vector(p, expected_n, None, C.byref(n)):
+            return None
+        out = np.empty(max(n.value, 1), _f64)
+        self.L.ref_mtx_load_vector(p, expected_n, _p(out), C.byref(n))
+        return out[:n.value]
+
     def solve_adaptive(self, rp, ci, v, b, x0=None, params=None, log_cap=8):
         A = _Csr(rp, ci, v)
         p = params or default_params()
@@ -286,6 +307,8 @@ class Reference:
         L.ref_extract_features.argtypes = [I32, V, V, V, V, pi]
         L.ref_solve_adaptive.argtypes = [I32, V, V, V, V, V, C.POINTER(Params), C.POINTER(Stats),
                                          C.POINTER(Escalation), I32, pi]
+        L.ref_mtx_load_matrix.argtypes = [C.c_char_p, pi, pi, pi, V, V, V]
+        L.ref_mtx_load_vector.argtypes = [C.c_char_p, I32, V, pi]
         self.L = L
         self.set_threads(1 if threads is None else threads)
 
@@ -382,6 +405,27 @@ class Reference:
         s = C.c_int32(0)
         self.L.ref_extract_features(*A.args(), _p(f), C.byref(s))
         return f, s.value
+
+    def mtx_load_matrix(self, path):
+        """MatrixMarketIO::load_matrix: (rows, cols, rp, ci, v), or None on an exception."""
+        r, c, nz = C.c_int32(), C.c_int32(), C.c_int32()
+        p = os.fsencode(path)
+        if self.L.ref_mtx_load_matrix(p, C.byref(r), C.byref(c), C.byref(nz), None, None, None):
+            return None
+        rp = np.empty(r.value + 1, _i32)
+        ci = np.empty(max(nz.value, 1), _i32)
+        v = np.empty(max(nz.value, 1), _f64)
+        self.L.ref_mtx_load_matrix(p, C.byref(r), C.byref(c), C.byref(nz), _p(rp), _p(ci), _p(v))
+        return r.value, c.value, rp, ci[:nz.value], v[:nz.value]
+
+    def mtx_load_vector(self, path, expected_n=0):
+        n = C.c_int32()
+        p = os.fsencode(path)
+        if self.L.ref_mtx_load_vector(p, expected_n, None, C.byref(n)):
+            return None
+        out = np.empty(max(n.value, 1), _f64)
+        self.L.ref_mtx_load_vector(p, expected_n, _p(out), C.byref(n))
+        return out[:n.value]
 
     def solve_adaptive(self, rp, ci, v, b, x0=None, params=None, log_cap=8):
         A = _Csr(rp, ci, v)

@@ -30,6 +30,7 @@
 #include "preconditioners/ilu.hpp"
 #include "preconditioners/amg.hpp"
 #include "adaptive/adaptive_selector.hpp"
+#include "utils/matrix_market_io.hpp"
 #undef private
 #undef protected
 
@@ -275,6 +276,35 @@ int ref_solve_adaptive(int32_t n, const int32_t* rp, const int32_t* ci, const do
         return ok ? 1 : 0;
     } catch (const std::exception& e) {
         return map_error(e);
+    }
+}
+
+// MatrixMarketIO::load_matrix: rows / cols / nnz, then (when the arrays are given) the CSR.
+int ref_mtx_load_matrix(const char* path, int32_t* rows, int32_t* cols, int32_t* nnz, int32_t* rp,
+                        int32_t* ci, double* v) {
+    try {
+        SparseMatrix A = MatrixMarketIO::load_matrix(path);
+        *rows = A.rows();
+        *cols = A.cols();
+        *nnz = A.nnz();
+        if (rp) std::memcpy(rp, A.row_ptr().data(), sizeof(int32_t) * (A.rows() + 1));
+        if (ci && A.nnz()) std::memcpy(ci, A.col_idx().data(), sizeof(int32_t) * A.nnz());
+        if (v && A.nnz()) std::memcpy(v, A.values().data(), sizeof(double) * A.nnz());
+        return 0;
+    } catch (const std::exception& e) {
+        return -1;
+    }
+}
+
+// MatrixMarketIO::load_vector(path, expected_n): *n values (v may be null to query).
+int ref_mtx_load_vector(const char* path, int32_t expected_n, double* v, int32_t* n) {
+    try {
+        Vector x = MatrixMarketIO::load_vector(path, expected_n);
+        *n = static_cast<int32_t>(x.size());
+        if (v && x.size()) std::memcpy(v, x.data(), sizeof(double) * x.size());
+        return 0;
+    } catch (const std::exception& e) {
+        return -1;
     }
 }
 
