@@ -1329,8 +1329,8 @@ bool raise_row_kernel_limits() {
 // Grid of k_spgemm_warp (kMergeWarps rows per block).
 template <typename K>
 int merge_grid(Ctx& ctx, K kernel, size_t smem, int nrows) {
-    static const bool raised = raise_row_kernel_limits();   // once per process, thread-safe
-    (void)raised;
+    static DeviceOnce raised;
+    raised(ctx.device, raise_row_kernel_limits);
     int per = 0;
     HAMLSS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, 32 * kMergeWarps, smem));
     return std::max(1, std::min(ceil_div(nrows, kMergeWarps), ctx.sm_count * std::max(per, 1)));
@@ -1338,8 +1338,8 @@ int merge_grid(Ctx& ctx, K kernel, size_t smem, int nrows) {
 
 template <typename K>
 int row_grid(Ctx& ctx, K kernel, size_t smem, int nrows) {
-    static const bool raised = raise_row_kernel_limits();   // once per process, thread-safe
-    (void)raised;
+    static DeviceOnce raised;
+    raised(ctx.device, raise_row_kernel_limits);
     int per = 0;
     HAMLSS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, kRowBlock, smem));
     return std::max(1, std::min(nrows, ctx.sm_count * std::max(per, 1)));

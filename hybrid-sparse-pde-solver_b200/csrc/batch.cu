@@ -803,7 +803,12 @@ double batch_run(Ctx& ctx, Batch& B, const double* b, double* x, unsigned class_
     a.max_outer = B.params.ir_max_outer;
     a.m = B.m;
     const size_t smem = batch_smem(wmin, B.m);
-    HAMLSS_CUDA(cudaFuncSetAttribute(k_batch_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    static DeviceOnce raised;            // the device's opt-in maximum, so no call lowers it
+    raised(ctx.device, [&] {
+        int optin = 0;
+        HAMLSS_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx.device));
+        HAMLSS_CUDA(cudaFuncSetAttribute(k_batch_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+    });
     int per_sm = occupancy_blocks(k_batch_solve, kBatchThreads, smem);
     const int blocks = std::max(1, per_sm * ctx.sm_count);
     HAMLSS_CUDA(cudaMemsetAsync(B.tickets.p, 0, sizeof(int) * kMaxPhases, s));

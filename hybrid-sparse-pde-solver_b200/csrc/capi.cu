@@ -415,11 +415,7 @@ int hamlss_precond_setup(hamlss_ctx* ctx, const hamlss_mat* A, int kind,
                 P = make_jacobi(ctx->c, Am, p.jacobi_omega);
                 break;
             case HAMLSS_PREC_ILU:
-                if (p.drop_tol > 0.0 || p.fill_per_row > 0)
-                    return set_err(HAMLSS_ERR_INVALID,
-                                   "ILUT (drop_tol > 0 or fill_per_row > 0) is not provided by "
-                                   "the engine; pass drop_tol = 0 for ILU(0)");
-                P = make_ilu0(ctx->c, Am);
+                P = make_ilu(ctx->c, Am, p);
                 break;
             case HAMLSS_PREC_AMG:
                 P = make_amg(ctx->c, Am, p);
@@ -505,6 +501,15 @@ int hamlss_ilu_factors(const hamlss_prec* M, double* lu_values) {
     return guarded([&]() -> int {
         if (!M || !lu_values) return set_err(HAMLSS_ERR_INVALID, "null argument");
         return ilu_copy_factors(M->p.get(), lu_values, M->ctx->c.lane.stream);
+    });
+}
+
+int hamlss_ilu_factor_csr(const hamlss_prec* M, int32_t* nnz, int32_t* row_ptr, int32_t* col_idx,
+                          double* values) {
+    return guarded([&]() -> int {
+        if (!M || !nnz) return set_err(HAMLSS_ERR_INVALID, "null argument");
+        const int rc = ilu_factor_csr(M->p.get(), nnz, row_ptr, col_idx, values, M->ctx->c.lane.stream);
+        return rc ? set_err(rc, "not an ILU preconditioner") : HAMLSS_OK;
     });
 }
 
@@ -658,11 +663,11 @@ int hamlss_solve_adaptive(hamlss_ctx* ctx, const hamlss_mat* A, const double* b,
             std::unique_ptr<Prec> P;
             if (kind == HAMLSS_PREC_JACOBI) P = make_jacobi(c, Am, p.jacobi_omega);
             else if (kind == HAMLSS_PREC_ILU) {
-                if (p.drop_tol > 0.0 || p.fill_per_row > 0)
-                    return set_err(HAMLSS_ERR_INVALID,
-                                   "the MODERATE state asks for ILUT (drop_tol > 0), which the "
-                                   "engine does not provide; pass drop_tol = 0 for ILU(0)");
-                P = make_ilu0(c, Am);
+                // the selector's ILU comes from SolverFactory::make_precond, which sets
+                // drop_tol only (solver_factory.cpp:73-77): fill_per_row stays 0
+                hamlss_params q = p;
+                q.fill_per_row = 0;
+                P = make_ilu(c, Am, q);
             } else P = make_amg(c, Am, p);
             HAMLSS_CUDA(cudaStreamSynchronize(s));
             double setup = now_s() - t0;

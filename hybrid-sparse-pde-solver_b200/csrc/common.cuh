@@ -7,6 +7,7 @@
 #include <chrono>
 #include <cstdint>
 #include <cstdio>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -61,6 +62,13 @@ inline cudaStream_t& alloc_scope_stream() {
 }
 // Keep freed pool memory cached in the process (once per device).
 void pool_keep_memory(int device);
+
+// One-time work per device and process (function attributes are per device), thread-safe.
+struct DeviceOnce {
+    std::once_flag flag[64];
+    template <typename F>
+    void operator()(int device, F&& f) { std::call_once(flag[device & 63], std::forward<F>(f)); }
+};
 
 struct AllocScope {
     cudaStream_t prev;

@@ -18,6 +18,7 @@
 // bit-identical to ILUPreconditioner::apply.
 #include <cooperative_groups.h>
 
+#include <climits>
 #include <cmath>
 #include <cstring>
 
@@ -276,6 +277,330 @@ __global__ void k_ilu_apply_grid(IluLevels<T> F, const T* __restrict__ r, T* y, 
     }
 }
 
+// ------------------------------------------------------------------------- ILUT
+// ILUT(tau, p) (ilu.cpp:94-220) on the device.  The reference eliminates row by row with
+// a dense work row; row i needs the finished U rows of the pivots k < i it eliminates.
+// Here one warp takes one row at a time, rows claimed in increasing order (atomic ticket,
+// cooperative launch: every claimed row belongs to a running warp, so a row only waits on
+// rows that can finish); the work row's touched columns live in the warp's shared memory
+// (column, value, active flag) and the pending pivots in a min-heap, so the columns are
+// visited in the reference's ascending order and every value gets the reference's
+// operations (separate multiply and subtract, the same division, the same drops).  The
+// keep-largest selection is the reference's heap select (make_heap / pop_heap over the
+// row in column order).  Each finished row is published (entries, counts, then a done
+// flag after a fence, then a count of finished rows); a wait on a done flag gives up when
+// no row at all has finished for about a second (the kernel records *err, every warp
+// stops, and the host fails with HAMLSS_ERR_TIMEOUT).
+constexpr int kIlutWarps = 4;
+constexpr int kIlutCap = 512;            // touched columns a work row may hold
+// per warp: columns, values, flags, pending heap, and a row buffer of kIlutCap + 1 entries
+constexpr size_t kIlutWarpBytes = (size_t)kIlutCap * (4 + 8 + 1 + 4) + 16 * ((size_t)kIlutCap + 1);
+constexpr long long kIlutWaitCycles = 2000000000LL;
+
+struct IlutArgs {
+    int n, fill_p;
+    double drop_tol;
+    const int* rp;
+    const int* ci;
+    const double* v;
+    const int* off;                      // capacity offsets: row i's L at off[i], U at off[i] + max(keep, 1)
+    int* ecol;
+    double* eval;
+    int* lcnt;
+    int* ucnt;
+    int* done;
+    int* ticket;
+    int* err;                            // 1 bounded wait ran out, 2 work row overflow
+    int* finished;                       // rows published so far
+};
+
+struct IlutEntry {
+    int col;
+    double val;
+};
+
+__device__ __forceinline__ bool ilut_first(const IlutEntry& a, const IlutEntry& b) {
+    return fabs(a.val) > fabs(b.val);
+}
+
+__device__ void ilut_adjust(IlutEntry* h, int hole, int len, IlutEntry value) {
+    const int top = hole;
+    int child = hole;
+    while (child < (len - 1) / 2) {
+        child = 2 * (child + 1);
+        if (ilut_first(h[child], h[child - 1])) --child;
+        h[hole] = h[child];
+        hole = child;
+    }
+    if ((len & 1) == 0 && child == (len - 2) / 2) {
+        child = 2 * (child + 1);
+        h[hole] = h[child - 1];
+        hole = child - 1;
+    }
+    int parent = (hole - 1) / 2;
+    while (hole > top && ilut_first(h[parent], value)) {
+        h[hole] = h[parent];
+        hole = parent;
+        parent = (hole - 1) / 2;
+    }
+    h[hole] = value;
+}
+
+// keep_largest (ilu.cpp:186-197) on a row in column order: heap select, then column order.
+__device__ void ilut_keep(IlutEntry* row, int* len, int keep) {
+    if (keep <= 0 || *len <= keep) return;
+    for (int parent = (keep - 2) / 2; keep >= 2; --parent) {
+        ilut_adjust(row, parent, keep, row[parent]);
+        if (parent == 0) break;
+    }
+    for (int t = keep; t < *len; ++t)
+        if (ilut_first(row[t], row[0])) {
+            IlutEntry v = row[t];
+            row[t] = row[0];
+            ilut_adjust(row, 0, keep, v);
+        }
+    *len = keep;
+    for (int a = 1; a < keep; ++a) {                 // insertion sort by column
+        IlutEntry x = row[a];
+        int b = a - 1;
+        while (b >= 0 && row[b].col > x.col) { row[b + 1] = row[b]; --b; }
+        row[b + 1] = x;
+    }
+}
+
+__device__ __forceinline__ void heap_push(int* h, int& nh, int x) {
+    int c = nh++;
+    h[c] = x;
+    while (c > 0 && h[(c - 1) / 2] > h[c]) {
+        const int t = h[c];
+        h[c] = h[(c - 1) / 2];
+        h[(c - 1) / 2] = t;
+        c = (c - 1) / 2;
+    }
+}
+
+__device__ __forceinline__ int heap_pop(int* h, int& nh) {
+    const int top = h[0];
+    h[0] = h[--nh];
+    for (int c = 0;;) {
+        const int l = 2 * c + 1, r = l + 1;
+        int m = c;
+        if (l < nh && h[l] < h[m]) m = l;
+        if (r < nh && h[r] < h[m]) m = r;
+        if (m == c) break;
+        const int t = h[c];
+        h[c] = h[m];
+        h[m] = t;
+        c = m;
+    }
+    return top;
+}
+
+__global__ void __launch_bounds__(32 * kIlutWarps) k_ilut_rows(IlutArgs a) {
+    extern __shared__ unsigned char ilut_smem[];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    unsigned char* base = ilut_smem + (size_t)wid * kIlutWarpBytes;
+    int* scol = reinterpret_cast<int*>(base);
+    double* sval = reinterpret_cast<double*>(base + 4 * kIlutCap);
+    unsigned char* sact = base + 12 * kIlutCap;
+    int* heap = reinterpret_cast<int*>(base + 13 * kIlutCap);
+    IlutEntry* row = reinterpret_cast<IlutEntry*>(base + 17 * kIlutCap);
+    for (;;) {
+        int i = 0;
+        if (lane == 0) i = *(volatile int*)a.err ? a.n : atomicAdd(a.ticket, 1);
+        i = __shfl_sync(0xffffffffu, i, 0);
+        if (i >= a.n) break;
+        const int rs = a.rp[i], re = a.rp[i + 1], orig = re - rs;
+        const int keep = orig + a.fill_p;
+        const int half = keep > 1 ? keep : 1;        // capacity of each half of the row
+        int nt = min(orig, kIlutCap);
+        bool overflow = orig > kIlutCap;
+        for (int t = lane; t < nt; t += 32) {
+            scol[t] = a.ci[rs + t];
+            sval[t] = a.v[rs + t];
+            sact[t] = 1;
+        }
+        __syncwarp();
+        double tau = 0.0;
+        int nh = 0;
+        if (lane == 0) {
+            double norm = 0.0;
+            for (int t = 0; t < nt; ++t) norm = __dadd_rn(norm, __dmul_rn(sval[t], sval[t]));
+            tau = a.drop_tol * sqrt(norm);
+            for (int t = 0; t < nt; ++t)
+                if (scol[t] < i) heap_push(heap, nh, scol[t]);
+        }
+        tau = __shfl_sync(0xffffffffu, tau, 0);
+        nh = __shfl_sync(0xffffffffu, nh, 0);
+        while (nh > 0) {
+            int k = 0;
+            if (lane == 0) k = heap_pop(heap, nh);
+            k = __shfl_sync(0xffffffffu, k, 0);
+            nh = __shfl_sync(0xffffffffu, nh, 0);
+            // slot of column k
+            int sk = -1;
+            for (int b0 = 0; b0 < nt && sk < 0; b0 += 32) {
+                const int t = b0 + lane;
+                const unsigned m = __ballot_sync(0xffffffffu, t < nt && scol[t] == k);
+                if (m) sk = b0 + __ffs(m) - 1;
+            }
+            if (sk < 0 || !sact[sk]) continue;
+            const double wk = sval[sk];
+            if (fabs(wk) < tau) {
+                __syncwarp();
+                if (lane == 0) { sval[sk] = 0.0; sact[sk] = 0; }
+                __syncwarp();
+                continue;
+            }
+            // row k must be finished
+            if (lane == 0) {
+                const volatile int* d = a.done + k;
+                if (*d == 0) {
+                    int seen = *(volatile int*)a.finished;
+                    long long t0 = clock64();
+                    while (*d == 0) {
+                        if (*(volatile int*)a.err) break;
+                        const int now = *(volatile int*)a.finished;
+                        if (now != seen) {
+                            seen = now;
+                            t0 = clock64();
+                        } else if (clock64() - t0 > kIlutWaitCycles) {
+                            atomicExch(a.err, 1);
+                            break;
+                        }
+                        __nanosleep(64);
+                    }
+                }
+                __threadfence();
+            }
+            __syncwarp();
+            const int kk = __ldcg(&a.rp[k + 1]) - __ldcg(&a.rp[k]) + a.fill_p;
+            const int us = __ldcg(&a.off[k]) + (kk > 1 ? kk : 1);
+            const int ul = __ldcg(&a.ucnt[k]);
+            const double ukk = (ul > 0 && __ldcg(&a.ecol[us]) == k) ? __ldcg(&a.eval[us]) : 0.0;
+            if (fabs(ukk) < 2.220446049250313e-16) {
+                __syncwarp();
+                if (lane == 0) sact[sk] = 0;
+                __syncwarp();
+                continue;
+            }
+            const double lik = wk / ukk;
+            __syncwarp();
+            if (lane == 0) sval[sk] = lik;
+            __syncwarp();
+            for (int q0 = 0; q0 < ul; q0 += 32) {
+                const int q = q0 + lane;
+                int j = -1;
+                double prod = 0.0;
+                if (q < ul) {
+                    j = __ldcg(&a.ecol[us + q]);
+                    if (j <= k) j = -1;
+                    else prod = __dmul_rn(lik, __ldcg(&a.eval[us + q]));
+                }
+                int slot = -1;
+                if (j >= 0)
+                    for (int t = 0; t < nt; ++t)
+                        if (scol[t] == j) { slot = t; break; }
+                const unsigned need = __ballot_sync(0xffffffffu, j >= 0 && slot < 0);
+                if (j >= 0 && slot < 0) {
+                    slot = nt + __popc(need & ((1u << lane) - 1u));
+                    if (slot < kIlutCap) {
+                        scol[slot] = j;
+                        sval[slot] = 0.0;
+                        sact[slot] = 0;
+                    }
+                }
+                nt += __popc(need);
+                if (nt > kIlutCap) { overflow = true; nt = kIlutCap; }
+                bool push = false;
+                if (j >= 0 && slot < kIlutCap) {
+                    if (!sact[slot] && fabs(prod) >= tau) {
+                        sact[slot] = 1;
+                        push = j < i;
+                    }
+                    sval[slot] = __dsub_rn(sval[slot], prod);
+                }
+                __syncwarp();
+                unsigned pm = __ballot_sync(0xffffffffu, push);
+                while (pm) {
+                    const int l = __ffs(pm) - 1;
+                    const int jj = __shfl_sync(0xffffffffu, j, l);
+                    if (lane == 0) heap_push(heap, nh, jj);
+                    pm &= pm - 1;
+                }
+                nh = __shfl_sync(0xffffffffu, nh, 0);
+                __syncwarp();
+            }
+        }
+        // collect L, the diagonal, U (lane 0) and publish the row
+        if (lane == 0) {
+            int nl = 0;
+            for (int t = 0; t < nt; ++t)
+                if (scol[t] < i && sact[t] && fabs(sval[t]) >= tau) { row[nl].col = scol[t]; row[nl].val = sval[t]; ++nl; }
+            for (int x = 1; x < nl; ++x) {
+                IlutEntry e = row[x];
+                int y = x - 1;
+                while (y >= 0 && row[y].col > e.col) { row[y + 1] = row[y]; --y; }
+                row[y + 1] = e;
+            }
+            ilut_keep(row, &nl, keep);
+            const int o = a.off[i];
+            for (int t = 0; t < nl; ++t) { a.ecol[o + t] = row[t].col; a.eval[o + t] = row[t].val; }
+            double diag = 0.0;
+            for (int t = 0; t < nt; ++t)
+                if (scol[t] == i) { diag = sval[t]; break; }
+            if (fabs(diag) < 2.220446049250313e-16) diag = (diag >= 0 ? 1.0 : -1.0) * 2.220446049250313e-16 * 1e6;
+            int nu = 0;
+            row[nu].col = i; row[nu].val = diag; ++nu;
+            const int first = nu;
+            for (int t = 0; t < nt; ++t)
+                if (scol[t] > i && sact[t] && fabs(sval[t]) >= tau) { row[nu].col = scol[t]; row[nu].val = sval[t]; ++nu; }
+            for (int x = first + 1; x < nu; ++x) {
+                IlutEntry e = row[x];
+                int y = x - 1;
+                while (y >= first && row[y].col > e.col) { row[y + 1] = row[y]; --y; }
+                row[y + 1] = e;
+            }
+            ilut_keep(row, &nu, keep);
+            for (int t = 0; t < nu; ++t) { a.ecol[o + half + t] = row[t].col; a.eval[o + half + t] = row[t].val; }
+            a.lcnt[i] = nl;
+            a.ucnt[i] = nu;
+            if (overflow) atomicExch(a.err, 2);
+            __threadfence();
+            *(volatile int*)(a.done + i) = 1;
+            atomicAdd(a.finished, 1);
+        }
+        __syncwarp();
+    }
+}
+
+// Capacity per row (2 * (row length + fill_p)): L in the first half, U in the second.
+__global__ void k_ilut_caps(int n, const int* __restrict__ rp, int fill_p, int* cap) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int keep = rp[i + 1] - rp[i] + fill_p;
+        cap[i] = 2 * (keep > 1 ? keep : 1);
+    }
+}
+
+__global__ void k_ilut_counts(int n, const int* __restrict__ lcnt, const int* __restrict__ ucnt, int* cnt) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        cnt[i] = lcnt[i] + ucnt[i];
+}
+
+// Compact the capacity layout into the L\U CSR (row: L entries, then U entries).
+__global__ void k_ilut_compact(int n, const int* __restrict__ rp, int fill_p, const int* __restrict__ off,
+                               const int* __restrict__ lcnt, const int* __restrict__ ucnt,
+                               const int* __restrict__ ecol, const double* __restrict__ eval,
+                               const int* __restrict__ frp, int* fci, double* flu) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int keep = rp[i + 1] - rp[i] + fill_p;
+        const int half = keep > 1 ? keep : 1;
+        int o = frp[i];
+        for (int t = 0; t < lcnt[i]; ++t, ++o) { fci[o] = ecol[off[i] + t]; flu[o] = eval[off[i] + t]; }
+        for (int t = 0; t < ucnt[i]; ++t, ++o) { fci[o] = ecol[off[i] + half + t]; flu[o] = eval[off[i] + half + t]; }
+    }
+}
+
 template <typename K>
 int coop_blocks(Ctx& ctx, K kernel, int threads) {
     int per = occupancy_blocks(kernel, threads);
@@ -294,6 +619,11 @@ void coop_launch(Ctx& ctx, K kernel, int blocks, int threads, Args... args) {
 // ---------------------------------------------------------------------- the object
 struct IluPrec : Prec {
     hamlss_mat* A = nullptr;
+    // pattern of the factor: A's for ILU(0); the factor's own (frp, fci) for ILUT
+    const int* prp = nullptr;
+    const int* pci = nullptr;
+    int pnnz = 0;
+    DBuf<int> frp, fci;
     DBuf<int> dpos, lcnt, ucnt, trp, trow, indeg, cnt, levelL, levelU, nlev;
     DBuf<int> ordL, lptrL, ordU, lptrU, Lrp, Lci, Urp, Uci;
     DBuf<double> lu, Lv, Uv, Ud;
@@ -345,8 +675,8 @@ struct IluPrec : Prec {
         Lv32.ensure(nnzL); Uv32.ensure(nnzU); Ud32.ensure(n); y32.ensure(n);
         int g = std::max(1, std::min(ceil_div(n, 256), ctx.sm_count * 8));
         if (n) {
-            k_fill_L<float><<<g, 256, 0, s>>>(n, ordL.p, A->A.rp.p, A->A.ci.p, lu.p, Lrp.p, Lci.p, Lv32.p);
-            k_fill_U<float><<<g, 256, 0, s>>>(n, ordU.p, A->A.rp.p, A->A.ci.p, lu.p, Urp.p, Uci.p, Uv32.p,
+            k_fill_L<float><<<g, 256, 0, s>>>(n, ordL.p, prp, pci, lu.p, Lrp.p, Lci.p, Lv32.p);
+            k_fill_U<float><<<g, 256, 0, s>>>(n, ordU.p, prp, pci, lu.p, Urp.p, Uci.p, Uv32.p,
                                               Ud32.p, nullptr);
             HAMLSS_LAUNCH_CHECK();
         }
@@ -359,6 +689,10 @@ struct IluPrec : Prec {
     bool has32() const override { return true; }
 };
 
+namespace {
+void finish_ilu(Ctx& ctx, IluPrec* P, bool factorise);
+}  // namespace
+
 std::unique_ptr<Prec> make_ilu0(Ctx& ctx, hamlss_mat* A) {
     auto P = std::make_unique<IluPrec>();
     P->kind = HAMLSS_PREC_ILU;
@@ -369,13 +703,111 @@ std::unique_ptr<Prec> make_ilu0(Ctx& ctx, hamlss_mat* A) {
     if (A->A.n != A->A.m) fail(HAMLSS_ERR_SIZE, "ILU needs a square matrix");
     cudaStream_t s = ctx.lane.stream;
     AllocScope scope(s);                 // setup buffers from the stream-ordered pool
-    const int g = std::max(1, std::min(ceil_div(n, 256), ctx.sm_count * 8));
-    const int* rp = A->A.rp.p;
-    const int* ci = A->A.ci.p;
+    P->prp = A->A.rp.p;
+    P->pci = A->A.ci.p;
+    P->pnnz = nnz;
     P->lu.ensure(nnz);
-    P->y.ensure(n);
     if (nnz) HAMLSS_CUDA(cudaMemcpyAsync(P->lu.p, A->A.v.p, sizeof(double) * nnz, cudaMemcpyDeviceToDevice, s));
-    if (n == 0) return P;
+    finish_ilu(ctx, P.get(), true);
+    return P;
+}
+
+std::unique_ptr<Prec> make_ilut(Ctx& ctx, hamlss_mat* A, double drop_tol, int fill_p) {
+    auto P = std::make_unique<IluPrec>();
+    P->kind = HAMLSS_PREC_ILU;
+    P->A = A;
+    const int n = A->A.n;
+    P->n = n;
+    if (A->A.n != A->A.m) fail(HAMLSS_ERR_SIZE, "ILU needs a square matrix");
+    if (fill_p < 0) fail(HAMLSS_ERR_INVALID, "ILUT: fill_per_row must be >= 0");
+    cudaStream_t s = ctx.lane.stream;
+    AllocScope scope(s);
+    const int g = std::max(1, std::min(ceil_div(n, 256), ctx.sm_count * 8));
+    // capacity layout: row i owns 2 * max(row length + fill_p, 1) slots
+    DBuf<int> off(n + 1), lcnt(std::max(n, 1)), ucnt(std::max(n, 1)), done(std::max(n, 1)), flags(3);
+    HAMLSS_CUDA(cudaMemsetAsync(off.p + n, 0, sizeof(int), s));
+    if (n) k_ilut_caps<<<g, 256, 0, s>>>(n, A->A.rp.p, fill_p, off.p);
+    HAMLSS_LAUNCH_CHECK();
+    const long long total = exclusive_scan(ctx, off.p, n + 1);
+    if (total > INT_MAX) fail(HAMLSS_ERR_NOMEM, "ILUT: factor capacity exceeds 2^31 entries");
+    DBuf<int> ecol(std::max<long long>(total, 1));
+    DBuf<double> eval(std::max<long long>(total, 1));
+    lcnt.zero(s);
+    ucnt.zero(s);
+    done.zero(s);
+    flags.zero(s);
+    if (n) {
+        static DeviceOnce raised;
+        raised(ctx.device, [] {
+            HAMLSS_CUDA(cudaFuncSetAttribute(k_ilut_rows, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)(kIlutWarpBytes * kIlutWarps)));
+        });
+        const size_t smem = kIlutWarpBytes * kIlutWarps;
+        int per = 0;
+        HAMLSS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_ilut_rows, 32 * kIlutWarps, smem));
+        const int blocks = std::max(1, std::min(std::max(per, 1) * ctx.sm_count, ceil_div(n, kIlutWarps)));
+        IlutArgs a;
+        a.n = n;
+        a.fill_p = fill_p;
+        a.drop_tol = drop_tol;
+        a.rp = A->A.rp.p;
+        a.ci = A->A.ci.p;
+        a.v = A->A.v.p;
+        a.off = off.p;
+        a.ecol = ecol.p;
+        a.eval = eval.p;
+        a.lcnt = lcnt.p;
+        a.ucnt = ucnt.p;
+        a.done = done.p;
+        a.ticket = flags.p;
+        a.err = flags.p + 1;
+        a.finished = flags.p + 2;
+        void* args[] = {&a};
+        HAMLSS_CUDA(cudaLaunchCooperativeKernel((const void*)k_ilut_rows, dim3(blocks), dim3(32 * kIlutWarps),
+                                                args, smem, s));
+        int h[2] = {0, 0};
+        flags.download(h, 2, s);
+        HAMLSS_CUDA(cudaStreamSynchronize(s));
+        if (h[1] == 1) fail(HAMLSS_ERR_TIMEOUT, "ILUT: a bounded wait for an earlier row ran out");
+        if (h[1] == 2) fail(HAMLSS_ERR_NOMEM, "ILUT: a work row touched more than 512 columns");
+    }
+    // compact into the L\U CSR
+    P->frp.ensure(n + 1);
+    HAMLSS_CUDA(cudaMemsetAsync(P->frp.p + n, 0, sizeof(int), s));
+    if (n) k_ilut_counts<<<g, 256, 0, s>>>(n, lcnt.p, ucnt.p, P->frp.p);
+    HAMLSS_LAUNCH_CHECK();
+    const long long fnnz = exclusive_scan(ctx, P->frp.p, n + 1);
+    P->fci.ensure(std::max<long long>(fnnz, 1));
+    P->lu.ensure(std::max<long long>(fnnz, 1));
+    if (n)
+        k_ilut_compact<<<g, 256, 0, s>>>(n, A->A.rp.p, fill_p, off.p, lcnt.p, ucnt.p, ecol.p, eval.p,
+                                          P->frp.p, P->fci.p, P->lu.p);
+    HAMLSS_LAUNCH_CHECK();
+    P->prp = P->frp.p;
+    P->pci = P->fci.p;
+    P->pnnz = (int)fnnz;
+    finish_ilu(ctx, P.get(), false);
+    return P;
+}
+
+std::unique_ptr<Prec> make_ilu(Ctx& ctx, hamlss_mat* A, const hamlss_params& p) {
+    if (p.drop_tol > 0.0 || p.fill_per_row > 0) return make_ilut(ctx, A, p.drop_tol, p.fill_per_row);
+    return make_ilu0(ctx, A);
+}
+
+namespace {
+// Pattern information, level sets, (for ILU(0)) the factorisation, and the level-ordered
+// L / U copies of an ILU preconditioner whose pattern (prp, pci, pnnz) and values (lu)
+// are set.
+void finish_ilu(Ctx& ctx, IluPrec* P, bool factorise) {
+    const int n = P->n;
+    const int nnz = P->pnnz;
+    cudaStream_t s = ctx.lane.stream;
+    const int g = std::max(1, std::min(ceil_div(n, 256), ctx.sm_count * 8));
+    const int* rp = P->prp;
+    const int* ci = P->pci;
+    P->y.ensure(n);
+    if (n == 0) return;
     P->dpos.ensure(n); P->lcnt.ensure(n); P->ucnt.ensure(n);
     k_row_info<<<g, 256, 0, s>>>(n, rp, ci, P->dpos.p, P->lcnt.p, P->ucnt.p);
     HAMLSS_LAUNCH_CHECK();
@@ -413,8 +845,8 @@ std::unique_ptr<Prec> make_ilu0(Ctx& ctx, hamlss_mat* A) {
         P->nlevU = hl[1];
     }
     P->wide = (double)n / std::max(1, std::min(P->nlevL, P->nlevU)) > 4096.0;
-    // factorisation
-    {
+    // factorisation (ILU(0); ILUT arrives factored)
+    if (factorise) {
         DBuf<int> status(1);
         int init = 0x7fffffff;
         status.upload(&init, 1, s);
@@ -465,8 +897,8 @@ std::unique_ptr<Prec> make_ilu0(Ctx& ctx, hamlss_mat* A) {
     }
     P->trow.release();
     P->indeg.release();
-    return P;
 }
+}  // namespace
 
 // Level sets of the strictly lower and strictly upper dependency DAGs of a square CSR
 // pattern (the definitions make_ilu0 uses), without factorising.  The batched solver
@@ -511,7 +943,18 @@ void pattern_levels(Ctx& ctx, int n, int nnz, const int* rp, const int* ci, DBuf
 int ilu_copy_factors(const Prec* M, double* out, cudaStream_t s) {
     auto* P = dynamic_cast<const IluPrec*>(M);
     if (!P) return HAMLSS_ERR_INVALID;
-    if (P->A->A.nnz) P->lu.download(out, P->A->A.nnz, s);
+    if (P->pnnz) P->lu.download(out, P->pnnz, s);
+    HAMLSS_CUDA(cudaStreamSynchronize(s));
+    return HAMLSS_OK;
+}
+
+int ilu_factor_csr(const Prec* M, int* nnz, int* rp, int* ci, double* v, cudaStream_t s) {
+    auto* P = dynamic_cast<const IluPrec*>(M);
+    if (!P) return HAMLSS_ERR_INVALID;
+    *nnz = P->pnnz;
+    if (rp) HAMLSS_CUDA(cudaMemcpyAsync(rp, P->prp, sizeof(int) * (P->n + 1), cudaMemcpyDeviceToHost, s));
+    if (ci && P->pnnz) HAMLSS_CUDA(cudaMemcpyAsync(ci, P->pci, sizeof(int) * P->pnnz, cudaMemcpyDeviceToHost, s));
+    if (v && P->pnnz) P->lu.download(v, P->pnnz, s);
     HAMLSS_CUDA(cudaStreamSynchronize(s));
     return HAMLSS_OK;
 }

@@ -34,9 +34,16 @@ struct JacobiPrec : Prec {
 
 std::unique_ptr<Prec> make_jacobi(Ctx& ctx, hamlss_mat* A, double omega);
 std::unique_ptr<Prec> make_ilu0(Ctx& ctx, hamlss_mat* A);
+// ILUT(drop_tol, fill_p) (ilu.cpp:94-220) on the device
+std::unique_ptr<Prec> make_ilut(Ctx& ctx, hamlss_mat* A, double drop_tol, int fill_p);
+// ILUPreconditioner::setup's dispatch (ilu.cpp:31-36): ILUT when drop_tol > 0 or
+// fill_per_row > 0, else ILU(0)
+std::unique_ptr<Prec> make_ilu(Ctx& ctx, hamlss_mat* A, const hamlss_params& p);
 std::unique_ptr<Prec> make_amg(Ctx& ctx, hamlss_mat* A, const hamlss_params& p);
 
 int ilu_copy_factors(const Prec* M, double* out, cudaStream_t s);
+// the L\U factor as CSR: *nnz, then rp / ci / v when non-null (host arrays)
+int ilu_factor_csr(const Prec* M, int* nnz, int* rp, int* ci, double* v, cudaStream_t s);
 int amg_num_levels(const Prec* P, int* levels);
 int amg_level_matrix(const Prec* P, int level, int which, int* rows, int* cols, int* nnz, int* rp,
                      int* ci, double* v, cudaStream_t s);

@@ -228,7 +228,9 @@ void hamlss_server::solve_lane(hamlss_ctx* ctx) {
             const int solver = state == HAMLSS_STATE_EASY ? HAMLSS_SOLVER_CG : HAMLSS_SOLVER_FGMRES;
             hamlss_prec* M = nullptr;
             double setup = 0.0;
-            if (hamlss_precond_setup(ctx, A, kind, &r->p, &M, &setup) != HAMLSS_OK) continue;
+            hamlss_params q = r->p;
+            q.fill_per_row = 0;              // the ladder's factory-made ILU (drop_tol only)
+            if (hamlss_precond_setup(ctx, A, kind, &q, &M, &setup) != HAMLSS_OK) continue;
             std::vector<double> x(x0);
             hamlss_stats s2;
             std::memset(&s2, 0, sizeof(s2));

@@ -266,7 +266,8 @@ class JacobiPreconditioner(PreconditionerBase):
 
 
 class ILUPreconditioner(PreconditionerBase):
-    """ILU(0) (ilu.cpp:41-89); drop_tol > 0 (ILUT) is refused like an unknown option."""
+    """ILU(0) (ilu.cpp:41-89), or ILUT(drop_tol, fill_per_row) (ilu.cpp:94-220) when
+    drop_tol > 0 or fill_per_row > 0 -- the dispatch of ilu.cpp:31-36."""
 
     kind, tier = PREC_ILU, "MODERATE"
 
@@ -284,9 +285,23 @@ class ILUPreconditioner(PreconditionerBase):
         return default_params(drop_tol=self.drop_tol, fill_per_row=self.fill_p)
 
     def factors(self):
-        lu = np.empty(self._A.nnz())
+        """Factor values in the factor's pattern (A's for ILU(0))."""
+        nnz = C.c_int32()
+        _check(lib().hamlss_ilu_factor_csr(self.h, C.byref(nnz), None, None, None))
+        lu = np.empty(max(nnz.value, 1))
         _check(lib().hamlss_ilu_factors(self.h, _ptr(lu)))
-        return lu
+        return lu[:nnz.value]
+
+    def factor_csr(self):
+        """(row_ptr, col_idx, values) of the L\\U factor (ilu.cpp's lu_row_ptr_, lu_col_ind_,
+        lu_val_)."""
+        nnz = C.c_int32()
+        _check(lib().hamlss_ilu_factor_csr(self.h, C.byref(nnz), None, None, None))
+        rp = np.empty(self._A.rows() + 1, np.int32)
+        ci = np.empty(max(nnz.value, 1), np.int32)
+        v = np.empty(max(nnz.value, 1))
+        _check(lib().hamlss_ilu_factor_csr(self.h, C.byref(nnz), _ptr(rp), _ptr(ci), _ptr(v)))
+        return rp, ci[:nnz.value], v[:nnz.value]
 
     def level_sets(self, which: int):
         lev = np.empty(self._A.rows(), np.int32)

@@ -246,6 +246,7 @@ def _declare(L: C.CDLL) -> None:
         "hamlss_amg_num_levels": (C.c_int, [P, pi]),
         "hamlss_amg_level_matrix": (C.c_int, [P, I32, I32, pi, pi, pi, V, V, V]),
         "hamlss_ilu_factors": (C.c_int, [P, V]),
+        "hamlss_ilu_factor_csr": (C.c_int, [P, pi, V, V, V]),
         "hamlss_ilu_levels": (C.c_int, [P, I32, V, pi]),
         "hamlss_batch_create": (C.c_int, [P, I32, V, V, V, V, V, V, C.c_int, C.POINTER(Params),
                                           pp]),

@@ -217,8 +217,12 @@ int hamlss_dot_noalloc(int32_t n, const double* x, const double* y, double* resu
  * Replaces SolverFactory::make_precond (solver_factory.cpp:54-97) followed by
  * PreconditionerBase::setup.  kind = HAMLSS_PREC_*; HAMLSS_PREC_NONE yields *out == NULL
  * like the reference's nullptr.  HAMLSS_PREC_ILU with params->drop_tol > 0 or
- * fill_per_row > 0 is ILUT in the reference (ilu.cpp:31-36); the engine implements
- * ILU(0) only and returns HAMLSS_ERR_INVALID for that request. */
+ * fill_per_row > 0 is ILUT(drop_tol, fill_per_row) (ilu.cpp:31-36, 94-220), factored on
+ * the device row by row in the reference's order; else ILU(0) (ilu.cpp:41-89).  An ILUT
+ * work row that touches more than 512 columns is refused with HAMLSS_ERR_NOMEM.
+ * fill_per_row is ILUPreconditioner::set_fill_per_row; SolverFactory::make_precond never
+ * sets it (solver_factory.cpp:73-77), so callers that mirror the factory pass 0, and the
+ * adaptive ladder (hamlss_solve_adaptive, the server) uses 0. */
 int hamlss_precond_setup(hamlss_ctx* ctx, const hamlss_mat* A, int kind,
                          const hamlss_params* params, hamlss_prec** out, double* setup_time_s);
 /* z = M^-1 r.  Replaces PreconditionerBase::apply (preconditioner_base.hpp:32). */
@@ -401,8 +405,14 @@ int hamlss_amg_num_levels(const hamlss_prec* M, int32_t* levels);
 int hamlss_amg_level_matrix(const hamlss_prec* M, int32_t level, int32_t which,
                             int32_t* rows, int32_t* cols, int32_t* nnz,
                             int32_t* row_ptr, int32_t* col_idx, double* values);
-/* ILU(0) factor values in the pattern of A (ilu.cpp:41-89's lu_val_). */
+/* ILU factor values in the factor's pattern (ilu.cpp's lu_val_): A's pattern for ILU(0). */
 int hamlss_ilu_factors(const hamlss_prec* M, double* lu_values);
+/* The L\U factor as CSR (ilu.cpp's lu_row_ptr_ / lu_col_ind_ / lu_val_; for ILUT each row
+ * holds its kept L entries, then its U entries, both by ascending column).  *nnz receives
+ * the entry count; row_ptr[rows + 1], col_idx[nnz], values[nnz] (host) are filled when
+ * non-NULL. */
+int hamlss_ilu_factor_csr(const hamlss_prec* M, int32_t* nnz, int32_t* row_ptr,
+                          int32_t* col_idx, double* values);
 /* Level sets of the lower (which = 0) or upper (which = 1) triangle of an ILU(0)
  * preconditioner: level[rows]; *n_levels their count. */
 int hamlss_ilu_levels(const hamlss_prec* M, int32_t which, int32_t* level, int32_t* n_levels);

@@ -153,6 +153,189 @@ int orc_ilu0_factor(int32_t n, const int32_t* rp, const int32_t* ci, const doubl
     return rc;
 }
 
+/* ===================================================================== ILUT(tau, p) */
+
+static int cmp_i32(const void* a, const void* b);
+
+typedef struct { int32_t col; double val; } ilut_entry;
+
+/* keep_largest (ilu.cpp:186-197): std::partial_sort by |value| (descending), i.e. a heap
+ * select over the row in column order -- a heap of the first `keep` entries whose top is
+ * the smallest magnitude, replaced by every later entry of strictly larger magnitude --
+ * then the kept entries sorted by column.  The heap operations are the standard ones:
+ * sift the hole down to a leaf along the child that comes first, then push the value
+ * back up (the library's make_heap / pop_heap). */
+static int ilut_first(const ilut_entry* a, const ilut_entry* b) {   /* comp(a, b) */
+    return fabs(a->val) > fabs(b->val);
+}
+
+static void ilut_adjust(ilut_entry* h, long hole, long len, ilut_entry value) {
+    const long top = hole;
+    long child = hole;
+    while (child < (len - 1) / 2) {
+        child = 2 * (child + 1);
+        if (ilut_first(&h[child], &h[child - 1])) --child;
+        h[hole] = h[child];
+        hole = child;
+    }
+    if ((len & 1) == 0 && child == (len - 2) / 2) {
+        child = 2 * (child + 1);
+        h[hole] = h[child - 1];
+        hole = child - 1;
+    }
+    long parent = (hole - 1) / 2;
+    while (hole > top && ilut_first(&h[parent], &value)) {
+        h[hole] = h[parent];
+        hole = parent;
+        parent = (hole - 1) / 2;
+    }
+    h[hole] = value;
+}
+
+static int ilut_by_col(const void* a, const void* b) {
+    const ilut_entry* x = (const ilut_entry*)a;
+    const ilut_entry* y = (const ilut_entry*)b;
+    return (x->col > y->col) - (x->col < y->col);
+}
+
+static void ilut_keep_largest(ilut_entry* row, int32_t* len, int32_t keep) {
+    if (keep <= 0 || *len <= keep) return;
+    for (long parent = (keep - 2) / 2; keep >= 2; --parent) {          /* make_heap */
+        ilut_adjust(row, parent, keep, row[parent]);
+        if (parent == 0) break;
+    }
+    for (int32_t i = keep; i < *len; ++i) {                           /* heap select */
+        if (ilut_first(&row[i], &row[0])) {
+            ilut_entry v = row[i];
+            row[i] = row[0];
+            ilut_adjust(row, 0, keep, v);
+        }
+    }
+    *len = keep;
+    qsort(row, (size_t)keep, sizeof(ilut_entry), ilut_by_col);
+}
+
+/* ILUPreconditioner::setup_ilut (ilu.cpp:94-220): row-by-row threshold factorisation with
+ * a dense work row.  The reference scans every k < i and every column to collect the row;
+ * here the work row's touched columns are kept in a list and the pending pivots in a min
+ * heap, which visits the same columns in the same (ascending) order.  Output: the L\U
+ * rows (L entries, then the diagonal and U entries, each in column order).  Call with
+ * out_ci == NULL to learn the entry count. */
+int orc_ilut_factor(int32_t n, const int32_t* rp, const int32_t* ci, const double* v, double drop_tol,
+                    int32_t fill_p, int32_t* out_rp, int32_t* out_ci, double* out_lu, int64_t* nnz_out) {
+    double* w = (double*)calloc((size_t)(n > 0 ? n : 1), sizeof(double));
+    unsigned char* active = (unsigned char*)calloc((size_t)(n > 0 ? n : 1), 1);
+    unsigned char* touched = (unsigned char*)calloc((size_t)(n > 0 ? n : 1), 1);
+    int32_t* tlist = (int32_t*)malloc(sizeof(int32_t) * (size_t)(n > 0 ? n : 1));
+    int32_t* heap = (int32_t*)malloc(sizeof(int32_t) * (size_t)(n > 0 ? n : 1));
+    int32_t* Lstart = (int32_t*)malloc(sizeof(int32_t) * (size_t)(n + 1));
+    int32_t* Ustart = (int32_t*)malloc(sizeof(int32_t) * (size_t)(n + 1));
+    size_t cap = (size_t)(rp[n] > 0 ? rp[n] : 1) * 2 + 16, used = 0;
+    ilut_entry* store = (ilut_entry*)malloc(sizeof(ilut_entry) * cap);
+    ilut_entry* rowbuf = (ilut_entry*)malloc(sizeof(ilut_entry) * (size_t)(n > 0 ? n : 1));
+    int32_t* ulen = (int32_t*)malloc(sizeof(int32_t) * (size_t)(n > 0 ? n : 1));
+    int32_t* llen = (int32_t*)malloc(sizeof(int32_t) * (size_t)(n > 0 ? n : 1));
+    for (int32_t i = 0; i < n; ++i) {
+        int32_t nt = 0, nh = 0;
+        double row_norm = 0.0;
+        for (int32_t p = rp[i]; p < rp[i + 1]; ++p) {
+            const int32_t j = ci[p];
+            w[j] = v[p];
+            active[j] = 1;
+            if (!touched[j]) { touched[j] = 1; tlist[nt++] = j; }
+            row_norm += v[p] * v[p];
+        }
+        row_norm = sqrt(row_norm);
+        const double tau = drop_tol * row_norm;
+        /* pending pivots: active columns < i, smallest first (binary min-heap) */
+#define HEAP_PUSH(x) do { int32_t c_ = nh++; heap[c_] = (x); \
+            while (c_ > 0 && heap[(c_ - 1) / 2] > heap[c_]) { int32_t t_ = heap[c_]; \
+                heap[c_] = heap[(c_ - 1) / 2]; heap[(c_ - 1) / 2] = t_; c_ = (c_ - 1) / 2; } } while (0)
+        for (int32_t t = 0; t < nt; ++t) if (tlist[t] < i) HEAP_PUSH(tlist[t]);
+        while (nh > 0) {
+            const int32_t k = heap[0];
+            heap[0] = heap[--nh];
+            for (int32_t c = 0;;) {
+                int32_t l = 2 * c + 1, r = l + 1, m = c;
+                if (l < nh && heap[l] < heap[m]) m = l;
+                if (r < nh && heap[r] < heap[m]) m = r;
+                if (m == c) break;
+                int32_t t = heap[c]; heap[c] = heap[m]; heap[m] = t; c = m;
+            }
+            if (!active[k]) continue;
+            if (fabs(w[k]) < tau) { w[k] = 0.0; active[k] = 0; continue; }
+            double ukk = 0.0;
+            const ilut_entry* U = store + Ustart[k];
+            for (int32_t q = 0; q < ulen[k]; ++q)
+                if (U[q].col == k) { ukk = U[q].val; break; }
+            if (fabs(ukk) < REAL_EPS) { active[k] = 0; continue; }
+            const double lik = w[k] / ukk;
+            w[k] = lik;
+            for (int32_t q = 0; q < ulen[k]; ++q) {
+                const int32_t j = U[q].col;
+                if (j <= k) continue;
+                const double prod = lik * U[q].val;
+                if (!touched[j]) { touched[j] = 1; tlist[nt++] = j; }
+                if (!active[j] && fabs(prod) >= tau) {
+                    active[j] = 1;
+                    if (j < i) HEAP_PUSH(j);
+                }
+                w[j] -= prod;
+            }
+        }
+#undef HEAP_PUSH
+        /* collect L (j < i), the diagonal, U (j > i) in column order */
+        qsort(tlist, (size_t)nt, sizeof(int32_t), cmp_i32);
+        int32_t nl = 0, nu = 0;
+        ilut_entry* Lrow = rowbuf;
+        for (int32_t t = 0; t < nt && tlist[t] < i; ++t) {
+            const int32_t j = tlist[t];
+            if (active[j] && fabs(w[j]) >= tau) { Lrow[nl].col = j; Lrow[nl].val = w[j]; ++nl; }
+        }
+        const int32_t orig = rp[i + 1] - rp[i];
+        ilut_keep_largest(Lrow, &nl, orig + fill_p);
+        if (used + (size_t)nl + (size_t)nt + 1 > cap) {
+            while (used + (size_t)nl + (size_t)nt + 1 > cap) cap *= 2;
+            store = (ilut_entry*)realloc(store, sizeof(ilut_entry) * cap);
+        }
+        Lstart[i] = (int32_t)used;
+        memcpy(store + used, Lrow, sizeof(ilut_entry) * (size_t)nl);
+        used += (size_t)nl;
+        llen[i] = nl;
+        ilut_entry* Urow = rowbuf;
+        double diag = w[i];
+        if (fabs(diag) < REAL_EPS) diag = (diag >= 0 ? 1.0 : -1.0) * REAL_EPS * 1e6;
+        Urow[nu].col = i; Urow[nu].val = diag; ++nu;
+        for (int32_t t = 0; t < nt; ++t) {
+            const int32_t j = tlist[t];
+            if (j <= i) continue;
+            if (active[j] && fabs(w[j]) >= tau) { Urow[nu].col = j; Urow[nu].val = w[j]; ++nu; }
+        }
+        ilut_keep_largest(Urow, &nu, orig + fill_p);
+        Ustart[i] = (int32_t)used;
+        memcpy(store + used, Urow, sizeof(ilut_entry) * (size_t)nu);
+        used += (size_t)nu;
+        ulen[i] = nu;
+        for (int32_t t = 0; t < nt; ++t) {
+            const int32_t j = tlist[t];
+            w[j] = 0.0; active[j] = 0; touched[j] = 0;
+        }
+    }
+    *nnz_out = (int64_t)used;
+    if (out_ci) {
+        int64_t pos = 0;
+        out_rp[0] = 0;
+        for (int32_t i = 0; i < n; ++i) {
+            for (int32_t q = 0; q < llen[i]; ++q) { out_ci[pos] = store[Lstart[i] + q].col; out_lu[pos] = store[Lstart[i] + q].val; ++pos; }
+            for (int32_t q = 0; q < ulen[i]; ++q) { out_ci[pos] = store[Ustart[i] + q].col; out_lu[pos] = store[Ustart[i] + q].val; ++pos; }
+            out_rp[i + 1] = (int32_t)pos;
+        }
+    }
+    free(w); free(active); free(touched); free(tlist); free(heap); free(Lstart); free(Ustart);
+    free(store); free(rowbuf); free(ulen); free(llen);
+    return HAMLSS_OK;
+}
+
 /* forward_sub / backward_sub / apply (ilu.cpp:225-271). */
 int orc_ilu_apply(int32_t n, const int32_t* rp, const int32_t* ci, const double* lu,
                   const double* r, double* z) {
@@ -547,9 +730,11 @@ void orc_amg_apply(const orc_amg* h, const double* r, double* z) {
 struct orc_prec {
     int kind;
     int32_t n;
-    const int32_t* rp;   /* pattern of A (caller keeps it alive) */
+    const int32_t* rp;   /* pattern of A (caller keeps it alive), or of the ILUT factor */
     const int32_t* ci;
     double* data;        /* Jacobi inv_diag or ILU factor values */
+    int32_t* frp;        /* ILUT: the factor's own pattern */
+    int32_t* fci;
     orc_amg* amg;
 };
 
@@ -563,8 +748,20 @@ orc_prec* orc_prec_setup(int kind, int32_t n, const int32_t* rp, const int32_t* 
         M->data = (double*)malloc(sizeof(double) * (size_t)(n > 0 ? n : 1));
         *status = orc_jacobi_setup(n, rp, ci, v, p->jacobi_omega, M->data);
     } else if (kind == HAMLSS_PREC_ILU) {
-        if (p->drop_tol > 0.0 || p->fill_per_row > 0) *status = HAMLSS_ERR_INVALID;
-        else {
+        /* SolverFactory::make_precond sets drop_tol only (solver_factory.cpp:73-77), so the
+         * dispatch of ilu.cpp:31-36 picks ILUT exactly when drop_tol > 0, with fill 0 */
+        if (p->drop_tol > 0.0) {
+            int64_t nnz = 0;
+            *status = orc_ilut_factor(n, rp, ci, v, p->drop_tol, 0, NULL, NULL, NULL, &nnz);
+            if (*status == HAMLSS_OK) {
+                M->frp = (int32_t*)malloc(sizeof(int32_t) * (size_t)(n + 1));
+                M->fci = (int32_t*)malloc(sizeof(int32_t) * (size_t)(nnz > 0 ? nnz : 1));
+                M->data = (double*)malloc(sizeof(double) * (size_t)(nnz > 0 ? nnz : 1));
+                *status = orc_ilut_factor(n, rp, ci, v, p->drop_tol, 0, M->frp, M->fci, M->data, &nnz);
+                M->rp = M->frp;
+                M->ci = M->fci;
+            }
+        } else {
             M->data = (double*)malloc(sizeof(double) * (size_t)(rp[n] > 0 ? rp[n] : 1));
             *status = orc_ilu0_factor(n, rp, ci, v, M->data);
         }
@@ -580,6 +777,8 @@ orc_prec* orc_prec_setup(int kind, int32_t n, const int32_t* rp, const int32_t* 
 void orc_prec_free(orc_prec* M) {
     if (!M) return;
     free(M->data);
+    free(M->frp);
+    free(M->fci);
     orc_amg_free(M->amg);
     free(M);
 }

@@ -38,6 +38,9 @@ int  orc_jacobi_setup(int32_t n, const int32_t* rp, const int32_t* ci, const dou
 /* ---- ILU(0) (ilu.cpp:41-89, :225-271) ---- */
 int  orc_ilu0_factor(int32_t n, const int32_t* rp, const int32_t* ci, const double* v,
                      double* lu);
+int  orc_ilut_factor(int32_t n, const int32_t* rp, const int32_t* ci, const double* v,
+                     double drop_tol, int32_t fill_p, int32_t* out_rp, int32_t* out_ci,
+                     double* out_lu, int64_t* nnz_out);
 int  orc_ilu_apply(int32_t n, const int32_t* rp, const int32_t* ci, const double* lu,
                    const double* r, double* z);
 /* level(i) = 1 + max level(j) over the strictly lower (which=0) or strictly upper

@@ -68,6 +68,7 @@ class Oracle:
         L.orc_dot.argtypes = [I32, V, V]
         L.orc_jacobi_setup.argtypes = [I32, V, V, V, D, V]
         L.orc_ilu0_factor.argtypes = [I32, V, V, V, V]
+        L.orc_ilut_factor.argtypes = [I32, V, V, V, D, I32, V, V, V, C.POINTER(C.c_int64)]
         L.orc_ilu_apply.argtypes = [I32, V, V, V, V, V]
         L.orc_levels.restype = I32
         L.orc_levels.argtypes = [I32, V, V, C.c_int, V]
@@ -127,6 +128,17 @@ class Oracle:
         lu = np.empty(len(A.v), _f64)
         rc = self.L.orc_ilu0_factor(*A.args(), _p(lu))
         return rc, lu
+
+    def ilut(self, rp, ci, v, drop_tol, fill_p=0):
+        """setup_ilut restated: the L\\U factor (rp, ci, values)."""
+        A = _Csr(rp, ci, v)
+        nnz = C.c_int64()
+        self.L.orc_ilut_factor(*A.args(), drop_tol, fill_p, None, None, None, C.byref(nnz))
+        frp = np.empty(A.n + 1, _i32)
+        fci = np.empty(max(nnz.value, 1), _i32)
+        flu = np.empty(max(nnz.value, 1), _f64)
+        self.L.orc_ilut_factor(*A.args(), drop_tol, fill_p, _p(frp), _p(fci), _p(flu), C.byref(nnz))
+        return frp, fci[:nnz.value], flu[:nnz.value]
 
     def ilu_apply(self, rp, ci, lu, r):
         A = _Csr(rp, ci, lu)
@@ -213,27 +225,6 @@ class Oracle:
         self.L.orc_extract_features(*A.args(), _p(f), C.byref(s))
         return f, s.value
 
-    def mtx_load_matrix(self, path):
-        """MatrixMarketIO::load_matrix: (rows, cols, rp, ci, v), or None on an exception."""
-        r, c, nz = C.c_int32(), C.c_int32(), C.c_int32()
-        p = os.fsencode(path)
-        if self.L.ref_mtx_load_matrix(p, C.byref(r), C.byref(c), C.byref(nz), None, None, None):
-            return None
-        rp = np.empty(r.value + 1, _i32)
-        ci = np.empty(max(nz.value, 1), _i32)
-        v = np.empty(max(nz.value, 1), _f64)
-        self.L.ref_mtx_load_matrix(p, C.byref(r), C.byref(c), C.byref(nz), _p(rp), _p(ci), _p(v))
-        return r.value, c.value, rp, ci[:nz.value], v[:nz.value]
-
-    def mtx_load_vector(self, path, expected_n=0):
-        n = C.c_int32()
-        p = os.fsencode(path)
-        if self.L.ref_mtx_load_vector(p, expected_n, None, C.byref(n)):
-            return None
-        out = np.empty(max(n.value, 1), _f64)
-        self.L.ref_mtx_load_vector(p, expected_n, _p(out), C.byref(n))
-        return out[:n.value]
-
     def solve_adaptive(self, rp, ci, v, b, x0=None, params=None, log_cap=8):
         A = _Csr(rp, ci, v)
         p = params or default_params()
@@ -308,6 +299,7 @@ class Reference:
         L.ref_solve_adaptive.argtypes = [I32, V, V, V, V, V, C.POINTER(Params), C.POINTER(Stats),
                                          C.POINTER(Escalation), I32, pi]
         L.ref_mtx_load_matrix.argtypes = [C.c_char_p, pi, pi, pi, V, V, V]
+        L.ref_ilut_factor.argtypes = [I32, V, V, V, D, I32, V, V, V, C.POINTER(C.c_int64)]
         L.ref_mtx_load_vector.argtypes = [C.c_char_p, I32, V, pi]
         self.L = L
         self.set_threads(1 if threads is None else threads)
@@ -405,6 +397,19 @@ class Reference:
         s = C.c_int32(0)
         self.L.ref_extract_features(*A.args(), _p(f), C.byref(s))
         return f, s.value
+
+    def ilut(self, rp, ci, v, drop_tol, fill_p=0):
+        """ILUPreconditioner::setup_ilut: the L\\U factor (rp, ci, values)."""
+        A = _Csr(rp, ci, v)
+        nnz = C.c_int64()
+        rc = self.L.ref_ilut_factor(*A.args(), drop_tol, fill_p, None, None, None, C.byref(nnz))
+        if rc:
+            raise RuntimeError(f"reference ILUT failed ({rc})")
+        frp = np.empty(A.n + 1, _i32)
+        fci = np.empty(max(nnz.value, 1), _i32)
+        flu = np.empty(max(nnz.value, 1), _f64)
+        self.L.ref_ilut_factor(*A.args(), drop_tol, fill_p, _p(frp), _p(fci), _p(flu), C.byref(nnz))
+        return frp, fci[:nnz.value], flu[:nnz.value]
 
     def mtx_load_matrix(self, path):
         """MatrixMarketIO::load_matrix: (rows, cols, rp, ci, v), or None on an exception."""

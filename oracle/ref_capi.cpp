@@ -279,6 +279,26 @@ int ref_solve_adaptive(int32_t n, const int32_t* rp, const int32_t* ci, const do
     }
 }
 
+// ILUPreconditioner::setup with drop_tol > 0 or fill_per_row > 0 (setup_ilut): the L\U
+// factor (row_ptr_, col_idx_, lu_val_).  *nnz first; the arrays when given.
+int ref_ilut_factor(int32_t n, const int32_t* rp, const int32_t* ci, const double* v, double drop_tol,
+                    int32_t fill_p, int32_t* frp, int32_t* fci, double* flu, int64_t* nnz) {
+    try {
+        SparseMatrix A = make_csr(n, rp, ci, v);
+        ILUPreconditioner ilu;
+        ilu.set_drop_tol(drop_tol);
+        ilu.set_fill_per_row(fill_p);
+        ilu.setup(A);
+        *nnz = static_cast<int64_t>(ilu.col_idx_.size());
+        if (frp) std::memcpy(frp, ilu.row_ptr_.data(), sizeof(int32_t) * (n + 1));
+        if (fci && *nnz) std::memcpy(fci, ilu.col_idx_.data(), sizeof(int32_t) * (size_t)*nnz);
+        if (flu && *nnz) std::memcpy(flu, ilu.lu_val_.data(), sizeof(double) * (size_t)*nnz);
+        return 0;
+    } catch (const std::exception& e) {
+        return map_error(e);
+    }
+}
+
 // MatrixMarketIO::load_matrix: rows / cols / nnz, then (when the arrays are given) the CSR.
 int ref_mtx_load_matrix(const char* path, int32_t* rows, int32_t* cols, int32_t* nnz, int32_t* rp,
                         int32_t* ci, double* v) {

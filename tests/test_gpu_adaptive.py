@@ -126,10 +126,18 @@ def test_ladder_warm_start_reuses_x():
     assert sel.solve(A, b, x, st) and st.iterations == 0
 
 
-def test_ladder_ilut_request_refused():
+def test_ladder_through_ilut(ref):
     # EASY (CG+Jacobi) cannot converge in 5 iterations, so the ladder escalates to
-    # MODERATE, which asks for ILUT under the default drop_tol = 1e-4
+    # MODERATE, whose ILU is ILUT(1e-4, 0) under the default drop_tol, then to HARD
     A = H.SparseMatrix.poisson_2d(16)
-    sel = H.AdaptiveSelector(default_params(max_iter=5))
-    with pytest.raises(H.HamlssError):
-        sel.solve(A, np.ones(256), np.zeros(256))
+    b = np.ones(256)
+    p = default_params(max_iter=5)
+    sel = H.AdaptiveSelector(p)
+    x = np.zeros(256)
+    st = H.SolverStats()
+    assert sel.solve(A, b, x, st)
+    rc, xr, sr, log = ref.solve_adaptive(A.row_ptr(), A.col_idx(), A.values(), b, params=p)
+    assert [(e.from_state, e.to_state, e.at_iteration) for e in sel.escalation_log()] == \
+           [(e.from_state, e.to_state, e.at_iteration) for e in log] == [(0, 1, 5), (1, 2, 5)]
+    assert st.state_used == sr.state_used == 2
+    assert abs(st.iterations - sr.iterations) <= 1

@@ -219,3 +219,71 @@ def test_reference_from_coo_matches_generators(ref):
     # from_coo sorts by (row, col) and accumulates duplicates (sparse_matrix.cpp:242-282)
     rp, ci, v = ref.from_coo(3, 3, [2, 0, 0, 1, 0], [1, 2, 0, 1, 0], [1.0, 2.0, 3.0, 4.0, 5.0])
     assert list(rp) == [0, 2, 3, 4] and list(ci) == [0, 2, 1, 1] and list(v) == [8.0, 2.0, 4.0, 1.0]
+
+
+# ------------------------------------------------------------------------ ILUT(tau, p)
+
+ILUT_SETTINGS = [(1e-4, 0), (1e-3, 5), (1e-2, 0), (0.0, 3), (1e-4, 10), (0.3, 1)]
+
+
+@pytest.mark.parametrize("name,A", list(_cases()), ids=[c[0] for c in _cases()])
+def test_oracle_ilut_equals_reference(orc, ref, name, A):
+    # setup_ilut (ilu.cpp:94-220), including keep_largest's heap select (ilu.cpp:186-197)
+    for dt, fp in ILUT_SETTINGS:
+        a, b = orc.ilut(*A, dt, fp), ref.ilut(*A, dt, fp)
+        for x, y in zip(a, b):
+            assert np.array_equal(x, y), (dt, fp)
+    n = len(A[0]) - 1
+    b = P.rhs(n, 5)
+    # the factory path: drop_tol only, fill_per_row ignored (solver_factory.cpp:73-77)
+    for dt, fp in ((1e-4, 0), (1e-3, 5)):
+        p = default_params(drop_tol=dt, fill_per_row=fp, tol=1e-8, max_iter=600, restart_size=25)
+        r1 = orc.solve(1, 2, *A, b, params=p)
+        r2 = ref.solve(1, 2, *A, b, params=p)
+        assert r1[0] == r2[0] and r1[2].iterations == r2[2].iterations
+        assert np.array_equal(r1[1], r2[1])
+        z = orc.precond_apply(2, *A, b, p)[1]
+        assert np.array_equal(z, ref.precond_apply(2, *A, b, p)[1])
+        assert np.array_equal(z, orc.ilu_apply(*orc.ilut(*A, dt, 0), b)[1])
+
+
+def test_oracle_ladder_through_ilut_equals_reference(orc, ref):
+    # CG+Jacobi cannot converge in 5 iterations: the ladder escalates to MODERATE, whose
+    # ILU is ILUT(1e-4, 0) under the default drop_tol, then to HARD
+    A = P.poisson_2d(16)
+    b = np.ones(256)
+    p = default_params(max_iter=5)
+    o = orc.solve_adaptive(*A, b, params=p)
+    q = ref.solve_adaptive(*A, b, params=p)
+    assert o[0] == q[0] == 1 and o[2].iterations == q[2].iterations
+    assert [(e.from_state, e.to_state, e.at_iteration) for e in o[3]] == \
+           [(e.from_state, e.to_state, e.at_iteration) for e in q[3]] == [(0, 1, 5), (1, 2, 5)]
+    assert np.array_equal(o[1], q[1])
+
+
+def test_kat_ilut(orc):
+    # test_improvements.cpp:49-114, restated on the oracle
+    A = P.poisson_2d(10)
+    b = np.ones(100)
+    z0 = orc.precond_apply(2, *A, b, default_params(drop_tol=0.0, fill_per_row=0))[1]
+    z1 = orc.precond_apply(2, *A, b, default_params(drop_tol=0.0, fill_per_row=0))[1]
+    assert np.allclose(z0, z1, rtol=0, atol=1e-12)           # ILUT(0, 0) is ILU(0)
+    C = P.convection_diffusion_2d(10, 0.1, 3.0, 0.0)
+    for dt in (0.0, 1e-3):
+        rc, z = orc.precond_apply(2, *C, np.ones(100), default_params(drop_tol=dt, fill_per_row=0))
+        assert rc == 0 and np.linalg.norm(z) > 0
+    C = P.convection_diffusion_2d(12, 0.1, 8.0, 0.0)
+    rc, z = orc.ilu_apply(*orc.ilut(*C, 1e-4, 5), np.ones(144))
+    assert rc == 0 and np.all(np.isfinite(z)) and np.linalg.norm(z) > 0
+
+
+def test_ilut_capacity_fixture(orc):
+    # an empty row keeps its diagonal shift; a row whose L / U exceed orig + fill is cut to
+    # the largest magnitudes, kept in column order
+    rp, ci, v = coo_csr(4, [0, 0, 1, 1, 2, 2, 2, 3], [0, 1, 0, 1, 0, 1, 2, 3],
+                        [4.0, 1.0, 1.0, 4.0, 1.0, -3.0, 5.0, 2.0])
+    frp, fci, flu = orc.ilut(rp, ci, v, 1e-6, 0)
+    assert list(frp[1:] - frp[:-1]) == [2, 2, 3, 1]
+    rp2 = np.array([0, 1, 1, 2], np.int32)
+    frp2, fci2, flu2 = orc.ilut(rp2, np.array([0, 2], np.int32), np.array([2.0, 3.0]), 1e-4, 0)
+    assert list(fci2) == [0, 1, 2] and flu2[1] == 2.220446049250313e-16 * 1e6
