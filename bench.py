@@ -64,6 +64,8 @@ def parse():
     ap.add_argument("--serving-requests", type=int, default=200,
                     help="requests in the serving stream (0 skips the serving measurement)")
     ap.add_argument("--serving-n-max", type=float, default=2.6e5)
+    ap.add_argument("--no-ilut", action="store_true",
+                    help="skip the ILUT side measurement (device vs reference setup_ilut)")
     ap.add_argument("--profile-step", action="store_true",
                     help="run the warm-up, then ONE step between cudaProfilerStart/Stop and exit "
                          "(for ncu --profile-from-start off); prints no result line")
@@ -539,7 +541,7 @@ def serving_params():
 
     return H.SolverParams(tol=TOL, max_iter=4000, restart_size=30, drop_tol=0.0,
                           precision=1, amg_omega=2.0 / 3.0, amg_coarse_limit=512, amg_levels=25,
-                          amg_stall_ratio=STALL, ladder_mode=2)
+                          amg_stall_ratio=STALL, ladder_mode=3)
 
 
 def _pct(lat, q):
@@ -550,15 +552,19 @@ def _pct(lat, q):
 
 def serve_plain(reqs, params, device):
     """One solve per call, in arrival order (the one-solve-per-launch path): upload, adaptive
-    ladder, download through the C ABI on one context.  Latency = completion - arrival."""
+    ladder, download through the C ABI on one context; when the ladder fails at its top, the
+    rungs it skipped are tried from x0 as the server does (same algorithm, no concurrency,
+    no coalescing).  Latency = completion - arrival."""
     import ctypes as C
 
     import hsps_b200 as H
     from hsps_b200 import _abi
+    from hsps_b200.mtx import _spd_like
 
     L = _abi.lib()
     ctx = H.Context(device)
     lat, res = [], []
+    setup_errors = (_abi.ERR_NOMEM, _abi.ERR_ZERO_PIVOT, _abi.ERR_TIMEOUT, _abi.ERR_ZERO_DIAG)
     t0 = time.perf_counter()
     for rp, ci, v, b, arr, _ in reqs:
         now = time.perf_counter() - t0
@@ -574,6 +580,25 @@ def serve_plain(reqs, params, device):
             rc = L.hamlss_solve_adaptive(ctx.h, mh, b.ctypes.data, x.ctypes.data, H.HOST,
                                          C.byref(params), C.byref(st), None, 0, C.byref(nlog),
                                          C.byref(init))
+            if rc in setup_errors:
+                rc, st.converged = 0, 0
+        for state in range(init.value - 1, -1, -1):
+            if rc or st.converged:
+                break
+            if state == 0 and not _spd_like(len(b), rp, ci, v):
+                continue
+            kind, solver = (H.PREC_JACOBI, H.SOLVER_CG) if state == 0 else (H.PREC_ILU, H.SOLVER_FGMRES)
+            M = C.c_void_p()
+            setup = C.c_double()
+            if L.hamlss_precond_setup(ctx.h, mh, kind, C.byref(params), C.byref(M), C.byref(setup)):
+                continue
+            x2 = np.zeros(len(b))
+            s2 = _abi.Stats()
+            rc2 = L.hamlss_solve(ctx.h, solver, mh, M, b.ctypes.data, x2.ctypes.data, H.HOST,
+                                 C.byref(params), C.byref(s2))
+            L.hamlss_precond_release(M)
+            if rc2 == 0 and s2.converged:
+                x, st = x2, s2
         L.hamlss_mat_release(mh)
         if rc:
             raise RuntimeError(L.hamlss_last_error())
@@ -635,6 +660,53 @@ def run_serving(args, local):
             "poisson_arrivals": {"rate_per_s": round(rate, 2), "server": eng_r, "plain": plain_r}}
 
 
+def run_ilut_side(args, local):
+    """ILUT(1e-4, 0) -- the factory's ILU under the default drop_tol -- set up on the device
+    and by the reference (setup_ilut, one host thread: it is sequential) on the upwind
+    conv-diff 128^2 (eps 1, beta (10, 5)); FGMRES(30) iterations with each; then the device
+    setup alone at 1024^2, where the reference's O(n^2) scans would take hours."""
+    import hsps_b200 as H
+    import oracle
+    from hsps_b200 import problems as P
+    from hsps_b200._abi import default_params
+
+    def device(A, solve):
+        n = len(A[0]) - 1
+        M = H.SparseMatrix(n, n, *A)
+        times = []
+        for _ in range(5):
+            I = H.ILUPreconditioner()
+            I.set_drop_tol(1e-4)
+            times.append(I.setup(M))
+        out = {"n": n, "setup_ms": round(1e3 * float(np.median(times)), 3),
+               "factor_nnz": int(len(I.factor_csr()[1]))}
+        if solve:
+            s = H.FGMRESSolver()
+            s.set_params(default_params(tol=1e-8, max_iter=2000, restart_size=30))
+            s.set_preconditioner(I)
+            st = H.SolverStats()
+            x = np.zeros(n)
+            t0 = time.perf_counter()
+            s.solve(M, np.ones(n), x, st)
+            out.update(iterations=st.iterations, solve_ms=round(1e3 * (time.perf_counter() - t0), 3))
+        return out
+
+    A = P.convection_diffusion_2d(128, 1.0, 10.0, 5.0)
+    dev = device(A, True)
+    R = oracle.Reference(fast=True, threads=1)
+    t0 = time.perf_counter()
+    frp, fci, flu = R.ilut(*A, 1e-4, 0)
+    ref_setup = time.perf_counter() - t0
+    p = default_params(tol=1e-8, max_iter=2000, restart_size=30)
+    rc, x, st = R.solve(1, 2, *A, np.ones(len(A[0]) - 1), params=p)
+    big = device(P.convection_diffusion_2d(1024, 1.0, 10.0, 5.0), False)
+    return {"problem": "upwind conv-diff eps 1, beta (10, 5); ILUT(1e-4, 0); FGMRES(30) to 1e-8, b = 1",
+            "device_128": dev,
+            "reference_128": {"setup_ms": round(1e3 * ref_setup, 3), "factor_nnz": int(len(fci)),
+                              "iterations": st.iterations, "threads": 1},
+            "device_1024": big}
+
+
 def main():
     args = parse()
     rank, world, local = dist_env()
@@ -661,6 +733,9 @@ def main():
         log("cpu baseline done")
     if rank == 0 and world == 1 and args.serving_requests > 0:
         out["serving"] = run_serving(args, local)
+    if rank == 0 and world == 1 and not args.no_ilut:
+        log("ILUT side measurement")
+        out["ilut"] = run_ilut_side(args, local)
     if world > 1:
         import torch
 

@@ -223,30 +223,111 @@ __device__ __forceinline__ float sub_mul<float>(float s, float a, float b) {
 }
 
 // L y = r (unit lower, forward_sub) then U z = y (backward_sub); one block.
+//
+// One level's critical path is a barrier plus the loads of the vector being solved for; the
+// rest of a row's inputs (its index, right-hand side, columns, values, diagonal) do not
+// depend on the sweep, so they are fetched ahead in a three-stage pipeline: stage 1 (row
+// index, row bounds) two levels ahead, stage 2 (rhs, up to kIluPre columns and values, the
+// diagonal) one level ahead, while the current level computes.  The level pointers sit in
+// shared memory.  A thread pipelines its first row of each level; rows beyond the block
+// width and rows longer than kIluPre take the plain path.  The block's own stores are read
+// back with ordinary loads after the barrier (block scope), and every row sums in its
+// stored (ascending column) order, so results are bit-identical to the plain loop.
+constexpr int kIluPre = 4;
+constexpr int kIluLptrSmem = 4096;
+
+template <typename T>
+struct IluStage2 {
+    int t, i, o0, cnt;
+    T rv, d;
+    int c[kIluPre];
+    T v[kIluPre];
+};
+
+template <typename T, bool DIV, int NT>
+__device__ __forceinline__ void ilu_sweep_block(int nlev, const int* __restrict__ lptr_g, const int* s_lptr,
+                                                const int* __restrict__ ord, const int* __restrict__ rp,
+                                                const int* __restrict__ ci, const T* __restrict__ v,
+                                                const T* __restrict__ dg, const T* rhs, T* out) {
+    auto lptr = [&](int l) { return l < kIluLptrSmem ? s_lptr[l] : __ldg(&lptr_g[l]); };
+    const int tid = threadIdx.x;
+    // stage 1 of a level: (t, i, o0, cnt) of this thread's first row, t = -1 if none
+    auto stage1 = [&](int l, int& t, int& i, int& o0, int& cnt) {
+        t = -1;
+        if (l < nlev) {
+            const int b = lptr(l), e = lptr(l + 1);
+            if (b + tid < e) {
+                t = b + tid;
+                i = ord[t];
+                o0 = rp[t];
+                cnt = rp[t + 1] - o0;
+            }
+        }
+    };
+    auto stage2 = [&](IluStage2<T>& q, int t, int i, int o0, int cnt) {
+        q.t = t;
+        if (t < 0) return;
+        q.i = i;
+        q.o0 = o0;
+        q.cnt = cnt;
+        q.rv = rhs[i];
+        if (DIV) q.d = dg[t];
+#pragma unroll
+        for (int k = 0; k < kIluPre; ++k)
+            if (k < cnt) {
+                q.c[k] = ci[o0 + k];
+                q.v[k] = v[o0 + k];
+            }
+    };
+    int t1, i1, o1, c1;                  // stage 1 of level l + 1
+    IluStage2<T> cur;
+    {
+        int t0, i0, o0, c0;
+        stage1(0, t0, i0, o0, c0);
+        stage2(cur, t0, i0, o0, c0);
+        stage1(1, t1, i1, o1, c1);
+    }
+    for (int l = 0; l < nlev; ++l) {
+        IluStage2<T> nxt;
+        stage2(nxt, t1, i1, o1, c1);     // level l + 1, in flight while level l computes
+        int t2, i2, o2, c2;
+        stage1(l + 2, t2, i2, o2, c2);   // level l + 2
+        if (cur.t >= 0) {
+            T s = cur.rv;
+            if (cur.cnt <= kIluPre) {
+#pragma unroll
+                for (int k = 0; k < kIluPre; ++k)
+                    if (k < cur.cnt) s = sub_mul<T>(s, cur.v[k], out[cur.c[k]]);
+            } else {
+                for (int o = cur.o0; o < cur.o0 + cur.cnt; ++o) s = sub_mul<T>(s, v[o], out[ci[o]]);
+            }
+            out[cur.i] = DIV ? s / cur.d : s;
+            // rows of this level beyond the block width
+            const int e = lptr(l + 1);
+            for (int t = cur.t + NT; t < e; t += NT) {
+                const int i = ord[t];
+                T s2 = rhs[i];
+                for (int o = rp[t]; o < rp[t + 1]; ++o) s2 = sub_mul<T>(s2, v[o], out[ci[o]]);
+                out[i] = DIV ? s2 / dg[t] : s2;
+            }
+        }
+        __syncthreads();
+        cur = nxt;
+        t1 = t2; i1 = i2; o1 = o2; c1 = c2;
+    }
+}
+
 template <typename T, int NT>
 __global__ void __launch_bounds__(NT)
 k_ilu_apply_block(IluLevels<T> F, const T* __restrict__ r, T* y, T* z, const int* gate) {
+    __shared__ int s_lptr[kIluLptrSmem];
     if (gate && *(volatile const int*)gate) return;
-    for (int l = 0; l < F.nlevL; ++l) {
-        const int b = F.lptrL[l], e = F.lptrL[l + 1];
-        for (int t = b + threadIdx.x; t < e; t += NT) {
-            const int i = F.ordL[t];
-            T s = r[i];
-            for (int o = F.Lrp[t]; o < F.Lrp[t + 1]; ++o) s = sub_mul<T>(s, F.Lv[o], __ldcg(&y[F.Lci[o]]));
-            y[i] = s;
-        }
-        __syncthreads();
-    }
-    for (int l = 0; l < F.nlevU; ++l) {
-        const int b = F.lptrU[l], e = F.lptrU[l + 1];
-        for (int t = b + threadIdx.x; t < e; t += NT) {
-            const int i = F.ordU[t];
-            T s = __ldcg(&y[i]);
-            for (int o = F.Urp[t]; o < F.Urp[t + 1]; ++o) s = sub_mul<T>(s, F.Uv[o], __ldcg(&z[F.Uci[o]]));
-            z[i] = s / F.Ud[t];
-        }
-        __syncthreads();
-    }
+    for (int l = threadIdx.x; l <= F.nlevL && l < kIluLptrSmem; l += NT) s_lptr[l] = F.lptrL[l];
+    __syncthreads();
+    ilu_sweep_block<T, false, NT>(F.nlevL, F.lptrL, s_lptr, F.ordL, F.Lrp, F.Lci, F.Lv, nullptr, r, y);
+    for (int l = threadIdx.x; l <= F.nlevU && l < kIluLptrSmem; l += NT) s_lptr[l] = F.lptrU[l];
+    __syncthreads();
+    ilu_sweep_block<T, true, NT>(F.nlevU, F.lptrU, s_lptr, F.ordU, F.Urp, F.Uci, F.Uv, F.Ud, y, z);
 }
 
 // Same sweeps with the whole grid (cooperative launch) for matrices with wide levels.

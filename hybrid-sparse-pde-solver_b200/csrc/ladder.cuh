@@ -7,7 +7,10 @@
 //   stall       history >= window entries and rel / history[size - window] > threshold
 //   budget      EASY and iteration > max_iter*4/10, MODERATE and iteration > max_iter*7/10
 // The reference defines this test but its solve loop never calls it (it escalates only
-// when an attempt exhausts max_iter); ladder_mode = 1 turns it on.
+// when an attempt exhausts max_iter); ladder_mode = 1 turns it on.  With no_stall set (the
+// CG rung under ladder_mode = 3) the windowed stall rule is skipped: CG's recursive
+// residual is not monotone, and on variable-coefficient problems it rises and falls over
+// tens of iterations, so a 15-iteration window ends attempts that were converging.
 #pragma once
 
 #include "common.cuh"
@@ -22,10 +25,11 @@ struct LadderCfg {
     int window = 15;
     double threshold = 0.95;
     int max_iter = 2000;
+    int no_stall = 0;
 };
 
 struct LadderDev {
-    int on, state, window, max_iter, count, reason;
+    int on, state, window, max_iter, count, reason, no_stall;
     double threshold, first;
     double ring[kLadderRing];
 };
@@ -41,6 +45,7 @@ inline LadderDev ladder_init(const LadderCfg* c) {
         d.window = c->window < 1 ? 1 : (c->window > kLadderRing ? kLadderRing : c->window);
         d.threshold = c->threshold;
         d.max_iter = c->max_iter;
+        d.no_stall = c->no_stall;
     }
     return d;
 }
@@ -51,7 +56,7 @@ __device__ __forceinline__ int ladder_check(LadderDev* L, int iteration, double 
     int reason = ESC_NONE;
     const int k = L->count;
     if (k >= 2 && rel > 10.0 * L->first) reason = ESC_DIVERGENCE;
-    else if (k >= L->window) {
+    else if (!L->no_stall && k >= L->window) {
         double prev = L->ring[(k - L->window) % kLadderRing];
         if (prev > 2.220446049250313e-16 && rel / prev > L->threshold) reason = ESC_STALL;
     }

@@ -99,6 +99,8 @@ typedef struct hamlss_params {
     int32_t ladder_mode;      /* 0: escalate when an attempt exhausts max_iter (reference)   */
                               /* 1: also escalate on the device-side stall / budget checks   */
                               /* 2: as 1, and end the top rung early on stall / divergence   */
+                              /* 3: as 2, but the CG rung skips the windowed stall rule (its */
+                              /*    residual is not monotone): divergence / budget only      */
     int32_t check_every;      /* iterations between device->host convergence polls (8)      */
     double  amg_stall_ratio;  /* 0: coarsen until amg_coarse_limit / amg_levels / no progress */
                               /* (reference); r in (0,1): also stop when n_c > r * n_f, the  */
