@@ -213,8 +213,8 @@ protected:
     hsps::Real omega_ = 1.0;
 };
 
-// ILU(0); a drop tolerance or fill > 0 (ILUT in the project) is refused with
-// std::invalid_argument at setup.
+// ILU(0), or ILUT(drop_tol, fill_per_row) when either is > 0 (ilu.cpp:31-36), factored on
+// the device in the project's order (bit-identical factors).
 class DeviceILU : public DevicePreconditioner {
 public:
     DeviceILU() : DevicePreconditioner(hsps::PrecondType::ILU) {}

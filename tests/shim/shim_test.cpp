@@ -3,6 +3,7 @@
 // Built against the project's headers and linked with the project's library (built from
 // its sources into oracle/_ref/) plus libhamlss_b200.so; run by tests/test_gpu_shim.py.
 // Each check runs the project's CPU class and the device class on the same inputs.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -80,6 +81,35 @@ int main() {
                       to_string(cpu.current_state()), to_string(dev.current_state()));
         CHECK(oc == od && cpu.escalation_log().size() == dev.escalation_log().size() &&
               cpu.current_state() == dev.current_state(), msg);
+    }
+
+    {   // ILUT: the factory's ILU under the default drop_tol, and the class with fill
+        SolverParams q = p;
+        q.drop_tol = 1e-4;
+        auto A = SparseMatrix::convection_diffusion_2d(32, 1.0, 200.0, 100.0);
+        Vector b(A.rows(), 1.0);
+        auto cpu = SolverFactory::make(SolverType::FGMRES, PrecondType::ILU, A, q);
+        auto dev = hsps_b200::DeviceSolverFactory::make(SolverType::FGMRES, PrecondType::ILU, A, q);
+        Vector xc(A.rows(), 0.0), xd;
+        SolverStats sc, sd;
+        bool oc = cpu.first->solve(A, b, xc, sc);
+        bool od = dev.first->solve(A, b, xd, sd);
+        char msg[256];
+        std::snprintf(msg, sizeof msg, "FGMRES+ILUT(1e-4): converged %d/%d iters %d/%d", (int)oc,
+                      (int)od, sc.iterations, sd.iterations);
+        CHECK(oc == od && std::abs(sc.iterations - sd.iterations) <= 1, msg);
+        ILUPreconditioner ic;
+        hsps_b200::DeviceILU id;
+        ic.set_drop_tol(1e-3); ic.set_fill_per_row(5); ic.setup(A);
+        id.set_drop_tol(1e-3); id.set_fill_per_row(5); id.setup(A);
+        Vector r(A.rows()), zc(A.rows()), zd(A.rows());
+        for (Index i = 0; i < A.rows(); ++i) r[i] = std::sin(0.37 * i);
+        ic.apply(r, zc);
+        id.apply(r, zd);
+        double diff = 0.0;
+        for (Index i = 0; i < A.rows(); ++i) diff = std::max(diff, std::abs(zc[i] - zd[i]));
+        std::snprintf(msg, sizeof msg, "ILUT(1e-3, 5) apply: max |cpu - device| = %.3e", diff);
+        CHECK(diff == 0.0, msg);
     }
 
     {   // error behaviour
