@@ -219,32 +219,14 @@ double bits_to_double(unsigned long long b) {
     return d;
 }
 
-}  // namespace
-
-int extract_features(Ctx& ctx, hamlss_mat* A, double feat[24], int* initial_state) {
+// K Lanczos steps from the uniform vector (the recurrence of adaptive_selector.cpp:66-89
+// and sparse_matrix.cpp:451-468, as fused SpMV + dot kernels), then the Gershgorin bounds
+// of the tridiagonal T (adaptive_selector.cpp:91-101, sparse_matrix.cpp:469-478).
+void lanczos_bounds(Ctx& ctx, hamlss_mat* A, int K, double* tmin_out, double* tmax_out) {
     const int n = A->A.n;
-    const int nnz = A->A.nnz;
-    if (n == 0) fail(HAMLSS_ERR_INVALID, "features of an empty matrix");
     const Lane& L = ctx.lane;
     cudaStream_t st = L.stream;
     Workspace& ws = A->ws;
-    ProfScope ps(L, "features", 0.0);
-    // ---- row statistics
-    DBuf<char> exbuf(sizeof(Extrema));
-    Extrema h0{};
-    h0.min_dd = 0x7ff0000000000000ULL;       // +inf
-    h0.min_posdiag = 0x7ff0000000000000ULL;
-    HAMLSS_CUDA(cudaMemcpyAsync(exbuf.p, &h0, sizeof(h0), cudaMemcpyHostToDevice, st));
-    DBuf<double> sums(4);
-    const int sample_rows = std::min(200, n);
-    const int stride = std::max(1, n / sample_rows);
-    const double mean = (double)nnz / n;
-    int blocks = std::max(1, std::min(ceil_div(n, 256), ctx.sm_count * 8));
-    k_features<<<blocks, 256, 0, st>>>(n, A->A.rp.p, A->A.ci.p, A->A.v.p, mean, stride,
-                                       reinterpret_cast<Extrema*>(exbuf.p), L.red(), sums.p);
-    HAMLSS_LAUNCH_CHECK();
-    // ---- Lanczos (K = min(n, 30) steps)
-    const int K = std::min(n, 30);
     double* q = (ws.d[0].ensure(n), ws.d[0].p);
     double* qp = (ws.d[1].ensure(n), ws.d[1].p);
     double* Aq = (ws.d[2].ensure(n), ws.d[2].p);
@@ -260,17 +242,9 @@ int extract_features(Ctx& ctx, hamlss_mat* A, double feat[24], int* initial_stat
         launch_vec<0>(ctx.sm_count, L, n, BodyLzShift{q, qp, Aq, lz, 0.0}, NoFin{}, &lz->halt,
                       "features", 32.0 * n);
     }
-    Extrema ex;
-    double hs[3];
     LzState hl;
-    HAMLSS_CUDA(cudaMemcpyAsync(&ex, exbuf.p, sizeof(ex), cudaMemcpyDeviceToHost, st));
-    HAMLSS_CUDA(cudaMemcpyAsync(hs, sums.p, sizeof(hs), cudaMemcpyDeviceToHost, st));
     HAMLSS_CUDA(cudaMemcpyAsync(&hl, lz, sizeof(hl), cudaMemcpyDeviceToHost, st));
     HAMLSS_CUDA(cudaStreamSynchronize(st));
-    // ---- assemble (adaptive_selector.cpp:37-220)
-    const double fro = std::sqrt(hs[0]);
-    double min_dd = bits_to_double(ex.min_dd);
-    const double diag_dom = std::isinf(min_dd) ? 1.0 : min_dd;
     int sz = hl.na;
     double tmin = hl.alpha[0], tmax = hl.alpha[0];
     for (int i = 0; i < sz; ++i) {
@@ -280,6 +254,48 @@ int extract_features(Ctx& ctx, hamlss_mat* A, double feat[24], int* initial_stat
         tmin = std::min(tmin, hl.alpha[i] - r);
         tmax = std::max(tmax, hl.alpha[i] + r);
     }
+    *tmin_out = tmin;
+    *tmax_out = tmax;
+}
+
+}  // namespace
+
+void spectral_interval(Ctx& ctx, hamlss_mat* A, int steps, double* lo, double* hi) {
+    lanczos_bounds(ctx, A, std::min(A->A.n, steps), lo, hi);
+}
+
+int extract_features(Ctx& ctx, hamlss_mat* A, double feat[24], int* initial_state) {
+    const int n = A->A.n;
+    const int nnz = A->A.nnz;
+    if (n == 0) fail(HAMLSS_ERR_INVALID, "features of an empty matrix");
+    const Lane& L = ctx.lane;
+    cudaStream_t st = L.stream;
+    ProfScope ps(L, "features", 0.0);
+    // ---- row statistics
+    DBuf<char> exbuf(sizeof(Extrema));
+    Extrema h0{};
+    h0.min_dd = 0x7ff0000000000000ULL;       // +inf
+    h0.min_posdiag = 0x7ff0000000000000ULL;
+    HAMLSS_CUDA(cudaMemcpyAsync(exbuf.p, &h0, sizeof(h0), cudaMemcpyHostToDevice, st));
+    DBuf<double> sums(4);
+    const int sample_rows = std::min(200, n);
+    const int stride = std::max(1, n / sample_rows);
+    const double mean = (double)nnz / n;
+    int blocks = std::max(1, std::min(ceil_div(n, 256), ctx.sm_count * 8));
+    k_features<<<blocks, 256, 0, st>>>(n, A->A.rp.p, A->A.ci.p, A->A.v.p, mean, stride,
+                                       reinterpret_cast<Extrema*>(exbuf.p), L.red(), sums.p);
+    HAMLSS_LAUNCH_CHECK();
+    double tmin = 0.0, tmax = 0.0;
+    lanczos_bounds(ctx, A, std::min(n, 30), &tmin, &tmax);     // adaptive_selector.cpp:66-101
+    Extrema ex;
+    double hs[3];
+    HAMLSS_CUDA(cudaMemcpyAsync(&ex, exbuf.p, sizeof(ex), cudaMemcpyDeviceToHost, st));
+    HAMLSS_CUDA(cudaMemcpyAsync(hs, sums.p, sizeof(hs), cudaMemcpyDeviceToHost, st));
+    HAMLSS_CUDA(cudaStreamSynchronize(st));
+    // ---- assemble (adaptive_selector.cpp:37-220)
+    const double fro = std::sqrt(hs[0]);
+    double min_dd = bits_to_double(ex.min_dd);
+    const double diag_dom = std::isinf(min_dd) ? 1.0 : min_dd;
     double lam_max = std::max(tmax, kEps);
     double lam_min = tmin;
     if (lam_min <= kEps) {

@@ -531,7 +531,13 @@ SolveResult solve_core(Ctx& c, int solver, hamlss_mat* Am, Prec* P, const double
                        const hamlss_params& p, const LadderCfg* lad, int* outer) {
     *outer = 1;
     Workspace& ws = Am->ws;
-    if (p.precision == HAMLSS_MIXED) return mixed_solve(c, solver, Am, P, db, dx, p, ws, outer, lad);
+    if (solver == HAMLSS_SOLVER_SSTEP_CG) return sstep_solve(c, Am, db, dx, p, ws);   // FP64 only
+    if (p.precision == HAMLSS_MIXED) {
+        const int inner = solver == HAMLSS_SOLVER_PIPELINED_FGMRES ? HAMLSS_SOLVER_FGMRES : solver;
+        return mixed_solve(c, inner, Am, P, db, dx, p, ws, outer, lad);
+    }
+    if (solver == HAMLSS_SOLVER_PIPELINED_FGMRES)
+        return fgmres_solve(c, Am, P, db, dx, p.tol, p.max_iter, p.restart_size, ws, lad, true);
     if (solver == HAMLSS_SOLVER_CG)
         return cg_solve<double>(c, Am, P, db, dx, p.tol, p.max_iter, p.check_every, ws, lad);
     return fgmres_solve(c, Am, P, db, dx, p.tol, p.max_iter, p.restart_size, ws, lad);
@@ -548,12 +554,16 @@ void fill_stats(Ctx& c, hamlss_mat* Am, int solver, const Prec* P, const SolveRe
     st.final_residual = r.final_residual;
     st.converged = r.converged;
     st.solve_time_s = wall_s;
-    st.solver_used = solver;
+    // PipelinedFGMRESSolver reports FGMRES (pipelined_fgmres_solver.cpp:189)
+    st.solver_used = solver == HAMLSS_SOLVER_PIPELINED_FGMRES ? HAMLSS_SOLVER_FGMRES : solver;
     st.precond_used = P ? P->kind : HAMLSS_PREC_NONE;
     st.state_used = HAMLSS_STATE_EASY;
     st.restarts = r.restarts;
+    st.sstep_k = r.sstep_k;
+    st.comm_bytes = r.comm_events;   // the reference counts one event per Gram reduction
     long long fl = 0, by = 0;
-    if (solver == HAMLSS_SOLVER_CG) cg_cost(n, nnz, r, &fl, &by);
+    if (r.flops >= 0) { fl = r.flops; by = r.bytes; }
+    else if (solver == HAMLSS_SOLVER_CG) cg_cost(n, nnz, r, &fl, &by);
     else fgmres_cost(n, nnz, r, &fl, &by);
     st.flop_count = fl;
     st.mem_bytes = by;
@@ -597,7 +607,8 @@ int hamlss_solve(hamlss_ctx* ctx, int solver, const hamlss_mat* A, const hamlss_
         hamlss_params p;
         if (params) p = *params; else hamlss_params_default(&p);
         if (solver == HAMLSS_SOLVER_BICGSTAB) solver = HAMLSS_SOLVER_FGMRES;  // solver_factory.cpp:34-37
-        if (solver != HAMLSS_SOLVER_CG && solver != HAMLSS_SOLVER_FGMRES)
+        if (solver != HAMLSS_SOLVER_CG && solver != HAMLSS_SOLVER_FGMRES &&
+            solver != HAMLSS_SOLVER_SSTEP_CG && solver != HAMLSS_SOLVER_PIPELINED_FGMRES)
             return set_err(HAMLSS_ERR_INVALID, "solver type not provided by the engine");
         Ctx& c = ctx->c;
         HAMLSS_CUDA(cudaSetDevice(c.device));

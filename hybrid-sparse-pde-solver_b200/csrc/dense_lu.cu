@@ -430,6 +430,8 @@ void dense_lu_inverse(Ctx& ctx, int n, double* M, double* Minv, int* piv) {
     HAMLSS_CUDA(cudaStreamSynchronize(s));
 }
 
+void* blas_stream_handle(Ctx& ctx) { return blas_of(ctx); }
+
 void blas_destroy(void* h) {
     if (h) cublasDestroy(static_cast<cublasHandle_t>(h));
 }

@@ -13,5 +13,8 @@ void dense_lu_inverse(Ctx& ctx, int n, double* M, double* Minv, int* piv);
 
 // Release a context's cuBLAS handle (Ctx::blas).
 void blas_destroy(void* handle);
+// The context's cuBLAS handle (a cublasHandle_t, created on first use), bound to the
+// context's stream.
+void* blas_stream_handle(Ctx& ctx);
 
 }  // namespace hamlss

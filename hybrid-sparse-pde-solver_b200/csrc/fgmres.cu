@@ -27,7 +27,7 @@ constexpr double kEps = 2.220446049250313e-16;
 
 struct GmState {
     double bnorm, tol_abs, beta, res, inv_beta, hn_inv, hn;
-    int jcount, halt, status, m, iter_base;
+    int jcount, halt, status, m, iter_base, pipelined;
     LadderDev lad;
 };
 
@@ -183,6 +183,9 @@ struct FinNorm {
         s->hn = hn;
         a.H[(j + 1) * m + j] = hn;
         s->hn_inv = (hn > kEps) ? 1.0 / hn : 0.0;
+        // PipelinedFGMRESSolver leaves the cycle on a lucky breakdown before rotating
+        // column j (pipelined_fgmres_solver.cpp:117-123)
+        if (s->pipelined && !(hn > kEps)) { s->jcount = j + 1; s->halt = 1; return; }
         for (int i = 0; i < j; ++i) rot(a.H[i * m + j], a.H[(i + 1) * m + j], a.cs[i], a.sn[i]);
         double r;
         givens(a.H[j * m + j], a.H[(j + 1) * m + j], a.cs[j], a.sn[j], r);
@@ -266,7 +269,7 @@ void launch_mdot(Ctx& ctx, int mode, int n, int nv, const double* V, long long l
 
 SolveResult fgmres_solve(Ctx& ctx, hamlss_mat* A, Prec* M, const double* b, double* x,
                          double tol, int max_iter, int restart, Workspace& ws,
-                         const LadderCfg* lad) {
+                         const LadderCfg* lad, bool pipelined) {
     const int n = A->A.n;
     const int m = std::max(1, std::min(restart, n));
     if (m > 63) fail(HAMLSS_ERR_INVALID, "FGMRES restart length above 63 is not supported");
@@ -295,6 +298,7 @@ SolveResult fgmres_solve(Ctx& ctx, hamlss_mat* A, Prec* M, const double* b, doub
     GmState* s = reinterpret_cast<GmState*>(ws.state.p);
     GmState h0{};
     h0.m = m;
+    h0.pipelined = pipelined ? 1 : 0;
     h0.lad = ladder_init(lad);
     HAMLSS_CUDA(cudaMemcpyAsync(s, &h0, sizeof(h0), cudaMemcpyHostToDevice, st));
     HAMLSS_CUDA(cudaEventRecord(ctx.ev0, st));
@@ -313,6 +317,7 @@ SolveResult fgmres_solve(Ctx& ctx, hamlss_mat* A, Prec* M, const double* b, doub
     if (h.bnorm < kEps) {           // fgmres_solver.cpp:179-183
         res.converged = 1;
         res.final_residual = 0.0;
+        if (pipelined) res.flops = res.bytes = 0;
         return res;
     }
     int total = 0, cycles = 0;
@@ -370,6 +375,14 @@ SolveResult fgmres_solve(Ctx& ctx, hamlss_mat* A, Prec* M, const double* b, doub
     res.iterations = total;
     res.restarts = cycles - 1;                     // fgmres_solver.cpp:231
     res.initial_residual = 0.0;
+    if (pipelined) {
+        // (inner steps + 1 primer) SpMVs per cycle plus 4n per step
+        // (pipelined_fgmres_solver.cpp:207-212)
+        const long long nn = n, nz = A->A.nnz;
+        const long long spmv = (long long)total + cycles;
+        res.flops = spmv * 2 * nz + (long long)total * 4 * nn;
+        res.bytes = spmv * ((nn + 1 + nz) * 4 + nz * 8 + nn * 16) + (long long)total * 4 * nn * 8;
+    }
     return res;
 }
 

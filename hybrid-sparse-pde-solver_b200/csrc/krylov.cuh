@@ -19,6 +19,10 @@ struct SolveResult {
     double final_residual = 0.0;
     double device_time_s = 0.0;
     int escalate = 0;         // ESC_* when the device-side ladder test stopped the solve
+    // set by solvers whose cost model is not the CG / FGMRES one (else left at -1)
+    long long flops = -1, bytes = -1;
+    int sstep_k = 0;          // s-step batch size (SStepCGSolver)
+    long long comm_events = 0;
 };
 
 // CGSolver::solve (cg_solver.cpp:37-191) on device vectors.  T = double runs the FP64
@@ -29,9 +33,21 @@ SolveResult cg_solve(Ctx& ctx, hamlss_mat* A, Prec* M, const T* b, T* x, double 
                      int max_iter, int check_every, Workspace& ws, const LadderCfg* lad = nullptr);
 
 // FGMRESSolver::solve (fgmres_solver.cpp:165-241) with CGS2 Arnoldi; FP64.
+// pipelined = true: PipelinedFGMRESSolver (pipelined_fgmres_solver.cpp:69-242), the same
+// Arnoldi process with that solver's lucky-breakdown exit and cost model.
 SolveResult fgmres_solve(Ctx& ctx, hamlss_mat* A, Prec* M, const double* b, double* x,
                          double tol, int max_iter, int restart, Workspace& ws,
-                         const LadderCfg* lad = nullptr);
+                         const LadderCfg* lad = nullptr, bool pipelined = false);
+
+// SStepCGSolver::solve (sstep_cg_solver.cpp:170-305): batches of k Newton-Chebyshev basis
+// vectors, one Gram matrix per batch, a k x k Cholesky solve, x += B y, and the true
+// residual.  k = params.sstep_k; the preconditioner is not applied (as in the reference).
+SolveResult sstep_solve(Ctx& ctx, hamlss_mat* A, const double* b, double* x,
+                        const hamlss_params& p, Workspace& ws);
+
+// SparseMatrix::spectral_interval(steps) (sparse_matrix.cpp:451-479): Lanczos from the
+// uniform vector, Gershgorin bounds of the tridiagonal.
+void spectral_interval(Ctx& ctx, hamlss_mat* A, int steps, double* lo, double* hi);
 
 // Mixed precision: FP64 iterative refinement around an FP32 inner PCG / FGMRES.
 SolveResult mixed_solve(Ctx& ctx, int solver, hamlss_mat* A, Prec* M, const double* b,

@@ -20,6 +20,7 @@ import numpy as np
 
 from . import _abi
 from ._abi import (DEVICE, HOST, PREC_AMG, PREC_ILU, PREC_JACOBI, PREC_NONE, SOLVER_CG,
+                   SOLVER_PIPELINED_FGMRES, SOLVER_SSTEP_CG,
                    SOLVER_FGMRES, STATE_EASY, STATE_HARD, STATE_MODERATE, Escalation, Params,
                    Stats, default_params, lib)
 from . import problems
@@ -408,6 +409,35 @@ class FGMRESSolver(SolverBase):
     solver_type = SOLVER_FGMRES
 
 
+class PipelinedFGMRESSolver(SolverBase):
+    """PipelinedFGMRESSolver (pipelined_fgmres_solver.hpp:44-74): FGMRES(m) whose cycle
+    forms A M^-1 v_{j+1} one step early; same Arnoldi values, its own lucky-breakdown exit
+    and cost model (pipelined_fgmres_solver.cpp:69-242).  Reports FGMRES as solver_used."""
+
+    solver_type = SOLVER_PIPELINED_FGMRES
+
+
+class SStepCGSolver(SolverBase):
+    """SStepCGSolver(k) (sstep_cg_solver.hpp:57-60, sstep_cg_solver.cpp:170-305): batches
+    of k Newton-Chebyshev basis vectors, one Gram matrix per batch.  The preconditioner is
+    recorded in the stats but not applied, as in the reference."""
+
+    solver_type = SOLVER_SSTEP_CG
+
+    def __init__(self, k: int = 4):
+        super().__init__()
+        self.k = k
+
+    def solve(self, A, b, x, stats=None) -> bool:
+        saved = self._params                     # the constructor's k wins over params
+        self._params = Params.from_buffer_copy(saved)
+        self._params.sstep_k = self.k
+        try:
+            return super().solve(A, b, x, stats)
+        finally:
+            self._params = saved
+
+
 _SOLVER_NAMES = {"CG": 0, "FGMRES": 1, "BICGSTAB": 2, "SSTEP_CG": 3, "SSTEP": 3, "S-STEP": 3,
                  "ASYNC_FGMRES": 4, "ASYNC": 4}
 _PREC_NAMES = {"NONE": 0, "IDENTITY": 0, "JACOBI": 1, "DIAG": 1, "ILU": 2, "ILU0": 2, "AMG": 3}
@@ -436,6 +466,8 @@ class SolverFactory:
             s = CGSolver()
         elif solver_type in (SOLVER_FGMRES, 2):
             s = FGMRESSolver()
+        elif solver_type == SOLVER_SSTEP_CG:
+            s = SStepCGSolver(params.sstep_k)    # solver_factory.cpp:38-40
         else:
             raise ValueError("SolverFactory: solver type not provided by the engine")
         s.set_params(params)

@@ -31,6 +31,7 @@ HOST, DEVICE = 0, 1
 
 # hsps::SolverType / PrecondType / AdaptiveState values (include/core/types.hpp:30-54)
 SOLVER_CG, SOLVER_FGMRES, SOLVER_BICGSTAB, SOLVER_SSTEP_CG, SOLVER_ASYNC_FGMRES = range(5)
+SOLVER_PIPELINED_FGMRES = 5          # engine value (PipelinedFGMRESSolver has no SolverType)
 PREC_NONE, PREC_JACOBI, PREC_ILU, PREC_AMG, PREC_BLOCK_JACOBI, PREC_CHEBYSHEV = range(6)
 STATE_EASY, STATE_MODERATE, STATE_HARD = range(3)
 FP64, MIXED = 0, 1

@@ -55,7 +55,10 @@ enum { HAMLSS_HOST = 0, HAMLSS_DEVICE = 1 };
 /* Same numeric values as hsps::SolverType / PrecondType / AdaptiveState
  * (include/core/types.hpp:30-54). */
 enum { HAMLSS_SOLVER_CG = 0, HAMLSS_SOLVER_FGMRES = 1, HAMLSS_SOLVER_BICGSTAB = 2,
-       HAMLSS_SOLVER_SSTEP_CG = 3, HAMLSS_SOLVER_ASYNC_FGMRES = 4 };
+       HAMLSS_SOLVER_SSTEP_CG = 3, HAMLSS_SOLVER_ASYNC_FGMRES = 4,
+       /* engine value: PipelinedFGMRESSolver (include/solvers/pipelined_fgmres_solver.hpp),
+        * which has no SolverType of its own and reports FGMRES */
+       HAMLSS_SOLVER_PIPELINED_FGMRES = 5 };
 enum { HAMLSS_PREC_NONE = 0, HAMLSS_PREC_JACOBI = 1, HAMLSS_PREC_ILU = 2, HAMLSS_PREC_AMG = 3,
        HAMLSS_PREC_BLOCK_JACOBI = 4, HAMLSS_PREC_CHEBYSHEV = 5 };
 enum { HAMLSS_STATE_EASY = 0, HAMLSS_STATE_MODERATE = 1, HAMLSS_STATE_HARD = 2 };
@@ -234,9 +237,13 @@ int hamlss_precond_type(const hamlss_prec* M, int32_t* kind);
 int hamlss_precond_release(hamlss_prec* M);
 
 /* --------------------------------------------------------------------- solve
- * Replaces SolverBase::solve (solver_base.hpp:32-35) for CGSolver (cg_solver.cpp:37-191)
- * and FGMRESSolver (fgmres_solver.cpp:165-241).  x holds the initial guess on entry
- * and the solution on exit.  M may be NULL (no preconditioner). */
+ * Replaces SolverBase::solve (solver_base.hpp:32-35) for CGSolver (cg_solver.cpp:37-191),
+ * FGMRESSolver (fgmres_solver.cpp:165-241), PipelinedFGMRESSolver
+ * (pipelined_fgmres_solver.cpp:69-242; HAMLSS_SOLVER_PIPELINED_FGMRES) and SStepCGSolver
+ * (sstep_cg_solver.cpp:170-305; HAMLSS_SOLVER_SSTEP_CG, batch size params->sstep_k in
+ * [1, 32], FP64 whatever params->precision says, M recorded but not applied as in the
+ * reference).  x holds the initial guess on entry and the solution on exit.  M may be
+ * NULL (no preconditioner). */
 int hamlss_solve(hamlss_ctx* ctx, int solver, const hamlss_mat* A, const hamlss_prec* M,
                  const double* b, double* x, int where, const hamlss_params* params,
                  hamlss_stats* stats);

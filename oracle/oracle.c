@@ -906,7 +906,7 @@ static void rot(double* dx, double* dy, double cs, double sn) {
 /* fgmres_cycle (fgmres_solver.cpp:72-160); H is (m+1) x m row-major. */
 static int fgmres_cycle(int32_t n, const int32_t* rp, const int32_t* ci, const double* v,
                         const orc_prec* M, const double* b, double* x, double tol_abs, int m,
-                        double* res_norm, int* rc) {
+                        double* res_norm, int* rc, int pipelined) {
     size_t sz = sizeof(double) * (size_t)(n > 0 ? n : 1);
     double* r = (double*)malloc(sz);
     orc_spmv(n, rp, ci, v, x, r);
@@ -943,6 +943,11 @@ static int fgmres_cycle(int32_t n, const int32_t* rp, const int32_t* ci, const d
             double* vn = V + (size_t)(j + 1) * n;
             double s = 1.0 / HH(j + 1, j);
             for (int32_t t = 0; t < n; ++t) vn[t] = w[t] * s;
+        } else if (pipelined) {
+            /* pipeline_cycle leaves on a lucky breakdown before rotating column j
+             * (pipelined_fgmres_solver.cpp:117-123) */
+            ++j;
+            break;
         }
         for (int i = 0; i < j; ++i) rot(&HH(i, j), &HH(i + 1, j), cs[i], sn[i]);
         double rv;
@@ -969,10 +974,13 @@ static int fgmres_cycle(int32_t n, const int32_t* rp, const int32_t* ci, const d
     return j;
 }
 
-/* FGMRESSolver::solve (fgmres_solver.cpp:165-241). */
-int orc_fgmres(int32_t n, const int32_t* rp, const int32_t* ci, const double* v,
-               const orc_prec* M, const double* b, double* x, const hamlss_params* p,
-               hamlss_stats* st) {
+/* FGMRESSolver::solve (fgmres_solver.cpp:165-241), or with pipelined = 1
+ * PipelinedFGMRESSolver::solve (pipelined_fgmres_solver.cpp:168-242): the same Arnoldi
+ * values (the pipelined cycle computes A M^-1 v_{j+1} one step early), its lucky-breakdown
+ * exit, and its cost model of (steps + 1) SpMVs per cycle. */
+static int fgmres_impl(int32_t n, const int32_t* rp, const int32_t* ci, const double* v,
+                       const orc_prec* M, const double* b, double* x, const hamlss_params* p,
+                       hamlss_stats* st, int pipelined) {
     double t0 = now_s();
     const int32_t nz = rp[n];
     const int m = p->restart_size < n ? p->restart_size : n;
@@ -988,9 +996,10 @@ int orc_fgmres(int32_t n, const int32_t* rp, const int32_t* ci, const double* v,
     while (total < p->max_iter && rc == HAMLSS_OK) {
         int remaining = p->max_iter - total;
         int cm = m < remaining ? m : remaining;
-        int it = fgmres_cycle(n, rp, ci, v, M, b, x, tol_abs, cm, &res, &rc);
-        flops += (int64_t)it * (spmv_flops(nz) + 4LL * n);
-        bytes += (int64_t)it * (spmv_bytes(n, nz) + 32LL * n);
+        int it = fgmres_cycle(n, rp, ci, v, M, b, x, tol_abs, cm, &res, &rc, pipelined);
+        const int64_t nspmv = it + (pipelined ? 1 : 0);
+        flops += nspmv * spmv_flops(nz) + (int64_t)it * 4LL * n;
+        bytes += nspmv * spmv_bytes(n, nz) + (int64_t)it * 32LL * n;
         total += it;
         ++restarts;
         double rel = res / bn;
@@ -1003,6 +1012,197 @@ int orc_fgmres(int32_t n, const int32_t* rp, const int32_t* ci, const double* v,
     st->mem_bytes = bytes;
     st->energy_joules = 2.0e-10 * (double)flops + 5.0e-9 * (double)bytes;
     if (rc != HAMLSS_OK) return rc;
+    return st->converged;
+}
+
+int orc_fgmres(int32_t n, const int32_t* rp, const int32_t* ci, const double* v,
+               const orc_prec* M, const double* b, double* x, const hamlss_params* p,
+               hamlss_stats* st) {
+    return fgmres_impl(n, rp, ci, v, M, b, x, p, st, 0);
+}
+
+int orc_pipelined_fgmres(int32_t n, const int32_t* rp, const int32_t* ci, const double* v,
+                         const orc_prec* M, const double* b, double* x, const hamlss_params* p,
+                         hamlss_stats* st) {
+    return fgmres_impl(n, rp, ci, v, M, b, x, p, st, 1);
+}
+
+/* ============================================================================ s-step */
+
+/* SparseMatrix::spectral_interval (sparse_matrix.cpp:451-479). */
+void orc_spectral_interval(int32_t n, const int32_t* rp, const int32_t* ci, const double* v,
+                           int steps, double* lo, double* hi) {
+    const int K = n < steps ? n : steps;
+    size_t sz = sizeof(double) * (size_t)(n > 0 ? n : 1);
+    double *q = (double*)malloc(sz), *qp = (double*)calloc((size_t)(n > 0 ? n : 1), sizeof(double));
+    double* Aq = (double*)malloc(sz);
+    double alpha[64], beta[64];
+    int na = 0, nb = 0;
+    const double inv_sq_n = 1.0 / sqrt((double)n);
+    for (int32_t i = 0; i < n; ++i) q[i] = inv_sq_n;
+    double bj = 0.0;
+    for (int j = 0; j < K && j < 64; ++j) {
+        orc_spmv(n, rp, ci, v, q, Aq);
+        const double aj = orc_dot(n, q, Aq);
+        alpha[na++] = aj;
+        for (int32_t i = 0; i < n; ++i) Aq[i] -= aj * q[i] + bj * qp[i];
+        bj = orc_norm2(n, Aq);
+        if (bj < REAL_EPS * 1e6) break;
+        beta[nb++] = bj;
+        memcpy(qp, q, sz);
+        memcpy(q, Aq, sz);
+        const double s = 1.0 / bj;
+        for (int32_t i = 0; i < n; ++i) q[i] *= s;
+    }
+    double tmin = alpha[0], tmax = alpha[0];
+    for (int i = 0; i < na; ++i) {
+        double r = 0.0;
+        if (i > 0) r += fabs(beta[i - 1]);
+        if (i < na - 1) r += fabs(beta[i]);
+        tmin = dmin(tmin, alpha[i] - r);
+        tmax = dmax(tmax, alpha[i] + r);
+    }
+    *lo = tmin;
+    *hi = tmax;
+    free(q); free(qp); free(Aq);
+}
+
+/* build_basis (sstep_cg_solver.cpp:44-66) into B (k columns of n) and gram_matrix (:71-80). */
+static void sstep_basis(int32_t n, const int32_t* rp, const int32_t* ci, const double* v,
+                        const double* r, double lam_min, double lam_max, int k, double* B,
+                        double* tmp, double* G) {
+    double shifts[64];
+    const double c = 0.5 * (lam_min + lam_max), h = 0.5 * (lam_max - lam_min);
+    for (int j = 0; j < k; ++j) shifts[j] = c + h * cos(3.14159265358979323846 * (2.0 * j + 1.0) / (2.0 * k));  /* M_PI */
+    size_t sz = sizeof(double) * (size_t)n;
+    memcpy(B, r, sz);
+    const double n0 = orc_norm2(n, B);
+    if (n0 > REAL_EPS) { const double s = 1.0 / n0; for (int32_t i = 0; i < n; ++i) B[i] *= s; }
+    for (int j = 1; j < k; ++j) {
+        double* prev = B + (size_t)(j - 1) * n;
+        double* cur = B + (size_t)j * n;
+        orc_spmv(n, rp, ci, v, prev, tmp);
+        memcpy(cur, tmp, sz);
+        const double a = -shifts[j - 1];
+        for (int32_t i = 0; i < n; ++i) cur[i] += a * prev[i];
+        const double nj = orc_norm2(n, cur);
+        if (nj > REAL_EPS) { const double s = 1.0 / nj; for (int32_t i = 0; i < n; ++i) cur[i] *= s; }
+    }
+    for (int i = 0; i < k; ++i)
+        for (int j = i; j < k; ++j) {
+            G[i * k + j] = orc_dot(n, B + (size_t)i * n, B + (size_t)j * n);
+            G[j * k + i] = G[i * k + j];
+        }
+}
+
+/* SStepCGSolver::solve (sstep_cg_solver.cpp:170-305) with gram_condition_estimate
+ * (:108-119) and local_lstsq (:125-164).  The preconditioner is not applied. */
+int orc_sstep_cg(int32_t n, const int32_t* rp, const int32_t* ci, const double* v,
+                 const orc_prec* M, const double* b, double* x, const hamlss_params* p,
+                 hamlss_stats* st) {
+    double t0 = now_s();
+    const int32_t nz = rp[n];
+    if (p->sstep_k < 1 || p->sstep_k > 32) return HAMLSS_ERR_INVALID;
+    int k = p->sstep_k;
+    const int kcap = n / 10 > 1 ? n / 10 : 1;
+    if (kcap < k) k = kcap;
+    double lo, hi;
+    orc_spectral_interval(n, rp, ci, v, 20, &lo, &hi);
+    const double lam_min = dmax(lo, REAL_EPS);
+    const double lam_max = dmax(hi, lam_min * 2.0);
+    size_t sz = sizeof(double) * (size_t)(n > 0 ? n : 1);
+    double* r = (double*)malloc(sz);
+    orc_spmv(n, rp, ci, v, x, r);
+    for (int32_t i = 0; i < n; ++i) r[i] = b[i] - r[i];
+    const double bn = orc_norm2(n, b);
+    double rn = orc_norm2(n, r);
+    st->initial_residual = rn;
+    if (bn < REAL_EPS) { st->converged = 1; st->final_residual = 0.0; free(r); return 1; }
+    double rel = rn / bn;
+    if (rel < p->tol) { st->converged = 1; st->final_residual = rel; free(r); return 1; }
+    st->solver_used = HAMLSS_SOLVER_SSTEP_CG;
+    st->precond_used = M ? M->kind : HAMLSS_PREC_NONE;
+    st->sstep_k = k;
+    double* B = (double*)malloc(sz * (size_t)k);
+    double* tmp = (double*)malloc(sz);
+    double* Ap = (double*)malloc(sz);
+    double G[32 * 32], L[32 * 32], rhs[32], z[32], y[32];
+    int64_t flops = 0, bytes = 0;
+    int total = 0;
+    while (total < p->max_iter && rel > p->tol) {
+        int kb = k;
+        sstep_basis(n, rp, ci, v, r, lam_min, lam_max, kb, B, tmp, G);
+        flops += (int64_t)kb * spmv_flops(nz);
+        bytes += (int64_t)kb * spmv_bytes(n, nz);
+        double mx = 0.0, mn = INFINITY;
+        for (int i = 0; i < kb; ++i) {
+            const double d = fabs(G[i * kb + i]);
+            mx = dmax(mx, d);
+            if (d > REAL_EPS) mn = dmin(mn, d);
+        }
+        const double cond = (mn >= mx) ? 1.0 : mx / mn;
+        if (cond > p->sstep_cond_tol && kb > 1) {
+            kb = kb / 2 > 1 ? kb / 2 : 1;
+            sstep_basis(n, rp, ci, v, r, lam_min, lam_max, kb, B, tmp, G);
+        }
+        st->comm_bytes += 1;
+        for (int i = 0; i < kb; ++i) rhs[i] = orc_dot(n, r, B + (size_t)i * n);
+        flops += (int64_t)kb * 2LL * n;
+        int ok = 1;
+        for (int i = 0; i < kb && ok; ++i)
+            for (int j = 0; j <= i; ++j) {
+                double s = G[i * kb + j];
+                for (int l = 0; l < j; ++l) s -= L[i * kb + l] * L[j * kb + l];
+                if (i == j) {
+                    if (s <= 0.0) { ok = 0; break; }
+                    L[i * kb + j] = sqrt(s);
+                } else {
+                    L[i * kb + j] = s / L[j * kb + j];
+                }
+            }
+        if (!ok) {
+            /* one steepest-descent step (:236-250) */
+            orc_spmv(n, rp, ci, v, r, Ap);
+            const double rr = orc_dot(n, r, r), rAp = orc_dot(n, r, Ap);
+            if (fabs(rAp) > REAL_EPS) {
+                const double alpha = rr / rAp;
+                for (int32_t i = 0; i < n; ++i) x[i] += alpha * r[i];
+                for (int32_t i = 0; i < n; ++i) r[i] += -alpha * Ap[i];
+            }
+            ++total;
+            rel = orc_norm2(n, r) / bn;
+            continue;
+        }
+        for (int i = 0; i < kb; ++i) {
+            double s = rhs[i];
+            for (int j = 0; j < i; ++j) s -= L[i * kb + j] * z[j];
+            z[i] = s / L[i * kb + i];
+        }
+        for (int i = kb - 1; i >= 0; --i) {
+            double s = z[i];
+            for (int j = i + 1; j < kb; ++j) s -= L[j * kb + i] * y[j];
+            y[i] = s / L[i * kb + i];
+        }
+        for (int i = 0; i < kb; ++i) {
+            const double* Bi = B + (size_t)i * n;
+            for (int32_t t = 0; t < n; ++t) x[t] += y[i] * Bi[t];
+        }
+        orc_spmv(n, rp, ci, v, x, r);
+        flops += spmv_flops(nz);
+        bytes += spmv_bytes(n, nz);
+        for (int32_t i = 0; i < n; ++i) r[i] = b[i] - r[i];
+        rn = orc_norm2(n, r);
+        rel = rn / bn;
+        total += kb;
+    }
+    st->iterations = total;
+    st->final_residual = rel;
+    st->converged = rel < p->tol;
+    st->solve_time_s = now_s() - t0;
+    st->flop_count = flops;
+    st->mem_bytes = bytes;
+    st->energy_joules = 2e-10 * (double)flops + 5e-9 * (double)bytes;
+    free(r); free(B); free(tmp); free(Ap);
     return st->converged;
 }
 

@@ -76,6 +76,14 @@ int orc_cg(int32_t n, const int32_t* rp, const int32_t* ci, const double* v,
 int orc_fgmres(int32_t n, const int32_t* rp, const int32_t* ci, const double* v,
                const orc_prec* M, const double* b, double* x, const hamlss_params* p,
                hamlss_stats* st);
+int  orc_pipelined_fgmres(int32_t n, const int32_t* rp, const int32_t* ci, const double* v,
+                          const orc_prec* M, const double* b, double* x,
+                          const hamlss_params* p, hamlss_stats* st);
+int  orc_sstep_cg(int32_t n, const int32_t* rp, const int32_t* ci, const double* v,
+                  const orc_prec* M, const double* b, double* x, const hamlss_params* p,
+                  hamlss_stats* st);
+void orc_spectral_interval(int32_t n, const int32_t* rp, const int32_t* ci, const double* v,
+                           int steps, double* lo, double* hi);
 
 /* ---- adaptive selector (adaptive_selector.cpp:37-394) ---- */
 int orc_extract_features(int32_t n, const int32_t* rp, const int32_t* ci, const double* v,

@@ -86,8 +86,9 @@ class Oracle:
         L.orc_prec_setup.argtypes = [C.c_int, I32, V, V, V, C.POINTER(Params), C.POINTER(C.c_int)]
         L.orc_prec_free.argtypes = [V]
         L.orc_prec_apply.argtypes = [V, V, V]
-        for f in (L.orc_cg, L.orc_fgmres):
+        for f in (L.orc_cg, L.orc_fgmres, L.orc_pipelined_fgmres, L.orc_sstep_cg):
             f.argtypes = [I32, V, V, V, V, V, V, C.POINTER(Params), C.POINTER(Stats)]
+        L.orc_spectral_interval.argtypes = [I32, V, V, V, C.c_int, C.POINTER(D), C.POINTER(D)]
         L.orc_extract_features.argtypes = [I32, V, V, V, V, pi]
         L.orc_solve_adaptive.argtypes = [I32, V, V, V, V, V, C.POINTER(Params), C.POINTER(Stats),
                                          C.POINTER(Escalation), I32, pi, pi]
@@ -211,12 +212,20 @@ class Oracle:
         b = _c(b, _f64)
         x = np.zeros(A.n, _f64) if x0 is None else _c(x0, _f64).copy()
         s = Stats()
-        f = self.L.orc_cg if solver == 0 else self.L.orc_fgmres
+        # 0 CGSolver, 1 FGMRESSolver, 3 SStepCGSolver, 5 PipelinedFGMRESSolver
+        f = {0: self.L.orc_cg, 1: self.L.orc_fgmres, 2: self.L.orc_fgmres, 3: self.L.orc_sstep_cg,
+             5: self.L.orc_pipelined_fgmres}[solver]
         try:
             rc = f(*A.args(), M, _p(b), _p(x), C.byref(p), C.byref(s))
         finally:
             self.L.orc_prec_free(M)
         return rc, x, s
+
+    def spectral_interval(self, rp, ci, v, steps=20):
+        A = _Csr(rp, ci, v)
+        lo, hi = C.c_double(), C.c_double()
+        self.L.orc_spectral_interval(*A.args(), steps, C.byref(lo), C.byref(hi))
+        return lo.value, hi.value
 
     def features(self, rp, ci, v):
         A = _Csr(rp, ci, v)
@@ -282,6 +291,9 @@ class Reference:
         L.ref_spmv.argtypes = [I32, V, V, V, V, V]
         L.ref_dot.restype = D
         L.ref_dot.argtypes = [I32, V, V]
+        L.ref_pipelined_solve.argtypes = [C.c_int, I32, V, V, V, V, V, C.POINTER(Params),
+                                          C.POINTER(Stats)]
+        L.ref_spectral_interval.argtypes = [I32, V, V, V, C.c_int, C.POINTER(D), C.POINTER(D)]
         L.ref_solve.argtypes = [C.c_int, C.c_int, I32, V, V, V, V, V, C.POINTER(Params),
                                 C.POINTER(Stats)]
         L.ref_precond_apply.argtypes = [C.c_int, I32, V, V, V, C.POINTER(Params), V, V]
@@ -345,8 +357,17 @@ class Reference:
         b = _c(b, _f64)
         x = np.zeros(A.n, _f64) if x0 is None else _c(x0, _f64).copy()
         s = Stats()
-        rc = self.L.ref_solve(solver, precond, *A.args(), _p(b), _p(x), C.byref(p), C.byref(s))
+        if solver == 5:        # PipelinedFGMRESSolver, built directly (no SolverType)
+            rc = self.L.ref_pipelined_solve(precond, *A.args(), _p(b), _p(x), C.byref(p), C.byref(s))
+        else:
+            rc = self.L.ref_solve(solver, precond, *A.args(), _p(b), _p(x), C.byref(p), C.byref(s))
         return rc, x, s
+
+    def spectral_interval(self, rp, ci, v, steps=20):
+        A = _Csr(rp, ci, v)
+        lo, hi = C.c_double(), C.c_double()
+        self.L.ref_spectral_interval(*A.args(), steps, C.byref(lo), C.byref(hi))
+        return lo.value, hi.value
 
     def precond_apply(self, kind, rp, ci, v, r, params=None):
         A = _Csr(rp, ci, v)

@@ -24,6 +24,7 @@
 #include "solvers/solver_base.hpp"
 #include "solvers/cg_solver.hpp"
 #include "solvers/fgmres_solver.hpp"
+#include "solvers/pipelined_fgmres_solver.hpp"
 #include "preconditioners/jacobi.hpp"
 #define private public
 #define protected public
@@ -62,7 +63,12 @@ SolverParams to_params(const hamlss_params* p) {
     s.stall_threshold = p->stall_threshold;
     s.verbose = false;
     s.print_every = p->print_every;
+    s.sstep_k = p->sstep_k;
+    s.sstep_cond_tol = p->sstep_cond_tol;
+    s.async_enabled = p->async_enabled != 0;
+    s.async_max_stale = p->async_max_stale;
     s.fill_per_row = p->fill_per_row;
+    s.block_size = p->block_size;
     return s;
 }
 
@@ -81,6 +87,10 @@ void from_stats(const SolverStats& s, hamlss_stats* o) {
     o->precond_used = static_cast<int32_t>(s.precond_used);
     o->state_used = static_cast<int32_t>(s.state_used);
     o->restarts = s.restarts;
+    o->sstep_k = s.sstep_k;
+    o->async_mode = s.async_mode ? 1 : 0;
+    o->comm_bytes = s.comm_bytes;
+    o->comm_time_s = s.comm_time_s;
 }
 
 int map_error(const std::exception& e) {
@@ -163,6 +173,37 @@ int ref_solve(int solver, int precond, int32_t n, const int32_t* rp, const int32
     } catch (const std::exception& e) {
         return map_error(e);
     }
+}
+
+// PipelinedFGMRESSolver (no SolverType of its own): make_precond(precond), then solve.
+int ref_pipelined_solve(int precond, int32_t n, const int32_t* rp, const int32_t* ci,
+                        const double* v, const double* b, double* x, const hamlss_params* p,
+                        hamlss_stats* st) {
+    try {
+        SparseMatrix A = make_csr(n, rp, ci, v);
+        SolverParams sp = to_params(p);
+        auto M = SolverFactory::make_precond(static_cast<PrecondType>(precond), A, sp);
+        PipelinedFGMRESSolver s;
+        s.set_params(sp);
+        s.set_preconditioner(M);
+        Vector bv(std::vector<Real>(b, b + n)), xv(std::vector<Real>(x, x + n));
+        SolverStats out;
+        bool ok = s.solve(A, bv, xv, out);
+        std::memcpy(x, xv.data(), sizeof(double) * n);
+        from_stats(out, st);
+        return ok ? 1 : 0;
+    } catch (const std::exception& e) {
+        return map_error(e);
+    }
+}
+
+// SparseMatrix::spectral_interval(steps).
+void ref_spectral_interval(int32_t n, const int32_t* rp, const int32_t* ci, const double* v,
+                           int steps, double* lo, double* hi) {
+    SparseMatrix A = make_csr(n, rp, ci, v);
+    auto pr = A.spectral_interval(steps);
+    *lo = pr.first;
+    *hi = pr.second;
 }
 
 // make_precond(kind, A, params) then apply(r, z).

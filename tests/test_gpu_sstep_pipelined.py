@@ -1,0 +1,183 @@
+"""SStepCGSolver and PipelinedFGMRESSolver on the device against the oracle / reference
+(-m gpu).
+
+s-step: the device builds the same Newton-Chebyshev basis, Gram matrix and Cholesky
+update as the reference (sstep_cg_solver.cpp:170-305); its dot products are tree sums
+and its Gram matrix is one DGEMM, so values differ from the oracle in the last bits.
+Bar: the same outcome (converged, stagnated or diverged); for converged and stagnated
+runs with k <= 4 iteration counts within one batch (k), and for converged runs the true relative
+residual below 10 tol.  Divergent runs (most unscaled problems: the reference's update
+is a projected Richardson step) end, as the reference's do, when the residual stops
+being finite or max_iter is spent; their growth amplifies last-bit differences, so only
+the outcome is compared.
+
+Pipelined FGMRES: the device FGMRES (CGS2) with the pipelined cycle's lucky-breakdown
+exit and cost model.  Bar: iteration count +-1, restarts, converged flag, and the cost
+model of pipelined_fgmres_solver.cpp:207-212 for the device's own iteration counts.
+"""
+import numpy as np
+import pytest
+
+from gpu_util import need_gpu
+import hsps_b200 as H
+from hsps_b200 import problems as P
+from hsps_b200._abi import default_params
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _gpu():
+    need_gpu()
+
+
+def unit_diagonal(A):
+    rp, ci, v = A
+    n = len(rp) - 1
+    rows = np.repeat(np.arange(n), np.diff(rp))
+    s = 1.0 / np.sqrt(v[ci == rows])
+    return rp, ci, v * s[rows] * s[ci]
+
+
+def cases():
+    bx, by = P.convdiff_wind(24, 30.0)
+    base = [("poisson24", P.poisson_2d(24)), ("varkappa32", P.varkappa_poisson_2d(32, 1.0, 11)),
+            ("convdiff24", P.convection_diffusion_2d(24, 1.0, bx, by)),
+            ("helmholtz16", P.helmholtz_2d(16, 7.0))]
+    for name, A in base:
+        yield name, A
+        yield "unit_" + name, unit_diagonal(A)
+
+
+CASES = list(cases())
+IDS = [c[0] for c in CASES]
+
+
+def run(solver, A, b, p, prec=None):
+    n = len(A[0]) - 1
+    M = H.SparseMatrix(n, n, *A)
+    s = solver
+    s.set_params(p)
+    if prec is not None:
+        I = H.SolverFactory.make_precond(prec, M, p)
+        s.set_preconditioner(I)
+    x = np.zeros(n)
+    st = H.SolverStats()
+    ok = s.solve(M, b, x, st)
+    return ok, x, st
+
+
+@pytest.mark.parametrize("name,A", CASES, ids=IDS)
+@pytest.mark.parametrize("k", [1, 2, 4, 8])
+def test_sstep_matches_oracle(orc, name, A, k):
+    n = len(A[0]) - 1
+    b = P.rhs(n, 3)
+    p = default_params(tol=1e-8, max_iter=400, sstep_k=k)
+    rc, xo, so = orc.solve(3, 1, *A, b, params=p)
+    ok, x, st = run(H.SStepCGSolver(k), A, b, p, H.PREC_JACOBI)
+    assert ok == bool(so.converged), (st.iterations, so.iterations)
+    diverged = not np.isfinite(so.final_residual) or so.final_residual > 1.0
+    if not diverged and k <= 4:
+        # at k = 8 the Gram matrices of these problems are near-singular: whether a
+        # Cholesky succeeds (or falls back to a single step) flips with the last bits
+        assert abs(st.iterations - so.iterations) <= k, (st.iterations, so.iterations)
+    assert st.sstep_k == so.sstep_k == min(k, max(1, n // 10))
+    assert st.solver_used == H._abi.SOLVER_SSTEP_CG and st.precond_used == H.PREC_JACOBI
+    if so.converged:
+        r = b - orc.spmv(*A, x)
+        assert np.linalg.norm(r) / np.linalg.norm(b) < 10 * p.tol
+        assert st.comm_bytes == so.comm_bytes and st.flop_count == so.flop_count
+    elif diverged:
+        # diverged: the growth amplifies last-bit differences, so only the outcome compares
+        assert not np.isfinite(st.final_residual) or st.final_residual > 1.0
+    else:
+        # stagnated below 1 within max_iter: same order of magnitude
+        assert np.isfinite(st.final_residual) and st.final_residual > 0
+        assert abs(np.log10(st.final_residual / so.final_residual)) < 1.0
+
+
+def test_sstep_factory_and_trivial_rhs(orc):
+    A = H.SparseMatrix(256, 256, *unit_diagonal(P.helmholtz_2d(16, 7.0)))
+    p = default_params(tol=1e-8, max_iter=400, sstep_k=4)
+    s, M = H.SolverFactory.make("SSTEP_CG", "JACOBI", A, p)
+    assert isinstance(s, H.SStepCGSolver) and s.k == 4
+    st = H.SolverStats()
+    x = np.zeros(256)
+    assert s.solve(A, np.ones(256), x, st) and st.sstep_k == 4 and st.comm_bytes > 0
+    x = np.zeros(256)
+    st = H.SolverStats()
+    assert s.solve(A, np.zeros(256), x, st) and st.iterations == 0 and st.final_residual == 0.0
+    with pytest.raises(H.HamlssError):
+        H.SStepCGSolver(0).solve(A, np.ones(256), np.zeros(256))
+
+
+@pytest.mark.parametrize("name,A", CASES, ids=IDS)
+@pytest.mark.parametrize("prec", [H.PREC_NONE, H.PREC_JACOBI, H.PREC_ILU])
+def test_pipelined_fgmres_parity(orc, ref, name, A, prec):
+    n = len(A[0]) - 1
+    b = P.rhs(n, 13)
+    p = default_params(tol=1e-8, max_iter=400, restart_size=20, drop_tol=0.0)
+    rc, xr, sr = ref.solve(5, prec, *A, b, params=p)
+    ok, x, st = run(H.PipelinedFGMRESSolver(), A, b, p, prec)
+    assert ok == bool(sr.converged), (st.iterations, sr.iterations)
+    assert abs(st.iterations - sr.iterations) <= 1, (st.iterations, sr.iterations)
+    assert st.solver_used == H._abi.SOLVER_FGMRES
+    nz = len(A[1])
+    cycles = st.restarts + 1
+    spmv = st.iterations + cycles
+    assert st.flop_count == spmv * 2 * nz + st.iterations * 4 * n
+    assert st.mem_bytes == spmv * ((n + 1 + nz) * 4 + nz * 8 + n * 16) + st.iterations * 32 * n
+    if sr.converged:
+        r = b - orc.spmv(*A, x)
+        assert np.linalg.norm(r) / np.linalg.norm(b) < 10 * p.tol
+        if st.iterations == sr.iterations:
+            assert st.restarts == sr.restarts and st.flop_count == sr.flop_count
+
+
+def test_pipelined_fgmres_kats(orc):
+    # test_improvements.cpp:240-290
+    p = default_params(tol=1e-8, max_iter=3000, restart_size=50)
+    A = H.SparseMatrix.poisson_2d(16)
+    s = H.PipelinedFGMRESSolver()
+    s.set_params(p)
+    I = H.ILUPreconditioner()
+    I.setup(A)
+    s.set_preconditioner(I)
+    x = np.zeros(256)
+    assert s.solve(A, np.ones(256), x)
+    assert np.linalg.norm(np.ones(256) - A.spmv(x)) / 16.0 < 1e-7
+    A = H.SparseMatrix.poisson_2d(12)
+    xs, xp = np.zeros(144), np.zeros(144)
+    for solver, x in ((H.FGMRESSolver(), xs), (H.PipelinedFGMRESSolver(), xp)):
+        I = H.ILUPreconditioner()
+        I.setup(A)
+        solver.set_params(p)
+        solver.set_preconditioner(I)
+        solver.solve(A, np.ones(144), x)
+    assert np.linalg.norm(xs - xp) / np.linalg.norm(xs) < 1e-5
+    C = H.SparseMatrix.convection_diffusion_2d(10, 0.1, 5.0, 0.0)
+    I = H.ILUPreconditioner()
+    I.setup(C)
+    s = H.PipelinedFGMRESSolver()
+    s.set_params(p)
+    s.set_preconditioner(I)
+    x = np.zeros(100)
+    st = H.SolverStats()
+    assert s.solve(C, np.ones(100), x, st) and st.final_residual < 1e-8
+
+
+def test_pipelined_lucky_breakdown(ref):
+    # b along an eigenvector of a diagonal matrix: the first Arnoldi vector is exactly
+    # invariant (h_10 = 0).  The pipelined cycle leaves before rotating that column, keeps
+    # the old residual estimate and restarts once (pipelined_fgmres_solver.cpp:117-123);
+    # the standard cycle converges in the same step without a restart.
+    A = (np.arange(5, dtype=np.int32), np.arange(4, dtype=np.int32), np.array([2.0, 3.0, 5.0, 7.0]))
+    b = np.array([2.0, 0.0, 0.0, 0.0])
+    p = default_params(tol=1e-10, max_iter=50, restart_size=4, drop_tol=0.0)
+    rc, xr, sr = ref.solve(5, 0, *A, b, params=p)
+    assert (sr.converged, sr.iterations, sr.restarts) == (1, 1, 1)
+    ok, x, st = run(H.PipelinedFGMRESSolver(), A, b, p, H.PREC_NONE)
+    assert ok and (st.iterations, st.restarts) == (1, 1)
+    assert np.array_equal(x, xr) and np.array_equal(x, [1.0, 0.0, 0.0, 0.0])
+    ok, x, st = run(H.FGMRESSolver(), A, b, p, H.PREC_NONE)
+    assert ok and (st.iterations, st.restarts) == (1, 0)

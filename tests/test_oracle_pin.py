@@ -287,3 +287,57 @@ def test_ilut_capacity_fixture(orc):
     rp2 = np.array([0, 1, 1, 2], np.int32)
     frp2, fci2, flu2 = orc.ilut(rp2, np.array([0, 2], np.int32), np.array([2.0, 3.0]), 1e-4, 0)
     assert list(fci2) == [0, 1, 2] and flu2[1] == 2.220446049250313e-16 * 1e6
+
+
+# ------------------------------------------------ s-step CG and pipelined FGMRES
+
+def _unit_diagonal(A):
+    """D^-1/2 A D^-1/2: the scaling under which the reference's s-step update converges."""
+    rp, ci, v = A
+    n = len(rp) - 1
+    rows = np.repeat(np.arange(n), np.diff(rp))
+    s = 1.0 / np.sqrt(v[ci == rows])
+    return rp, ci, v * s[rows] * s[ci]
+
+
+def _sstep_cases():
+    for name, A in _cases():
+        yield name, A
+        yield "unit_" + name, _unit_diagonal(A)
+
+
+@pytest.mark.parametrize("name,A", list(_sstep_cases()), ids=[c[0] for c in _sstep_cases()])
+def test_oracle_sstep_and_pipelined_equal_reference(orc, ref, name, A):
+    # spectral_interval (sparse_matrix.cpp:451-479), SStepCGSolver (sstep_cg_solver.cpp:
+    # 170-305) -- divergent runs included, NaN for NaN -- and PipelinedFGMRESSolver
+    # (pipelined_fgmres_solver.cpp:69-242), bit for bit
+    assert orc.spectral_interval(*A) == ref.spectral_interval(*A)
+    n = len(A[0]) - 1
+    b = P.rhs(n, 3)
+    for k in (1, 2, 4, 8):
+        p = default_params(tol=1e-8, max_iter=400, sstep_k=k)
+        o, r = orc.solve(3, 1, *A, b, params=p), ref.solve(3, 1, *A, b, params=p)
+        assert o[0] == r[0] and o[2].iterations == r[2].iterations
+        assert np.array_equal(o[1], r[1], equal_nan=True)
+        assert (o[2].flop_count, o[2].mem_bytes, o[2].comm_bytes, o[2].sstep_k) == \
+               (r[2].flop_count, r[2].mem_bytes, r[2].comm_bytes, r[2].sstep_k)
+    for prec in (0, 1, 2):
+        p = default_params(tol=1e-8, max_iter=400, restart_size=20, drop_tol=0.0)
+        o, r = orc.solve(5, prec, *A, b, params=p), ref.solve(5, prec, *A, b, params=p)
+        assert o[0] == r[0] and o[2].iterations == r[2].iterations and o[2].restarts == r[2].restarts
+        assert np.array_equal(o[1], r[1])
+        assert (o[2].flop_count, o[2].mem_bytes) == (r[2].flop_count, r[2].mem_bytes)
+
+
+def test_kat_pipelined_fgmres(orc):
+    # test_improvements.cpp:240-290, restated on the oracle
+    p = default_params(tol=1e-8, max_iter=3000, restart_size=50, drop_tol=0.0)
+    A = P.poisson_2d(16)
+    rc, x, st = orc.solve(5, 2, *A, np.ones(256), params=p)
+    assert rc == 1 and np.linalg.norm(np.ones(256) - orc.spmv(*A, x)) / 16.0 < 1e-7
+    A = P.poisson_2d(12)
+    x_std = orc.solve(1, 2, *A, np.ones(144), params=p)[1]
+    x_pip = orc.solve(5, 2, *A, np.ones(144), params=p)[1]
+    assert np.linalg.norm(x_std - x_pip) / np.linalg.norm(x_std) < 1e-5
+    C = P.convection_diffusion_2d(10, 0.1, 5.0, 0.0)
+    assert orc.solve(5, 2, *C, np.ones(100), params=p)[0] == 1
