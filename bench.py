@@ -64,6 +64,8 @@ def parse():
     ap.add_argument("--serving-requests", type=int, default=200,
                     help="requests in the serving stream (0 skips the serving measurement)")
     ap.add_argument("--serving-n-max", type=float, default=2.6e5)
+    ap.add_argument("--no-variants", action="store_true",
+                    help="skip the Krylov-variant side measurement (s-step CG, pipelined FGMRES)")
     ap.add_argument("--no-ilut", action="store_true",
                     help="skip the ILUT side measurement (device vs reference setup_ilut)")
     ap.add_argument("--profile-step", action="store_true",
@@ -707,6 +709,48 @@ def run_ilut_side(args, local):
             "device_1024": big}
 
 
+def run_variants_side(args, local):
+    """CG, FGMRES(30), PipelinedFGMRES(30) (Jacobi) and SStepCG(k = 4) on the unit-diagonal
+    shifted Helmholtz operator D^-1/2 (A + cI) D^-1/2 on 512^2 (c = 7; a spectrum inside
+    (0, 2), where the reference's s-step update converges), to 1e-8: device time and
+    iterations, and the reference's own solvers on the same system (all host threads)."""
+    import hsps_b200 as H
+    import oracle
+    from hsps_b200 import problems as P
+    from hsps_b200._abi import default_params
+
+    rp, ci, v = P.helmholtz_2d(512, 7.0)
+    n = len(rp) - 1
+    rows = np.repeat(np.arange(n), np.diff(rp))
+    d = 1.0 / np.sqrt(v[ci == rows])
+    v = v * d[rows] * d[ci]
+    b = P.rhs(n, 5)
+    p = default_params(tol=1e-8, max_iter=2000, restart_size=30, sstep_k=4)
+    M = H.SparseMatrix(n, n, rp, ci, v)
+    R = oracle.Reference(fast=True, threads=cpu_threads())
+    out = {"problem": "unit-diagonal shifted Helmholtz 512^2 (c = 7), tol 1e-8, Jacobi"}
+    for name, solver, code in (("cg", H.CGSolver, 0), ("fgmres", H.FGMRESSolver, 1),
+                               ("pipelined_fgmres", H.PipelinedFGMRESSolver, 5),
+                               ("sstep_cg_k4", lambda: H.SStepCGSolver(4), 3)):
+        times = []
+        for _ in range(4):
+            s = solver()
+            s.set_params(p)
+            s.set_preconditioner(H.SolverFactory.make_precond(H.PREC_JACOBI, M, p))
+            st = H.SolverStats()
+            x = np.zeros(n)
+            s.solve(M, b, x, st)
+            times.append(st.device_time_s)
+        t0 = time.perf_counter()
+        rc, xr, sr = R.solve(code, H.PREC_JACOBI, rp, ci, v, b, params=p)
+        ref_s = time.perf_counter() - t0
+        out[name] = {"device_ms": round(1e3 * float(np.median(times[1:])), 3), "iterations": st.iterations,
+                     "converged": bool(st.converged), "reference_ms": round(1e3 * ref_s, 3),
+                     "reference_iterations": sr.iterations, "reference_converged": bool(sr.converged)}
+    out["reference_threads"] = cpu_threads()
+    return out
+
+
 def main():
     args = parse()
     rank, world, local = dist_env()
@@ -733,6 +777,9 @@ def main():
         log("cpu baseline done")
     if rank == 0 and world == 1 and args.serving_requests > 0:
         out["serving"] = run_serving(args, local)
+    if rank == 0 and world == 1 and not args.no_variants:
+        log("Krylov-variant side measurement")
+        out["krylov_variants"] = run_variants_side(args, local)
     if rank == 0 and world == 1 and not args.no_ilut:
         log("ILUT side measurement")
         out["ilut"] = run_ilut_side(args, local)

@@ -19,6 +19,7 @@
 // reference's `while (... && rel_res > tol)` does.  Reproduced, not repaired.
 #include <climits>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <vector>
 
@@ -366,6 +367,9 @@ SolveResult sstep_solve(Ctx& ctx, hamlss_mat* A, const double* b, double* x, con
             ++total;
             rnorm = std::sqrt(rn2);
             rel = rnorm / bnorm;
+            if (p.verbose)
+                std::fprintf(stderr, "  s-step CG: Cholesky failed, steepest step (r.Ap = %.3e)  iters=%d  rel_res=%.4e\n",
+                             h.rap, total, rel);
             continue;
         }
         Coeffs c{};
@@ -385,6 +389,9 @@ SolveResult sstep_solve(Ctx& ctx, hamlss_mat* A, const double* b, double* x, con
         rnorm = std::sqrt(h.rr);
         rel = rnorm / bnorm;
         total += kb;
+        if (p.verbose)                                   // sstep_cg_solver.cpp:268-272
+            std::fprintf(stderr, "  s-step CG: iters=%d  k=%d  kappa(G)=%.4e  rel_res=%.4e\n", total, kb,
+                         cond, rel);
     }
     HAMLSS_CUDA(cudaEventRecord(ctx.ev1, st));
     HAMLSS_CUDA(cudaEventSynchronize(ctx.ev1));

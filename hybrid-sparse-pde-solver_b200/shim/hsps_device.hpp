@@ -90,6 +90,8 @@ inline void to_stats(const hamlss_stats& h, hsps::SolverStats& s) {
     s.precond_used = static_cast<hsps::PrecondType>(h.precond_used);
     s.state_used = static_cast<hsps::AdaptiveState>(h.state_used);
     s.restarts = h.restarts;
+    s.sstep_k = h.sstep_k;
+    s.comm_bytes = h.comm_bytes;
     s.energy_joules_hw = h.energy_joules_hw;
     s.rapl_start_j = h.rapl_start_j;
     s.rapl_end_j = h.rapl_end_j;
@@ -257,7 +259,8 @@ protected:
 // ------------------------------------------------------------------------ solvers
 class DeviceSolver : public hsps::SolverBase {
 public:
-    explicit DeviceSolver(hsps::SolverType t) : hsps::SolverBase(t) {}
+    explicit DeviceSolver(hsps::SolverType t, int engine_id = -1)
+        : hsps::SolverBase(t), engine_id_(engine_id < 0 ? static_cast<int>(t) : engine_id) {}
 
     bool solve(const hsps::SparseMatrix& A, const hsps::Vector& b, hsps::Vector& x,
                hsps::SolverStats& stats) override {
@@ -275,9 +278,10 @@ public:
         Device& d = Device::get();
         hamlss_params p = to_params(params_);
         p.precision = precision_;
+        adjust(p);
         hamlss_stats st;
-        check(hamlss_solve(d.ctx(), static_cast<int>(type_), d.matrix(A), M, b.data(), x.data(),
-                           HAMLSS_HOST, &p, &st));
+        check(hamlss_solve(d.ctx(), engine_id_, d.matrix(A), M, b.data(), x.data(), HAMLSS_HOST, &p,
+                           &st));
         to_stats(st, stats);
         true_residual_ = st.true_residual;
         return stats.converged;
@@ -288,6 +292,8 @@ public:
     double last_true_residual() const { return true_residual_; }
 
 protected:
+    virtual void adjust(hamlss_params&) const {}
+    int engine_id_;
     int precision_ = HAMLSS_FP64;
     double true_residual_ = 0.0;
 };
@@ -302,6 +308,25 @@ public:
     DeviceFGMRESSolver() : DeviceSolver(hsps::SolverType::FGMRES) {}
 };
 
+// PipelinedFGMRESSolver (include/solvers/pipelined_fgmres_solver.hpp:44-74): a SolverBase of
+// type FGMRES, like the project's class.
+class DevicePipelinedFGMRESSolver : public DeviceSolver {
+public:
+    DevicePipelinedFGMRESSolver()
+        : DeviceSolver(hsps::SolverType::FGMRES, HAMLSS_SOLVER_PIPELINED_FGMRES) {}
+};
+
+// SStepCGSolver(k) (include/solvers/sstep_cg_solver.hpp:57-60); the preconditioner is
+// recorded, not applied, as in the project.
+class DeviceSStepCGSolver : public DeviceSolver {
+public:
+    explicit DeviceSStepCGSolver(int k = 4) : DeviceSolver(hsps::SolverType::SSTEP_CG), k_(k) {}
+
+protected:
+    void adjust(hamlss_params& p) const override { p.sstep_k = k_; }
+    int k_;
+};
+
 // ------------------------------------------------------------------------ factory
 struct DeviceSolverFactory {
     static std::unique_ptr<hsps::SolverBase> make_solver(hsps::SolverType t, const hsps::SolverParams& p) {
@@ -310,6 +335,9 @@ struct DeviceSolverFactory {
             case hsps::SolverType::CG: s = std::make_unique<DeviceCGSolver>(); break;
             case hsps::SolverType::FGMRES:
             case hsps::SolverType::BICGSTAB: s = std::make_unique<DeviceFGMRESSolver>(); break;
+            case hsps::SolverType::SSTEP_CG:                     // solver_factory.cpp:38-40
+                s = std::make_unique<DeviceSStepCGSolver>(p.sstep_k);
+                break;
             default: throw std::invalid_argument("SolverFactory: solver type not provided on the device");
         }
         s->set_params(p);

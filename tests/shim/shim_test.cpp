@@ -16,6 +16,7 @@
 #include "preconditioners/jacobi.hpp"
 #include "solvers/cg_solver.hpp"
 #include "solvers/fgmres_solver.hpp"
+#include "solvers/pipelined_fgmres_solver.hpp"
 
 using namespace hsps;
 
@@ -110,6 +111,50 @@ int main() {
         for (Index i = 0; i < A.rows(); ++i) diff = std::max(diff, std::abs(zc[i] - zd[i]));
         std::snprintf(msg, sizeof msg, "ILUT(1e-3, 5) apply: max |cpu - device| = %.3e", diff);
         CHECK(diff == 0.0, msg);
+    }
+
+    {   // pipelined FGMRES and s-step CG, side by side with the project's classes
+        auto A = SparseMatrix::convection_diffusion_2d(24, 1.0, 40.0, 20.0);
+        Vector b(A.rows(), 1.0);
+        SolverParams q = p;
+        q.restart_size = 20;
+        auto Mc = SolverFactory::make_precond(PrecondType::ILU, A, q);
+        auto Md = hsps_b200::DeviceSolverFactory::make_precond(PrecondType::ILU, A, q);
+        PipelinedFGMRESSolver pc;
+        hsps_b200::DevicePipelinedFGMRESSolver pd;
+        pc.set_params(q); pc.set_preconditioner(Mc);
+        pd.set_params(q); pd.set_preconditioner(Md);
+        Vector xc(A.rows(), 0.0), xd;
+        SolverStats sc, sd;
+        bool oc = pc.solve(A, b, xc, sc), od = pd.solve(A, b, xd, sd);
+        char msg[256];
+        std::snprintf(msg, sizeof msg, "pipelined FGMRES+ILU: converged %d/%d iters %d/%d", (int)oc,
+                      (int)od, sc.iterations, sd.iterations);
+        CHECK(oc == od && std::abs(sc.iterations - sd.iterations) <= 1 &&
+              sd.solver_used == SolverType::FGMRES, msg);
+        // the s-step update converges on a unit-diagonal operator: D^-1/2 A D^-1/2
+        auto H = SparseMatrix::poisson_2d(16);
+        std::vector<Index> r, c;
+        std::vector<Real> v;
+        for (Index i = 0; i < H.rows(); ++i)
+            for (Index k = H.row_ptr()[i]; k < H.row_ptr()[i + 1]; ++k) {
+                r.push_back(i);
+                c.push_back(H.col_idx()[k]);
+                v.push_back(H.values()[k] / 8.0 + (H.col_idx()[k] == i ? 0.5 : 0.0));
+            }
+        auto S = SparseMatrix::from_coo(H.rows(), H.cols(), r, c, v);
+        Vector bs(S.rows(), 1.0);
+        q.sstep_k = 4;
+        q.max_iter = 400;
+        auto cpu = SolverFactory::make(SolverType::SSTEP_CG, PrecondType::JACOBI, S, q);
+        auto dev = hsps_b200::DeviceSolverFactory::make(SolverType::SSTEP_CG, PrecondType::JACOBI, S, q);
+        Vector yc(S.rows(), 0.0), yd;
+        SolverStats tc, td;
+        bool ac = cpu.first->solve(S, bs, yc, tc), ad = dev.first->solve(S, bs, yd, td);
+        std::snprintf(msg, sizeof msg, "s-step CG (k = 4): converged %d/%d iters %d/%d sstep_k %d/%d",
+                      (int)ac, (int)ad, tc.iterations, td.iterations, tc.sstep_k, td.sstep_k);
+        CHECK(ac == ad && std::abs(tc.iterations - td.iterations) <= 4 && tc.sstep_k == td.sstep_k &&
+              td.solver_used == SolverType::SSTEP_CG, msg);
     }
 
     {   // error behaviour
