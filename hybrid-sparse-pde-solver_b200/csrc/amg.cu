@@ -297,6 +297,35 @@ __global__ void k_t_sort(int m, const int* __restrict__ trp, int* tci, double* t
 // (3 ints per nonzero of A at 3 * rp[i]).
 constexpr int kHeads = 24;
 
+// Capacity of row i of C = A B: min(products of the row, columns of B).
+__global__ void k_spgemm_bound(int m, const int* __restrict__ arp, const int* __restrict__ aci,
+                               const int* __restrict__ brp, int bcols, int* cap) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+        long long u = 0;
+        for (int t = arp[i]; t < arp[i + 1]; ++t) {
+            const int j = aci[t];
+            u += brp[j + 1] - brp[j];
+        }
+        cap[i] = (int)(u < bcols ? u : bcols);
+    }
+}
+
+// Move row i's cnt[i] entries from its capacity slot (at off[i]) to its CSR place; one warp
+// per row.
+__global__ void k_spgemm_compact(int m, const int* __restrict__ off, const int* __restrict__ cnt,
+                                 const int* __restrict__ wci, const double* __restrict__ wv,
+                                 const int* __restrict__ crp, int* cci, double* cv) {
+    const int lane = threadIdx.x & 31;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < m; i += nw) {
+        const int src = off[i], dst = crp[i], c = cnt[i];
+        for (int t = lane; t < c; t += 32) {
+            cci[dst + t] = wci[src + t];
+            cv[dst + t] = wv[src + t];
+        }
+    }
+}
+
 template <bool FILL>
 __global__ void k_spgemm(int m, const int* __restrict__ arp, const int* __restrict__ aci,
                          const double* __restrict__ av, const int* __restrict__ brp,
@@ -333,7 +362,7 @@ __global__ void k_spgemm(int m, const int* __restrict__ arp, const int* __restri
                 ++o;
             }
         }
-        if (!FILL) ccnt[i] = o;
+        if (ccnt) ccnt[i] = FILL ? o - crp[i] : o;
     }
 }
 
@@ -596,7 +625,7 @@ __global__ void k_spgemm_warp(const int* __restrict__ rows, int nrows, int KH,
                 ++o;
             }
         }
-        if (!FILL && lane == 0) ccnt[i] = o;
+        if (ccnt && lane == 0) ccnt[i] = FILL ? o - crp[i] : o;
         __syncwarp();
     }
 }
@@ -655,9 +684,8 @@ __global__ void k_spgemm_dense(const int* __restrict__ rows, int nrows, int bcol
             total += s_warp[w];
         }
         before += incl - mine;
-        if (!FILL) {
-            if (threadIdx.x == 0) ccnt[i] = total;
-        } else {
+        if (ccnt && threadIdx.x == 0) ccnt[i] = total;
+        if (FILL) {
             int o = crp[i] + before;
             for (int c = c0; c < c1; ++c)
                 if (hit[c] && fabs(acc[c]) > kEps * kEps) {
@@ -720,9 +748,8 @@ __global__ void k_spgemm_rows(const int* __restrict__ rows, int nrows, int S,
                 sm_keys[atomicAdd(&s_n, 1)] = ((unsigned long long)(unsigned)cols[t] << 32) | (unsigned)t;
         __syncthreads();
         const int cnt = s_n;
-        if (!FILL) {
-            if (threadIdx.x == 0) ccnt[i] = cnt;
-        } else {
+        if (ccnt && threadIdx.x == 0) ccnt[i] = cnt;
+        if (FILL) {
             const int N = pow2_at_least(cnt > 0 ? cnt : 1);
             for (int t = cnt + threadIdx.x; t < N; t += blockDim.x) sm_keys[t] = kNoKey;
             block_bitonic(sm_keys, N);
@@ -1421,6 +1448,53 @@ void spgemm(Ctx& ctx, const Csr<double>& A, const Csr<double>& B, DCsr& C) {
     const size_t smem = 20 * (size_t)S;                 // u64 keys + doubles + ints per slot
     const size_t dsmem = 9 * (size_t)std::max(B.m, 1);   // dense accumulator + hit flags
     const int* dlist = list.p + A.n;
+    // One numeric pass into per-row capacity slots (min(products, B.m) each), then a
+    // compaction into the CSR -- when the slots fit (below 2^31 entries and 8 GB); else the
+    // counting pass below followed by the numeric pass in place.
+    {
+        DBuf<int> off(A.n + 1);
+        HAMLSS_CUDA(cudaMemsetAsync(off.p + A.n, 0, sizeof(int), s));
+        if (A.n) k_spgemm_bound<<<g, 256, 0, s>>>(A.n, A.rp, A.ci, B.rp, std::max(B.m, 1), off.p);
+        HAMLSS_LAUNCH_CHECK();
+        const long long total = exclusive_scan(ctx, off.p, A.n + 1);
+        if (total <= INT_MAX && total * 12 <= (8LL << 30)) {
+            if ((size_t)total > ctx.gemm_ci.n || (size_t)total > ctx.gemm_v.n) {
+                AllocScope plain(nullptr);          // long-lived: plain device memory, not the pool
+                ctx.gemm_ci.ensure(std::max(total, 1LL) + (1 << 20));
+                ctx.gemm_v.ensure(std::max(total, 1LL) + (1 << 20));
+            }
+            DBuf<int>& wci = ctx.gemm_ci;
+            DBuf<double>& wv = ctx.gemm_v;
+            k_spgemm<true><<<g, 256, 0, s>>>(A.n, A.rp, A.ci, A.v, B.rp, B.ci, B.v, cnt.p, off.p, wci.p,
+                                             wv.p, heads.p, cls.p);
+            HAMLSS_LAUNCH_CHECK();
+            if (nlong) {
+                const int gb = row_grid(ctx, k_spgemm_rows<true>, smem, nlong);
+                k_spgemm_rows<true><<<gb, kRowBlock, smem, s>>>(list.p, nlong, S, A.rp, A.ci, A.v, B.rp, B.ci,
+                                                                B.v, cnt.p, off.p, wci.p, wv.p);
+                HAMLSS_LAUNCH_CHECK();
+            }
+            if (nwarp) {
+                const int gb = merge_grid(ctx, k_spgemm_warp<true>, wsmem, nwarp);
+                k_spgemm_warp<true><<<gb, 32 * kMergeWarps, wsmem, s>>>(wlist, nwarp, KH, A.rp, A.ci, A.v,
+                                                                         B.rp, B.ci, B.v, cnt.p, off.p,
+                                                                         wci.p, wv.p);
+                HAMLSS_LAUNCH_CHECK();
+            }
+            if (ndense) {
+                const int gb = row_grid(ctx, k_spgemm_dense<true>, dsmem, ndense);
+                k_spgemm_dense<true><<<gb, kRowBlock, dsmem, s>>>(dlist, ndense, B.m, A.rp, A.ci, A.v, B.rp,
+                                                                  B.ci, B.v, cnt.p, off.p, wci.p, wv.p);
+                HAMLSS_LAUNCH_CHECK();
+            }
+            build_csr_counts(ctx, C, A.n, B.m, cnt);
+            if (A.n)
+                k_spgemm_compact<<<std::max(1, std::min(ceil_div(A.n, 8), ctx.sm_count * 16)), 256, 0, s>>>(
+                    A.n, off.p, cnt.p, wci.p, wv.p, C.rp.p, C.ci.p, C.v.p);
+            HAMLSS_LAUNCH_CHECK();
+            return;
+        }
+    }
     k_spgemm<false><<<g, 256, 0, s>>>(A.n, A.rp, A.ci, A.v, B.rp, B.ci, B.v, cnt.p, nullptr, nullptr,
                                       nullptr, heads.p, cls.p);
     HAMLSS_LAUNCH_CHECK();
