@@ -5,9 +5,10 @@
 // pivoting (amg.cpp:260-291).  Coarse operators of the smoothed-aggregation hierarchy
 // become dense, and when the hierarchy is cut where coarsening stalls the coarsest level
 // can hold thousands of rows.  Blocked for the GPU (row-major n x n, nb = 64), first
-// without interchanges -- diagonal block in shared memory, L21 and U12 by triangular
-// solves, A22 by DGEMM, no grid-wide synchronisation -- and, if a pivot falls below 1e-10
-// of the largest entry, again with partial pivoting as the reference does:
+// without interchanges -- diagonal block factored in shared memory, the inverses of its
+// two triangles formed by one block (64 x 64 each), L21 = A21 U11^-1 and U12 = L11^-1 A12
+// as DGEMMs, A22 by DGEMM, no grid-wide synchronisation -- and, if a pivot falls below
+// 1e-10 of the largest entry, again with partial pivoting as the reference does:
 //   panel     columns [k0, k0+nb): one cooperative kernel over all SMs, one column at a
 //             time -- pivot search (largest |a_ij|, first index on ties, like the
 //             reference), row swap inside the panel, multipliers l = a_ij * (1/a_jj),
@@ -16,7 +17,9 @@
 //   U12       L11^-1 A12, one thread per column (unit lower triangular solve)
 //   trailing  A22 -= L21 U12, a library DGEMM (cuBLAS)
 // The inverse solves A X = I: X = P I, then L Y = X and U X = Y, blocked the same way
-// (triangular solve of a 64-row block per column, DGEMM update of the rest).
+// (each 64-row block multiplied by its diagonal block's inverse, DGEMM update of the
+// rest): every step is a GEMM, where column-per-thread triangular solves were a long
+// dependent chain per launch.
 #include <cooperative_groups.h>
 #include <cublas_v2.h>
 
@@ -191,25 +194,6 @@ __global__ void k_lu_diag_nopiv(int n, int k0, int kb, double* M, double floor, 
     }
 }
 
-// L21 = A21 U11^-1 for rows [k0+kb, n), one thread per row (U11 in shared memory).
-__global__ void k_lu_l21(int n, int k0, int kb, double* M) {
-    __shared__ double u[kNb][kNb + 1];
-    for (int t = threadIdx.x; t < kb * kb; t += blockDim.x) {
-        const int r = t / kb, c = t - r * kb;
-        u[r][c] = M[(size_t)(k0 + r) * n + k0 + c];
-    }
-    __syncthreads();
-    for (int r = k0 + kb + blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
-        double* row = M + (size_t)r * n + k0;
-        for (int j = 0; j < kb; ++j) {
-            double acc = row[j];
-            for (int q = 0; q < j; ++q) acc = __dsub_rn(acc, __dmul_rn(row[q], u[q][j]));
-            const double d = u[j][j];
-            row[j] = __dmul_rn(acc, (d != 0.0) ? 1.0 / d : 0.0);
-        }
-    }
-}
-
 __global__ void k_abs_max(long long count, const double* __restrict__ a, unsigned long long* out) {
     double m = 0.0;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < count;
@@ -255,22 +239,47 @@ __global__ void k_trsm_lower_unit(int n, int k0, int kb, const double* __restric
     }
 }
 
-// B := U11^-1 B for rows [k0, k0+kb) (upper U11 = U[k0.., k0..] with its diagonal).
-__global__ void k_trsm_upper(int n, int k0, int kb, const double* __restrict__ U, int ldu, double* B,
-                             int ldb, int c0, int c1) {
-    __shared__ double su[kNb][kNb];
+// Inverses of the factors of diagonal block b (k0 = b * kNb): Li = L11^-1 (unit lower) and
+// Ui = U11^-1 (upper), kb x kb row-major with ld kNb at inv + 2 * b * kNb * kNb.  Thread c
+// solves column c (substitution in the factor's row order); the block is in shared memory.
+__global__ void k_block_inverses(int n, int b0, const double* __restrict__ M, double* inv) {
+    __shared__ double a[kNb][kNb + 1];
+    const int b = b0 + blockIdx.x;
+    const int k0 = b * kNb, kb = min(kNb, n - k0);
+    double* Li = inv + 2LL * b * kNb * kNb;
+    double* Ui = Li + kNb * kNb;
     for (int t = threadIdx.x; t < kb * kb; t += blockDim.x) {
-        const int r = t / kb, q = t - r * kb;
-        su[r][q] = U[(size_t)(k0 + r) * ldu + k0 + q];
+        const int r = t / kb, c = t - r * kb;
+        a[r][c] = M[(size_t)(k0 + r) * n + k0 + c];
     }
     __syncthreads();
-    for (int c = c0 + blockIdx.x * blockDim.x + threadIdx.x; c < c1; c += gridDim.x * blockDim.x) {
-        for (int r = kb - 1; r >= 0; --r) {
-            double acc = B[(size_t)(k0 + r) * ldb + c];
-            for (int q = r + 1; q < kb; ++q)
-                acc = __dsub_rn(acc, __dmul_rn(su[r][q], B[(size_t)(k0 + q) * ldb + c]));
-            B[(size_t)(k0 + r) * ldb + c] = acc / su[r][r];
+    const int c = threadIdx.x;
+    if (c < kb) {
+        for (int r = 0; r < kb; ++r) {              // L x = e_c
+            double acc = (r == c) ? 1.0 : 0.0;
+            if (r > c)
+                for (int q = c; q < r; ++q) acc = __dsub_rn(acc, __dmul_rn(a[r][q], Li[q * kNb + c]));
+            Li[r * kNb + c] = r < c ? 0.0 : acc;
         }
+        for (int r = kb - 1; r >= 0; --r) {         // U x = e_c
+            double acc = (r == c) ? 1.0 : 0.0;
+            if (r <= c) {
+                for (int q = r + 1; q <= c; ++q) acc = __dsub_rn(acc, __dmul_rn(a[r][q], Ui[q * kNb + c]));
+                acc = acc / a[r][r];
+            }
+            Ui[r * kNb + c] = r > c ? 0.0 : acc;
+        }
+    }
+}
+
+// dst (rows x cols, ld ldd) = src (ld lds), row-major.
+__global__ void k_copy_block(int rows, int cols, const double* __restrict__ src, int lds, double* dst,
+                             int ldd) {
+    const long long total = (long long)rows * cols;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int r = (int)(t / cols), c = (int)(t - (long long)r * cols);
+        dst[(size_t)r * ldd + c] = src[(size_t)r * lds + c];
     }
 }
 
@@ -300,6 +309,19 @@ void gemm_sub(cublasHandle_t h, int n, int m, int p, int k, const double* A, con
                  "dgemm");
 }
 
+// Row-major C (m x p, ldc) = A (m x k, lda) * B (k x p, ldb).
+void gemm_set(cublasHandle_t h, int m, int p, int k, const double* A, int lda, const double* B, int ldb,
+              double* C, int ldc) {
+    if (m <= 0 || p <= 0 || k <= 0) return;
+    const double one = 1.0, zero = 0.0;
+    cublas_check(cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, p, m, k, &one, B, ldb, A, lda, &zero, C, ldc),
+                 "dgemm");
+}
+
+int copy_grid(Ctx& ctx, long long count) {
+    return (int)std::max<long long>(1, std::min<long long>((count + 255) / 256, ctx.sm_count * 8LL));
+}
+
 int col_grid(Ctx& ctx, int cols) {
     return std::max(1, std::min(ceil_div(cols, 128), ctx.sm_count * 4));
 }
@@ -322,21 +344,30 @@ cublasHandle_t blas_of(Ctx& ctx) {
 }
 
 // Blocked LU without row interchanges; false when a pivot falls below `floor`.
-bool factor_nopivot(Ctx& ctx, cublasHandle_t h, int n, double* M, double floor) {
+// L21 = A21 U11^-1 and U12 = L11^-1 A12 are GEMMs with the diagonal block's inverses
+// (k_block_inverses) through the scratch T (n x kNb doubles).
+bool factor_nopivot(Ctx& ctx, cublasHandle_t h, int n, double* M, double floor, double* inv, double* T) {
     cudaStream_t s = ctx.lane.stream;
     DBuf<int> tiny(1);
     tiny.zero(s);
     for (int k0 = 0; k0 < n; k0 += kNb) {
         const int kb = std::min(kNb, n - k0);
         k_lu_diag_nopiv<<<1, 256, 0, s>>>(n, k0, kb, M, floor, tiny.p);
+        k_block_inverses<<<1, kNb, 0, s>>>(n, k0 / kNb, M, inv);
         HAMLSS_LAUNCH_CHECK();
         const int rest = n - k0 - kb;
         if (rest > 0) {
-            k_lu_l21<<<col_grid(ctx, rest), 128, 0, s>>>(n, k0, kb, M);
-            k_trsm_lower_unit<<<col_grid(ctx, rest), 128, 0, s>>>(n, k0, kb, M, n, M, n, k0 + kb, n);
+            const double* Li = inv + 2LL * (k0 / kNb) * kNb * kNb;
+            const double* Ui = Li + kNb * kNb;
+            double* A21 = M + (size_t)(k0 + kb) * n + k0;
+            double* A12 = M + (size_t)k0 * n + k0 + kb;
+            gemm_set(h, rest, kb, kb, A21, n, Ui, kNb, T, kNb);
+            k_copy_block<<<copy_grid(ctx, (long long)rest * kb), 256, 0, s>>>(rest, kb, T, kNb, A21, n);
             HAMLSS_LAUNCH_CHECK();
-            gemm_sub(h, n, rest, rest, kb, M + (size_t)(k0 + kb) * n + k0, M + (size_t)k0 * n + k0 + kb,
-                     M + (size_t)(k0 + kb) * n + k0 + kb);
+            gemm_set(h, kb, rest, kb, Li, kNb, A12, n, T, rest);
+            k_copy_block<<<copy_grid(ctx, (long long)rest * kb), 256, 0, s>>>(kb, rest, T, rest, A12, n);
+            HAMLSS_LAUNCH_CHECK();
+            gemm_sub(h, n, rest, rest, kb, A21, A12, M + (size_t)(k0 + kb) * n + k0 + kb);
         }
     }
     int t = 0;
@@ -402,19 +433,27 @@ void dense_lu_inverse(Ctx& ctx, int n, double* M, double* Minv, int* piv) {
     HAMLSS_CUDA(cudaStreamSynchronize(s));
     double big = 0.0;
     std::memcpy(&big, &bits, sizeof big);
-    if (factor_nopivot(ctx, h, n, M, 1e-10 * big)) {
+    const int nblk = (n + kNb - 1) / kNb;
+    DBuf<double> inv(2LL * nblk * kNb * kNb), T((size_t)n * kNb);
+    if (factor_nopivot(ctx, h, n, M, 1e-10 * big, inv.p, T.p)) {
         k_iota<<<cg_, 128, 0, s>>>(n, piv);
         HAMLSS_LAUNCH_CHECK();
     } else {
         HAMLSS_CUDA(cudaMemcpyAsync(M, Minv, bytes, cudaMemcpyDeviceToDevice, s));
         factor_pivot(ctx, h, n, M, piv);
+        k_block_inverses<<<nblk, kNb, 0, s>>>(n, 0, M, inv.p);
+        HAMLSS_LAUNCH_CHECK();
     }
-    // X = P I; L Y = X (forward, unit lower); U X = Y (backward)
+    // X = P I; L Y = X (forward, unit lower); U X = Y (backward).  The diagonal blocks are
+    // applied as GEMMs with their inverses, the off-diagonal blocks as GEMM updates.
     k_perm_identity<<<cg_, 128, 0, s>>>(n, piv, Minv);
     HAMLSS_LAUNCH_CHECK();
+    DBuf<double> W((size_t)kNb * n);
     for (int k0 = 0; k0 < n; k0 += kNb) {
         const int kb = std::min(kNb, n - k0);
-        k_trsm_lower_unit<<<cg_, 128, 0, s>>>(n, k0, kb, M, n, Minv, n, 0, n);
+        const double* Li = inv.p + 2LL * (k0 / kNb) * kNb * kNb;
+        gemm_set(h, kb, n, kb, Li, kNb, Minv + (size_t)k0 * n, n, W.p, n);
+        k_copy_block<<<copy_grid(ctx, (long long)kb * n), 256, 0, s>>>(kb, n, W.p, n, Minv + (size_t)k0 * n, n);
         HAMLSS_LAUNCH_CHECK();
         const int rest = n - k0 - kb;
         gemm_sub(h, n, rest, n, kb, M + (size_t)(k0 + kb) * n + k0, Minv + (size_t)k0 * n,
@@ -423,7 +462,9 @@ void dense_lu_inverse(Ctx& ctx, int n, double* M, double* Minv, int* piv) {
     const int last = ((n - 1) / kNb) * kNb;
     for (int k0 = last; k0 >= 0; k0 -= kNb) {
         const int kb = std::min(kNb, n - k0);
-        k_trsm_upper<<<cg_, 128, 0, s>>>(n, k0, kb, M, n, Minv, n, 0, n);
+        const double* Ui = inv.p + 2LL * (k0 / kNb) * kNb * kNb + kNb * kNb;
+        gemm_set(h, kb, n, kb, Ui, kNb, Minv + (size_t)k0 * n, n, W.p, n);
+        k_copy_block<<<copy_grid(ctx, (long long)kb * n), 256, 0, s>>>(kb, n, W.p, n, Minv + (size_t)k0 * n, n);
         HAMLSS_LAUNCH_CHECK();
         gemm_sub(h, n, k0, n, kb, M + k0, Minv + (size_t)k0 * n, Minv);
     }
