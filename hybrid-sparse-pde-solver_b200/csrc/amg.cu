@@ -297,16 +297,26 @@ __global__ void k_t_sort(int m, const int* __restrict__ trp, int* tci, double* t
 // (3 ints per nonzero of A at 3 * rp[i]).
 constexpr int kHeads = 24;
 
-// Capacity of row i of C = A B: min(products of the row, columns of B).
+// Capacity of row i of C = A B: min(products of the row, columns of B, the span from the
+// smallest first column to the largest last column of the selected rows of B).
 __global__ void k_spgemm_bound(int m, const int* __restrict__ arp, const int* __restrict__ aci,
-                               const int* __restrict__ brp, int bcols, int* cap) {
+                               const int* __restrict__ brp, const int* __restrict__ bci, int bcols,
+                               int* cap) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
         long long u = 0;
+        int lo = INT_MAX, hi = -1;
         for (int t = arp[i]; t < arp[i + 1]; ++t) {
             const int j = aci[t];
-            u += brp[j + 1] - brp[j];
+            const int p0 = brp[j], p1 = brp[j + 1];
+            u += p1 - p0;
+            if (p1 > p0) {
+                lo = min(lo, bci[p0]);
+                hi = max(hi, bci[p1 - 1]);
+            }
         }
-        cap[i] = (int)(u < bcols ? u : bcols);
+        long long c = u < bcols ? u : bcols;
+        const long long span = hi >= lo ? (long long)hi - lo + 1 : 0;
+        cap[i] = (int)(c < span ? c : span);
     }
 }
 
@@ -1454,7 +1464,7 @@ void spgemm(Ctx& ctx, const Csr<double>& A, const Csr<double>& B, DCsr& C) {
     {
         DBuf<int> off(A.n + 1);
         HAMLSS_CUDA(cudaMemsetAsync(off.p + A.n, 0, sizeof(int), s));
-        if (A.n) k_spgemm_bound<<<g, 256, 0, s>>>(A.n, A.rp, A.ci, B.rp, std::max(B.m, 1), off.p);
+        if (A.n) k_spgemm_bound<<<g, 256, 0, s>>>(A.n, A.rp, A.ci, B.rp, B.ci, std::max(B.m, 1), off.p);
         HAMLSS_LAUNCH_CHECK();
         const long long total = exclusive_scan(ctx, off.p, A.n + 1);
         if (total <= INT_MAX && total * 12 <= (8LL << 30)) {

@@ -205,6 +205,10 @@ int hamlss_mat_upload(hamlss_ctx* ctx, int32_t rows, int32_t cols, int32_t nnz,
             (nnz > 0 && (!col_idx || !values)))
             return set_err(HAMLSS_ERR_INVALID, "hamlss_mat_upload: bad arguments");
         HAMLSS_CUDA(cudaSetDevice(ctx->c.device));
+        // the matrix, and the workspaces later cached on it, come from the device's
+        // stream-ordered pool: a serving loop that uploads and releases a matrix per request
+        // then reuses memory instead of mapping and unmapping it each time
+        AllocScope scope(ctx->c.lane.stream);
         auto* M = new hamlss_mat();
         M->ctx = ctx;
         DevMat& A = M->A;
@@ -270,6 +274,7 @@ int hamlss_mat_release(hamlss_mat* M) {
     return guarded([&]() -> int {
         if (!M) return HAMLSS_OK;
         cudaStreamSynchronize(M->ctx->c.lane.stream);
+        AllocScope scope(M->ctx->c.lane.stream);     // pooled buffers go back on this stream
         delete M;
         return HAMLSS_OK;
     });
@@ -404,6 +409,7 @@ int hamlss_precond_setup(hamlss_ctx* ctx, const hamlss_mat* A, int kind,
         hamlss_params p;
         if (params) p = *params; else hamlss_params_default(&p);
         *out = nullptr;
+        AllocScope scope(ctx->c.lane.stream);
         double t0 = now_s();
         auto* Am = const_cast<hamlss_mat*>(A);
         std::unique_ptr<Prec> P;
@@ -440,6 +446,7 @@ int hamlss_precond_apply(hamlss_ctx* ctx, const hamlss_prec* M, const double* r,
         if (!ctx || !M || !r || !z) return set_err(HAMLSS_ERR_INVALID, "null argument");
         Ctx& c = ctx->c;
         cudaStream_t s = c.lane.stream;
+        AllocScope scope(s);
         const int n = M->p->n;
         Workspace& ws = M->A->ws;
         const double* dr = r;
@@ -467,6 +474,7 @@ int hamlss_precond_release(hamlss_prec* M) {
     return guarded([&]() -> int {
         if (!M) return HAMLSS_OK;
         cudaStreamSynchronize(M->ctx->c.lane.stream);
+        AllocScope scope(M->ctx->c.lane.stream);
         delete M;
         return HAMLSS_OK;
     });
@@ -613,6 +621,7 @@ int hamlss_solve(hamlss_ctx* ctx, int solver, const hamlss_mat* A, const hamlss_
         Ctx& c = ctx->c;
         HAMLSS_CUDA(cudaSetDevice(c.device));
         cudaStream_t s = c.lane.stream;
+        AllocScope scope(s);
         auto* Am = const_cast<hamlss_mat*>(A);
         Prec* P = M ? M->p.get() : nullptr;
         IoVecs io = stage_in(Am, b, x, where, s);
@@ -655,6 +664,7 @@ int hamlss_solve_adaptive(hamlss_ctx* ctx, const hamlss_mat* A, const double* b,
         Ctx& c = ctx->c;
         HAMLSS_CUDA(cudaSetDevice(c.device));
         cudaStream_t s = c.lane.stream;
+        AllocScope scope(s);
         auto* Am = const_cast<hamlss_mat*>(A);
         double feat[24];
         int state = 0;
