@@ -628,11 +628,12 @@ def serve_plain(reqs, params, device):
             "p99_ms": round(1e3 * _pct(lat, 0.99), 2), "max_true_residual": max(res)}
 
 
-def serve_engine(reqs, params, device):
-    """The continuous-batching server: requests submitted at their arrival times."""
+def serve_engine(reqs, params, device, order=0):
+    """The continuous-batching server: requests submitted at their arrival times; order 0
+    admits in arrival order, 1 fewest nonzeros first."""
     from hsps_b200.serve import Server
 
-    with Server(device=device, slots=4, batch_max_rows=16384) as srv:
+    with Server(device=device, slots=4, batch_max_rows=16384, order=order) as srv:
         hs = []
         t0 = time.perf_counter()
         for rp, ci, v, b, arr, _ in reqs:
@@ -672,11 +673,13 @@ def run_serving(args, local):
     timed = P.serving_stream(R, 77, 1e3, args.serving_n_max, rate=rate)
     plain_r = serve_plain(timed, params, local)
     eng_r = serve_engine(timed, params, local)
+    eng_s = serve_engine(timed, params, local, order=1)
     return {"requests": R, "n_range": [1e3, args.serving_n_max], "tol": TOL,
             "mix": "50% var-kappa Poisson, 35% upwind conv-diff, 15% shifted Helmholtz",
             "inner": "mixed precision (FP32 inner, FP64 refinement), adaptive ladder",
             "burst": {"server": eng_b, "plain": plain_b},
-            "poisson_arrivals": {"rate_per_s": round(rate, 2), "server": eng_r, "plain": plain_r}}
+            "poisson_arrivals": {"rate_per_s": round(rate, 2), "server": eng_r,
+                                 "server_fewest_nonzeros_first": eng_s, "plain": plain_r}}
 
 
 def run_ilut_side(args, local):

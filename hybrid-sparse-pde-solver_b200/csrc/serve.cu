@@ -7,8 +7,12 @@
 //
 //   admission   a request is admitted once its estimated device footprint fits the HBM
 //               budget next to the requests already admitted; one that can never fit is
-//               refused at submit time (HAMLSS_ERR_BUDGET).  Requests that fit may pass a
-//               head that does not, at most kMaxBypass times, so large requests never starve.
+//               refused at submit time (HAMLSS_ERR_BUDGET).  Queue order (config.order):
+//               0 (default) arrival order, where a request that fits may pass a head that
+//               does not, at most kMaxBypass times; 1 fewest nonzeros first -- the least
+//               work first, which keeps the median latency down under steady load but
+//               leaves the largest requests to the end of a burst -- where a request passed
+//               kMaxAgeBypass times leads and is passed by nobody.
 //   solve lanes `slots` worker threads, each with its own engine context (its own CUDA
 //               stream), take admitted requests and run the adaptive ladder on them; their
 //               kernels overlap on the device.
@@ -42,6 +46,7 @@
 namespace {
 
 constexpr int kMaxBypass = 8;           // how often queued requests may pass the head
+constexpr int kMaxAgeBypass = 32;       // fewest-nonzeros order: passes before a request leads
 constexpr int kBatchMaxRestart = 32;    // the batch kernel's FGMRES restart limit
 
 double now_s() {
@@ -144,6 +149,29 @@ struct hamlss_server {
 
     // ---- queue selection (mu held)
     Request* pick(std::deque<Request*>& q) {
+        if (cfg.order == 1 && !q.empty()) {
+            // fewest nonzeros first (the least work first keeps the median latency low when
+            // the lanes are busy); a request passed kMaxAgeBypass times goes first, and while
+            // it does not fit nobody passes it
+            Request* h = q.front();
+            if (h->bypassed >= kMaxAgeBypass) {
+                if (admitted + h->footprint > cfg.hbm_budget_bytes) return nullptr;
+                q.pop_front();
+                admit(h);
+                return h;
+            }
+            long best = -1;
+            for (size_t i = 0; i < q.size(); ++i)
+                if (admitted + q[i]->footprint <= cfg.hbm_budget_bytes &&
+                    (best < 0 || q[i]->nnz < q[(size_t)best]->nnz))
+                    best = (long)i;
+            if (best < 0) return nullptr;
+            for (long j = 0; j < best; ++j) ++q[(size_t)j]->bypassed;
+            Request* r = q[(size_t)best];
+            q.erase(q.begin() + best);
+            admit(r);
+            return r;
+        }
         for (size_t i = 0; i < q.size(); ++i) {
             Request* r = q[i];
             if (admitted + r->footprint <= cfg.hbm_budget_bytes) {
@@ -369,6 +397,7 @@ void hamlss_server_config_default(hamlss_server_config* c) {
     c->hbm_budget_bytes = 150LL * 1000 * 1000 * 1000;
     c->batch_max_rows = 16384;
     c->batch_max_count = 2048;
+    c->order = 0;
 }
 
 int hamlss_server_create(const hamlss_server_config* config, hamlss_server** out) {
@@ -378,6 +407,7 @@ int hamlss_server_create(const hamlss_server_config* config, hamlss_server** out
     if (config) c = *config;
     else hamlss_server_config_default(&c);
     if (c.slots < 1 || c.slots > 64) return fail(HAMLSS_ERR_INVALID, "slots must be in [1, 64]");
+    if (c.order != 0 && c.order != 1) return fail(HAMLSS_ERR_INVALID, "order must be 0 or 1");
     if (c.hbm_budget_bytes <= 0) return fail(HAMLSS_ERR_INVALID, "hbm_budget_bytes must be > 0");
     if (c.batch_max_rows < 0 || (c.batch_max_rows > 0 && c.batch_max_count < 1))
         return fail(HAMLSS_ERR_INVALID, "batch_max_rows >= 0 and batch_max_count >= 1");

@@ -159,6 +159,7 @@ class ServerConfig(C.Structure):
         ("hbm_budget_bytes", C.c_int64),
         ("batch_max_rows", C.c_int32),
         ("batch_max_count", C.c_int32),
+        ("order", C.c_int32),
     ]
 
 

@@ -339,6 +339,9 @@ typedef struct hamlss_server_config {
     int64_t hbm_budget_bytes;  /* admission budget for request state (150e9)                */
     int32_t batch_max_rows;    /* coalesce requests with n <= this; 0 disables (16384)      */
     int32_t batch_max_count;   /* systems per coalesced launch (2048)                       */
+    int32_t order;             /* solve-lane queue: 0 arrival order (a fitting request may  */
+                               /* pass a head that does not fit, at most 8 times) (0); 1    */
+                               /* fewest nonzeros first, a request passed 32 times leads    */
 } hamlss_server_config;
 
 typedef struct hamlss_server_report {

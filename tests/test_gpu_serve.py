@@ -124,3 +124,19 @@ def test_batch_failure_escalates():
         rep = srv.report()
     assert rep["escalated"] == 1 and rep["coalesced"] == 0, rep
     assert st.state_used == H.STATE_HARD and not st.converged
+
+
+def test_fewest_nonzeros_first_order(orc):
+    # order = 1 with one solve lane and no coalescing: while the first (largest) request
+    # runs, the queued ones are admitted smallest first; results are those of the ladder
+    reqs = [r for r in stream(12, 11, 2000, 40000)]
+    reqs.sort(key=lambda r: -len(r[2]))
+    with Server(slots=1, batch_max_rows=0, order=1) as srv:
+        handles = [srv.submit(rp, ci, v, b, params=params()) for rp, ci, v, b in reqs]
+        out = [h.wait(timeout=600) for h in handles]
+        rep = srv.report()
+    assert rep["completed"] == len(reqs) and rep["failed"] == 0 and rep["peak_running"] == 1, rep
+    for (rp, ci, v, b), (x, st) in zip(reqs, out):
+        assert st.converged and rel_res(orc, rp, ci, v, b, x) <= 1.5 * TOL
+    with pytest.raises(Exception):
+        Server(order=2)
