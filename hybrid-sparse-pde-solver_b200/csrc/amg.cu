@@ -515,22 +515,31 @@ constexpr int kWarpMergeK = 512;        // long rows with at most this many left
 constexpr int kMergeWarps = 4;          // warps (rows) per block of k_spgemm_warp
 
 __global__ void k_spgemm_classify(int m, const int* __restrict__ arp, const int* __restrict__ aci,
-                                  const int* __restrict__ brp, int bcols, int* cls, int* list,
-                                  int* count) {
+                                  const int* __restrict__ brp, const int* __restrict__ bci, int bcols,
+                                  int* cls, int* list, int* count, int* wlo, int* wspan) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
         const int s = arp[i], k = arp[i + 1] - s;
         long long u = 0;
+        int lo = INT_MAX, hi = -1;
         for (int t = 0; t < k; ++t) {
             const int j = aci[s + t];
-            u += brp[j + 1] - brp[j];
+            const int p0 = brp[j], p1 = brp[j + 1];
+            u += p1 - p0;
+            if (p1 > p0) {
+                lo = min(lo, bci[p0]);
+                hi = max(hi, bci[p1 - 1]);
+            }
         }
+        const long long span = hi >= lo ? (long long)hi - lo + 1 : 0;
         const long long h = u < bcols ? u : bcols;
         const bool lng = k > kHeads || u > 512;
         // dense accumulation pays one barrier per left entry: worth it when the right rows
-        // are long (>= 64 products a step); the warp merge pays per output column
+        // are long (>= 64 products a step, or >= 32 over a window of the columns); the warp
+        // merge pays per output column
         const bool dense_ok = bcols <= kDenseCols && h > kHashMax / 4;
         int c = 0;
         if (lng && dense_ok && u >= 64LL * k) c = 2;
+        else if (lng && !dense_ok && span <= kDenseCols && u >= 32LL * k && h > kHashMax / 4) c = 4;
         else if (lng && k <= kWarpMergeK) c = 3;
         else if (lng && dense_ok) c = 2;
         else if (lng && h <= kHashMax) c = 1;
@@ -544,6 +553,11 @@ __global__ void k_spgemm_classify(int m, const int* __restrict__ arp, const int*
         } else if (c == 3) {
             list[2LL * m + atomicAdd(count + 3, 1)] = i;
             atomicMax(count + 4, k);
+        } else if (c == 4) {
+            list[3LL * m + atomicAdd(count + 5, 1)] = i;
+            atomicMax(count + 6, (int)span);
+            wlo[i] = lo;
+            wspan[i] = (int)span;
         }
     }
 }
@@ -700,6 +714,76 @@ __global__ void k_spgemm_dense(const int* __restrict__ rows, int nrows, int bcol
             for (int c = c0; c < c1; ++c)
                 if (hit[c] && fabs(acc[c]) > kEps * kEps) {
                     cci[o] = c;
+                    cv[o] = acc[c];
+                    ++o;
+                }
+        }
+        for (int c = c0; c < c1; ++c) {
+            acc[c] = 0.0;
+            hit[c] = 0;
+        }
+        __syncthreads();
+    }
+}
+
+// Row i of C = A B for the listed rows, one block per row, with a dense accumulator over the
+// row's column window [lo_i, lo_i + span_i) (the span of the selected rows of B, at most
+// W columns): the arithmetic and output order of k_spgemm_dense, for right operands with
+// more columns than fit in shared memory.  Shared memory: W doubles + W flag bytes.
+template <bool FILL>
+__global__ void k_spgemm_window(const int* __restrict__ rows, int nrows, int W,
+                                const int* __restrict__ wlo, const int* __restrict__ wspan,
+                                const int* __restrict__ arp, const int* __restrict__ aci,
+                                const double* __restrict__ av, const int* __restrict__ brp,
+                                const int* __restrict__ bci, const double* __restrict__ bv,
+                                int* ccnt, const int* __restrict__ crp, int* cci, double* cv) {
+    extern __shared__ double acc[];
+    unsigned char* hit = reinterpret_cast<unsigned char*>(acc + W);
+    __shared__ int s_warp[kRowBlock / 32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int c = threadIdx.x; c < W; c += blockDim.x) {
+        acc[c] = 0.0;
+        hit[c] = 0;
+    }
+    __syncthreads();
+    for (int r = blockIdx.x; r < nrows; r += gridDim.x) {
+        const int i = rows[r];
+        const int s = arp[i], k = arp[i + 1] - s;
+        const int lo = wlo[i], span = wspan[i];
+        for (int t = 0; t < k; ++t) {
+            const int j = aci[s + t];
+            const double a = av[s + t];
+            const int e1 = brp[j + 1];
+            for (int e = brp[j] + threadIdx.x; e < e1; e += blockDim.x) {
+                const int c = bci[e] - lo;
+                acc[c] = __dadd_rn(acc[c], __dmul_rn(a, bv[e]));
+                hit[c] = 1;
+            }
+            __syncthreads();
+        }
+        const int chunk = (span + blockDim.x - 1) / blockDim.x;
+        const int c0 = min(span, (int)threadIdx.x * chunk), c1 = min(span, c0 + chunk);
+        int mine = 0;
+        for (int c = c0; c < c1; ++c) mine += (hit[c] && fabs(acc[c]) > kEps * kEps) ? 1 : 0;
+        int incl = mine;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        if (lane == 31) s_warp[wid] = incl;
+        __syncthreads();
+        int before = 0, total = 0;
+        for (int w = 0; w < nw; ++w) {
+            if (w < wid) before += s_warp[w];
+            total += s_warp[w];
+        }
+        before += incl - mine;
+        if (ccnt && threadIdx.x == 0) ccnt[i] = total;
+        if (FILL) {
+            int o = crp[i] + before;
+            for (int c = c0; c < c1; ++c)
+                if (hit[c] && fabs(acc[c]) > kEps * kEps) {
+                    cci[o] = lo + c;
                     cv[o] = acc[c];
                     ++o;
                 }
@@ -1360,6 +1444,8 @@ bool raise_row_kernel_limits() {
     raise_smem_limit(k_t_sort_rows);
     raise_smem_limit(k_spgemm_warp<false>);
     raise_smem_limit(k_spgemm_warp<true>);
+    raise_smem_limit(k_spgemm_window<false>);
+    raise_smem_limit(k_spgemm_window<true>);
     return true;
 }
 
@@ -1440,15 +1526,19 @@ void spgemm(Ctx& ctx, const Csr<double>& A, const Csr<double>& B, DCsr& C) {
     cudaStream_t s = ctx.lane.stream;
     const int g = grid_for(ctx, A.n);
     DBuf<int> heads(3LL * std::max(A.nnz, 1));
-    DBuf<int> cnt(std::max(A.n, 1)), cls(std::max(A.n, 1)), list(3LL * std::max(A.n, 1)), meta(5);
+    DBuf<int> cnt(std::max(A.n, 1)), cls(std::max(A.n, 1)), list(4LL * std::max(A.n, 1)), meta(7);
+    DBuf<int> wlo(std::max(A.n, 1)), wspan(std::max(A.n, 1));
     meta.zero(s);
     if (A.n)
-        k_spgemm_classify<<<g, 256, 0, s>>>(A.n, A.rp, A.ci, B.rp, B.m, cls.p, list.p, meta.p);
+        k_spgemm_classify<<<g, 256, 0, s>>>(A.n, A.rp, A.ci, B.rp, B.ci, B.m, cls.p, list.p, meta.p, wlo.p,
+                                            wspan.p);
     HAMLSS_LAUNCH_CHECK();
-    int hm[5] = {0, 0, 0, 0, 0};
-    meta.download(hm, 5, s);
+    int hm[7] = {0, 0, 0, 0, 0, 0, 0};
+    meta.download(hm, 7, s);
     HAMLSS_CUDA(cudaStreamSynchronize(s));
-    const int nlong = hm[0], ndense = hm[2], nwarp = hm[3];
+    const int nlong = hm[0], ndense = hm[2], nwarp = hm[3], nwin = hm[5];
+    const int* winlist = list.p + 3LL * A.n;
+    const size_t winsmem = 9 * (size_t)std::max(hm[6], 1);   // window accumulator + hit flags
     int KH = 32;
     while (KH < hm[4]) KH <<= 1;
     const size_t wsmem = sizeof(int) * 3 * (size_t)KH * kMergeWarps;
@@ -1497,6 +1587,13 @@ void spgemm(Ctx& ctx, const Csr<double>& A, const Csr<double>& B, DCsr& C) {
                                                                   B.ci, B.v, cnt.p, off.p, wci.p, wv.p);
                 HAMLSS_LAUNCH_CHECK();
             }
+            if (nwin) {
+                const int gb = row_grid(ctx, k_spgemm_window<true>, winsmem, nwin);
+                k_spgemm_window<true><<<gb, kRowBlock, winsmem, s>>>(winlist, nwin, hm[6], wlo.p, wspan.p,
+                                                                     A.rp, A.ci, A.v, B.rp, B.ci, B.v,
+                                                                     cnt.p, off.p, wci.p, wv.p);
+                HAMLSS_LAUNCH_CHECK();
+            }
             build_csr_counts(ctx, C, A.n, B.m, cnt);
             if (A.n)
                 k_spgemm_compact<<<std::max(1, std::min(ceil_div(A.n, 8), ctx.sm_count * 16)), 256, 0, s>>>(
@@ -1526,6 +1623,13 @@ void spgemm(Ctx& ctx, const Csr<double>& A, const Csr<double>& B, DCsr& C) {
                                                            B.v, cnt.p, nullptr, nullptr, nullptr);
         HAMLSS_LAUNCH_CHECK();
     }
+    if (nwin) {
+        const int gb = row_grid(ctx, k_spgemm_window<false>, winsmem, nwin);
+        k_spgemm_window<false><<<gb, kRowBlock, winsmem, s>>>(winlist, nwin, hm[6], wlo.p, wspan.p, A.rp, A.ci,
+                                                              A.v, B.rp, B.ci, B.v, cnt.p, nullptr, nullptr,
+                                                              nullptr);
+        HAMLSS_LAUNCH_CHECK();
+    }
     build_csr_counts(ctx, C, A.n, B.m, cnt);
     k_spgemm<true><<<g, 256, 0, s>>>(A.n, A.rp, A.ci, A.v, B.rp, B.ci, B.v, nullptr, C.rp.p, C.ci.p,
                                      C.v.p, heads.p, cls.p);
@@ -1546,6 +1650,13 @@ void spgemm(Ctx& ctx, const Csr<double>& A, const Csr<double>& B, DCsr& C) {
         const int gb = row_grid(ctx, k_spgemm_dense<true>, dsmem, ndense);
         k_spgemm_dense<true><<<gb, kRowBlock, dsmem, s>>>(dlist, ndense, B.m, A.rp, A.ci, A.v, B.rp, B.ci,
                                                           B.v, nullptr, C.rp.p, C.ci.p, C.v.p);
+        HAMLSS_LAUNCH_CHECK();
+    }
+    if (nwin) {
+        const int gb = row_grid(ctx, k_spgemm_window<true>, winsmem, nwin);
+        k_spgemm_window<true><<<gb, kRowBlock, winsmem, s>>>(winlist, nwin, hm[6], wlo.p, wspan.p, A.rp, A.ci,
+                                                             A.v, B.rp, B.ci, B.v, nullptr, C.rp.p, C.ci.p,
+                                                             C.v.p);
         HAMLSS_LAUNCH_CHECK();
     }
 }

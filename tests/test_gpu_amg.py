@@ -98,6 +98,15 @@ def test_hierarchy_bitwise_large_vs_oracle(orc):
     assert_same_hierarchy(hierarchy(M), orc.amg_hierarchy(*A))
 
 
+def test_hierarchy_bitwise_wide_coarse_vs_oracle(orc):
+    # 1024^2: coarse operators with more columns (132,780 and 35,719) than a shared-memory
+    # accumulator holds, where long Galerkin rows take the windowed accumulator
+    A = P.varkappa_poisson_2d(1024, 1.0, 2)
+    M = H.AMGPreconditioner()
+    M.setup(dev(A))
+    assert_same_hierarchy(hierarchy(M), orc.amg_hierarchy(*A))
+
+
 @pytest.mark.parametrize("name,A", SMALL, ids=SIDS)
 def test_vcycle_bitwise_vs_reference(ref, name, A):
     n = len(A[0]) - 1
