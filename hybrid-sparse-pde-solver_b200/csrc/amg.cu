@@ -534,12 +534,11 @@ __global__ void k_spgemm_classify(int m, const int* __restrict__ arp, const int*
         const long long h = u < bcols ? u : bcols;
         const bool lng = k > kHeads || u > 512;
         // dense accumulation pays one barrier per left entry: worth it when the right rows
-        // are long (>= 64 products a step, or >= 32 over a window of the columns); the warp
-        // merge pays per output column
+        // are long (>= 32 products a step); over the window of columns the row can reach it
+        // also scans only that window.  The warp merge pays per output column
         const bool dense_ok = bcols <= kDenseCols && h > kHashMax / 4;
         int c = 0;
-        if (lng && dense_ok && u >= 64LL * k) c = 2;
-        else if (lng && !dense_ok && span <= kDenseCols && u >= 32LL * k && h > kHashMax / 4) c = 4;
+        if (lng && span <= kDenseCols && u >= 32LL * k && h > kHashMax / 4) c = 4;
         else if (lng && k <= kWarpMergeK) c = 3;
         else if (lng && dense_ok) c = 2;
         else if (lng && h <= kHashMax) c = 1;
