@@ -240,8 +240,9 @@ __global__ void k_trsm_lower_unit(int n, int k0, int kb, const double* __restric
 }
 
 // Inverses of the factors of diagonal block b (k0 = b * kNb): Li = L11^-1 (unit lower) and
-// Ui = U11^-1 (upper), kb x kb row-major with ld kNb at inv + 2 * b * kNb * kNb.  Thread c
-// solves column c (substitution in the factor's row order); the block is in shared memory.
+// Ui = U11^-1 (upper), kb x kb row-major with ld kNb at inv + 2 * b * kNb * kNb; blockIdx.y
+// 0 forms Li, 1 forms Ui.  Thread c solves column c (substitution in the factor's row
+// order); the block is in shared memory.
 __global__ void k_block_inverses(int n, int b0, const double* __restrict__ M, double* inv) {
     __shared__ double a[kNb][kNb + 1];
     const int b = b0 + blockIdx.x;
@@ -254,13 +255,15 @@ __global__ void k_block_inverses(int n, int b0, const double* __restrict__ M, do
     }
     __syncthreads();
     const int c = threadIdx.x;
-    if (c < kb) {
+    if (c < kb && blockIdx.y == 0) {
         for (int r = 0; r < kb; ++r) {              // L x = e_c
             double acc = (r == c) ? 1.0 : 0.0;
             if (r > c)
                 for (int q = c; q < r; ++q) acc = __dsub_rn(acc, __dmul_rn(a[r][q], Li[q * kNb + c]));
             Li[r * kNb + c] = r < c ? 0.0 : acc;
         }
+    }
+    if (c < kb && blockIdx.y == 1) {
         for (int r = kb - 1; r >= 0; --r) {         // U x = e_c
             double acc = (r == c) ? 1.0 : 0.0;
             if (r <= c) {
@@ -353,7 +356,7 @@ bool factor_nopivot(Ctx& ctx, cublasHandle_t h, int n, double* M, double floor, 
     for (int k0 = 0; k0 < n; k0 += kNb) {
         const int kb = std::min(kNb, n - k0);
         k_lu_diag_nopiv<<<1, 256, 0, s>>>(n, k0, kb, M, floor, tiny.p);
-        k_block_inverses<<<1, kNb, 0, s>>>(n, k0 / kNb, M, inv);
+        k_block_inverses<<<dim3(1, 2), kNb, 0, s>>>(n, k0 / kNb, M, inv);
         HAMLSS_LAUNCH_CHECK();
         const int rest = n - k0 - kb;
         if (rest > 0) {
@@ -441,7 +444,7 @@ void dense_lu_inverse(Ctx& ctx, int n, double* M, double* Minv, int* piv) {
     } else {
         HAMLSS_CUDA(cudaMemcpyAsync(M, Minv, bytes, cudaMemcpyDeviceToDevice, s));
         factor_pivot(ctx, h, n, M, piv);
-        k_block_inverses<<<nblk, kNb, 0, s>>>(n, 0, M, inv.p);
+        k_block_inverses<<<dim3(nblk, 2), kNb, 0, s>>>(n, 0, M, inv.p);
         HAMLSS_LAUNCH_CHECK();
     }
     // X = P I; L Y = X (forward, unit lower); U X = Y (backward).  The diagonal blocks are
