@@ -477,6 +477,54 @@ __device__ __forceinline__ int heap_pop(int* h, int& nh) {
     return top;
 }
 
+// The work-row slots that are active, at least tau in magnitude and below (lower) or above
+// column i, gathered by the warp into dst[0..count) and sorted by column (warp bitonic sort;
+// columns are distinct).  dst must hold the next power of two >= count entries.
+__device__ int ilut_gather_sorted(const int* scol, const double* sval, const unsigned char* sact, int nt,
+                                  int i, double tau, bool lower, IlutEntry* dst, int lane) {
+    int cnt = 0;
+    for (int b0 = 0; b0 < nt; b0 += 32) {
+        const int t = b0 + lane;
+        bool take = false;
+        int c = 0;
+        double v = 0.0;
+        if (t < nt) {
+            c = scol[t];
+            v = sval[t];
+            take = sact[t] && fabs(v) >= tau && (lower ? c < i : c > i);
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, take);
+        if (take) {
+            const int q = cnt + __popc(m & ((1u << lane) - 1u));
+            dst[q].col = c;
+            dst[q].val = v;
+        }
+        cnt += __popc(m);
+    }
+    int N = 1;
+    while (N < cnt) N <<= 1;
+    for (int t = cnt + lane; t < N; t += 32) {
+        dst[t].col = INT_MAX;
+        dst[t].val = 0.0;
+    }
+    __syncwarp();
+    for (int kk = 2; kk <= N; kk <<= 1)
+        for (int jj = kk >> 1; jj > 0; jj >>= 1) {
+            for (int t = lane; t < N; t += 32) {
+                const int p = t ^ jj;
+                if (p > t) {
+                    const IlutEntry x = dst[t], y = dst[p];
+                    if ((x.col > y.col) == ((t & kk) == 0)) {
+                        dst[t] = y;
+                        dst[p] = x;
+                    }
+                }
+            }
+            __syncwarp();
+        }
+    return cnt;
+}
+
 __global__ void __launch_bounds__(32 * kIlutWarps) k_ilut_rows(IlutArgs a) {
     extern __shared__ unsigned char ilut_smem[];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -613,41 +661,48 @@ __global__ void __launch_bounds__(32 * kIlutWarps) k_ilut_rows(IlutArgs a) {
                 __syncwarp();
             }
         }
-        // collect L, the diagonal, U (lane 0) and publish the row
+        // collect L and U (the warp gathers and sorts by column; lane 0 applies the fill
+        // limit, a sequential heap select) and publish the row
+        int nl = ilut_gather_sorted(scol, sval, sact, nt, i, tau, true, row, lane);
+        if (lane == 0) ilut_keep(row, &nl, keep);
+        nl = __shfl_sync(0xffffffffu, nl, 0);
+        __syncwarp();
+        const int o = a.off[i];
+        for (int t = lane; t < nl; t += 32) {
+            a.ecol[o + t] = row[t].col;
+            a.eval[o + t] = row[t].val;
+        }
+        __syncwarp();                                  // row[] is reused for U
+        double diag = 0.0;
+        for (int b0 = 0; b0 < nt; b0 += 32) {
+            const int t = b0 + lane;
+            const unsigned m = __ballot_sync(0xffffffffu, t < nt && scol[t] == i);
+            if (m) {
+                diag = __shfl_sync(0xffffffffu, t < nt ? sval[t] : 0.0, __ffs(m) - 1);
+                break;
+            }
+        }
+        if (fabs(diag) < 2.220446049250313e-16) diag = (diag >= 0 ? 1.0 : -1.0) * 2.220446049250313e-16 * 1e6;
+        int nu = 1 + ilut_gather_sorted(scol, sval, sact, nt, i, tau, false, row + 1, lane);
         if (lane == 0) {
-            int nl = 0;
-            for (int t = 0; t < nt; ++t)
-                if (scol[t] < i && sact[t] && fabs(sval[t]) >= tau) { row[nl].col = scol[t]; row[nl].val = sval[t]; ++nl; }
-            for (int x = 1; x < nl; ++x) {
-                IlutEntry e = row[x];
-                int y = x - 1;
-                while (y >= 0 && row[y].col > e.col) { row[y + 1] = row[y]; --y; }
-                row[y + 1] = e;
-            }
-            ilut_keep(row, &nl, keep);
-            const int o = a.off[i];
-            for (int t = 0; t < nl; ++t) { a.ecol[o + t] = row[t].col; a.eval[o + t] = row[t].val; }
-            double diag = 0.0;
-            for (int t = 0; t < nt; ++t)
-                if (scol[t] == i) { diag = sval[t]; break; }
-            if (fabs(diag) < 2.220446049250313e-16) diag = (diag >= 0 ? 1.0 : -1.0) * 2.220446049250313e-16 * 1e6;
-            int nu = 0;
-            row[nu].col = i; row[nu].val = diag; ++nu;
-            const int first = nu;
-            for (int t = 0; t < nt; ++t)
-                if (scol[t] > i && sact[t] && fabs(sval[t]) >= tau) { row[nu].col = scol[t]; row[nu].val = sval[t]; ++nu; }
-            for (int x = first + 1; x < nu; ++x) {
-                IlutEntry e = row[x];
-                int y = x - 1;
-                while (y >= first && row[y].col > e.col) { row[y + 1] = row[y]; --y; }
-                row[y + 1] = e;
-            }
+            row[0].col = i;
+            row[0].val = diag;
             ilut_keep(row, &nu, keep);
-            for (int t = 0; t < nu; ++t) { a.ecol[o + half + t] = row[t].col; a.eval[o + half + t] = row[t].val; }
+        }
+        nu = __shfl_sync(0xffffffffu, nu, 0);
+        __syncwarp();
+        for (int t = lane; t < nu; t += 32) {
+            a.ecol[o + half + t] = row[t].col;
+            a.eval[o + half + t] = row[t].val;
+        }
+        if (lane == 0) {
             a.lcnt[i] = nl;
             a.ucnt[i] = nu;
             if (overflow) atomicExch(a.err, 2);
-            __threadfence();
+        }
+        __threadfence();                               // every lane's entries, then the flag
+        __syncwarp();
+        if (lane == 0) {
             *(volatile int*)(a.done + i) = 1;
             atomicAdd(a.finished, 1);
         }
