@@ -64,6 +64,9 @@ def parse():
     ap.add_argument("--serving-requests", type=int, default=200,
                     help="requests in the serving stream (0 skips the serving measurement)")
     ap.add_argument("--serving-n-max", type=float, default=2.6e5)
+    ap.add_argument("--no-batch", action="store_true",
+                    help="skip the batched-systems side measurement (4096 uneven systems)")
+    ap.add_argument("--batch-count", type=int, default=4096)
     ap.add_argument("--no-variants", action="store_true",
                     help="skip the Krylov-variant side measurement (s-step CG, pipelined FGMRES)")
     ap.add_argument("--no-ilut", action="store_true",
@@ -729,6 +732,77 @@ def run_ilut_side(args, local):
             "device_1024": big}
 
 
+def run_batch_side(args, local):
+    """Batched uneven systems: `count` problems with side s ~ U{16..128}, half
+    variable-kappa Poisson (sigma 0.5; CG + Jacobi), half upwind conv-diff (cell Peclet
+    log-uniform in [1, 100]; FGMRES(20) + ILU(0)), rhs U[0, 1), rtol 1e-8, FP32 inner
+    iterations inside FP64 refinement -- all of them in one persistent launch.  Beside it:
+    one solve call per problem through the C ABI (a sample of 256, scaled), and the
+    reference's own solvers one after another on a sample of 64 (scaled)."""
+    import hsps_b200 as H
+    import oracle
+    from hsps_b200 import batch as B
+    from hsps_b200 import problems as P
+    from hsps_b200._abi import default_params
+
+    count = args.batch_count
+    rng = np.random.default_rng(2024)
+    systems, solvers, precs, rhs = [], [], [], []
+    for k in range(count):
+        side = int(rng.integers(16, 129))
+        if k % 2 == 0:
+            systems.append(P.varkappa_poisson_2d(side, 0.5, 7000 + k))
+            solvers.append(H.SOLVER_CG)
+            precs.append(H.PREC_JACOBI)
+        else:
+            pe = float(np.exp(rng.uniform(0.0, np.log(100.0))))
+            systems.append(P.convection_diffusion_2d(side, 1.0, *P.convdiff_wind(side, pe)))
+            solvers.append(H.SOLVER_FGMRES)
+            precs.append(H.PREC_ILU)
+        rhs.append(P.rhs(side * side, 9000 + k))
+    p = default_params(tol=1e-8, max_iter=4000, restart_size=20, drop_tol=0.0)
+    n_tot = sum(len(sy[0]) - 1 for sy in systems)
+    nnz_tot = sum(len(sy[2]) for sy in systems)
+    bs = B.BatchSolver(systems, solvers, precs, p)
+    bflat = bs.join(rhs)
+    bs.solve(bflat)                                          # warm-up (autotune defaults)
+    times = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        x, res, tot = bs.solve(bflat)
+        times.append(time.perf_counter() - t0)
+    conv = sum(r["converged"] for r in res)
+    worst = max(r["final_residual"] for r in res)
+    bs.release()
+    batch_s = float(np.median(times))
+    # one solve call per problem (host buffers), a sample
+    ctx = H.Context(local)
+    sample = list(range(0, count, max(1, count // 256)))[:256]
+    t0 = time.perf_counter()
+    for k in sample:
+        rp, ci, v = systems[k]
+        n = len(rp) - 1
+        M = H.SparseMatrix(n, n, rp, ci, v, ctx)
+        s, _ = H.SolverFactory.make(solvers[k], precs[k], M, p)
+        x = np.zeros(n)
+        s.solve(M, rhs[k], x)
+    loop_s = (time.perf_counter() - t0) * count / len(sample)
+    R = oracle.Reference(fast=True, threads=1)
+    rsample = sample[:64]
+    t0 = time.perf_counter()
+    for k in rsample:
+        R.solve(0 if solvers[k] == H.SOLVER_CG else 1, 1 if precs[k] == H.PREC_JACOBI else 2,
+                *systems[k], rhs[k], params=p)
+    ref_s = (time.perf_counter() - t0) * count / len(rsample)
+    return {"problem": f"{count} systems, side U{{16..128}}, half var-kappa Poisson (CG+Jacobi), "
+                       "half upwind conv-diff Pe 1-100 (FGMRES(20)+ILU(0)), rtol 1e-8",
+            "rows": n_tot, "nnz": nnz_tot, "converged": conv, "max_final_residual": worst,
+            "batch_s": round(batch_s, 4), "batch_solves_per_s": round(count / batch_s, 1),
+            "one_call_per_problem_s": round(loop_s, 3), "one_call_sample": len(sample),
+            "reference_sequential_s": round(ref_s, 3), "reference_sample": len(rsample),
+            "reference_threads": 1}
+
+
 def run_variants_side(args, local):
     """CG, FGMRES(30), PipelinedFGMRES(30) (Jacobi) and SStepCG(k = 4) on the unit-diagonal
     shifted Helmholtz operator D^-1/2 (A + cI) D^-1/2 on 512^2 (c = 7; a spectrum inside
@@ -797,6 +871,9 @@ def main():
         log("cpu baseline done")
     if rank == 0 and world == 1 and args.serving_requests > 0:
         out["serving"] = run_serving(args, local)
+    if rank == 0 and world == 1 and not args.no_batch:
+        log("batched-systems side measurement")
+        out["batched"] = run_batch_side(args, local)
     if rank == 0 and world == 1 and not args.no_variants:
         log("Krylov-variant side measurement")
         out["krylov_variants"] = run_variants_side(args, local)
