@@ -64,6 +64,8 @@ def parse():
     ap.add_argument("--serving-requests", type=int, default=200,
                     help="requests in the serving stream (0 skips the serving measurement)")
     ap.add_argument("--serving-n-max", type=float, default=2.6e5)
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the C1 / C2 latency side measurement")
     ap.add_argument("--no-batch", action="store_true",
                     help="skip the batched-systems side measurement (4096 uneven systems)")
     ap.add_argument("--batch-count", type=int, default=4096)
@@ -732,6 +734,48 @@ def run_ilut_side(args, local):
             "device_1024": big}
 
 
+def run_config_side(args, local):
+    """Latency of one complete solve call (host buffers in, solution out; preconditioner
+    setup included) for the small configurations: C1 Poisson 64^2 PCG + Jacobi and C2
+    upwind conv-diff 512^2 (cell Peclet 10) FGMRES(30) + ILU(0), both to rtol 1e-8 -- the
+    device (median of 10) against the reference's own solvers (all host threads, median of
+    3)."""
+    import hsps_b200 as H
+    import oracle
+    from hsps_b200 import problems as P
+    from hsps_b200._abi import default_params
+
+    R = oracle.Reference(fast=True, threads=cpu_threads())
+    ctx = H.Context(local)
+    out = {"reference_threads": cpu_threads()}
+    cases = (("C1_poisson64_pcg_jacobi", P.poisson_2d(64), 0, "CG", "JACOBI",
+              default_params(tol=1e-8, max_iter=1000)),
+             ("C2_convdiff512_pe10_fgmres30_ilu0",
+              P.convection_diffusion_2d(512, 1.0, *P.convdiff_wind(512, 10.0)), 2, "FGMRES", "ILU",
+              default_params(tol=1e-8, max_iter=3000, restart_size=30, drop_tol=0.0)))
+    for name, A, seed, sname, pname, p in cases:
+        n = len(A[0]) - 1
+        b = P.rhs(n, seed)
+        dev = []
+        for _ in range(11):
+            t0 = time.perf_counter()
+            M = H.SparseMatrix(n, n, *A, ctx)
+            s, _ = H.SolverFactory.make(sname, pname, M, p)
+            x = np.zeros(n)
+            st = H.SolverStats()
+            s.solve(M, b, x, st)
+            dev.append(time.perf_counter() - t0)
+        ref = []
+        for _ in range(3):
+            t0 = time.perf_counter()
+            rc, xr, sr = R.solve(0 if sname == "CG" else 1, 1 if pname == "JACOBI" else 2, *A, b, params=p)
+            ref.append(time.perf_counter() - t0)
+        out[name] = {"n": n, "nnz": len(A[2]), "device_ms": round(1e3 * float(np.median(dev[1:])), 3),
+                     "iterations": st.iterations, "reference_ms": round(1e3 * float(np.median(ref)), 3),
+                     "reference_iterations": sr.iterations}
+    return out
+
+
 def run_batch_side(args, local):
     """Batched uneven systems: `count` problems with side s ~ U{16..128}, half
     variable-kappa Poisson (sigma 0.5; CG + Jacobi), half upwind conv-diff (cell Peclet
@@ -871,6 +915,9 @@ def main():
         log("cpu baseline done")
     if rank == 0 and world == 1 and args.serving_requests > 0:
         out["serving"] = run_serving(args, local)
+    if rank == 0 and world == 1 and not args.no_configs:
+        log("C1 / C2 latency side measurement")
+        out["configs"] = run_config_side(args, local)
     if rank == 0 and world == 1 and not args.no_batch:
         log("batched-systems side measurement")
         out["batched"] = run_batch_side(args, local)
