@@ -355,7 +355,7 @@ def run_ours(args, rank, world, local):
     value = replica_throughput(args.steps, world, max_ms)
 
     # ---- solve phase alone, hierarchy resident: mixed precision against all-FP64 on the
-    #      same AMG hierarchy (the north-star comparison of the two arithmetic schemes)
+    #      same AMG hierarchy (the two arithmetic schemes compared on equal terms)
     solve_only = None
     if ptype == H.PREC_AMG:
         h = C.c_void_p()

@@ -696,7 +696,7 @@ int hamlss_solve_adaptive(hamlss_ctx* ctx, const hamlss_mat* A, const double* b,
             // mode 1: the device-side checks escalate the lower rungs; mode 2: they also end
             // the top rung early on a stall or divergence (its caller then decides)
             lad.on = (p.ladder_mode == 1 && state != HAMLSS_STATE_HARD) || p.ladder_mode >= 2;
-            // mode 3: the CG rung is judged by the divergence and budget rules only
+            // mode 3: the CG rung escalates on the divergence and budget rules only
             lad.no_stall = p.ladder_mode == 3 && solver == HAMLSS_SOLVER_CG;
             lad.state = state;
             lad.window = p.stall_window;
