@@ -26,8 +26,9 @@ def test_struct_layouts_match_header():
     import subprocess, tempfile
     src = (
         '#include <stdio.h>\n#include "hamlss.h"\n'
-        'int main(){printf("%zu %zu %zu\\n", sizeof(hamlss_params), sizeof(hamlss_stats),'
-        ' sizeof(hamlss_escalation));return 0;}\n')
+        'int main(){printf("%zu %zu %zu %zu %zu %zu\\n", sizeof(hamlss_params), sizeof(hamlss_stats),'
+        ' sizeof(hamlss_escalation), sizeof(hamlss_server_config), sizeof(hamlss_server_report),'
+        ' sizeof(hamlss_batch_result));return 0;}\n')
     with tempfile.TemporaryDirectory() as d:
         c = os.path.join(d, "s.c")
         open(c, "w").write(src)
@@ -35,7 +36,28 @@ def test_struct_layouts_match_header():
         subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), c, "-o", exe], check=True)
         out = subprocess.run([exe], capture_output=True, text=True, check=True).stdout.split()
     assert [int(x) for x in out] == [ctypes.sizeof(_abi.Params), ctypes.sizeof(_abi.Stats),
-                                     ctypes.sizeof(_abi.Escalation)]
+                                     ctypes.sizeof(_abi.Escalation), ctypes.sizeof(_abi.ServerConfig),
+                                     ctypes.sizeof(_abi.ServerReport), ctypes.sizeof(_abi.BatchResult)]
+
+
+def test_server_config_defaults():
+    c = _abi.ServerConfig()
+    _abi.lib().hamlss_server_config_default(ctypes.byref(c))
+    assert (c.device, c.slots, c.hbm_budget_bytes, c.batch_max_rows, c.batch_max_count, c.order) == \
+           (0, 4, 150 * 10**9, 16384, 2048, 0)
+
+
+def test_solver_classes_mirror_reference():
+    # PipelinedFGMRESSolver has no SolverType and reports FGMRES; SStepCGSolver(k = 4)
+    # (sstep_cg_solver.hpp:57-60) is made by the factory with params.sstep_k
+    import hsps_b200 as H
+    assert H.PipelinedFGMRESSolver.solver_type == _abi.SOLVER_PIPELINED_FGMRES == 5
+    assert H.SStepCGSolver().k == 4
+    s = H.SolverFactory.make_solver(H.SolverFactory.parse_solver("s-step"), _abi.default_params(sstep_k=6))
+    assert isinstance(s, H.SStepCGSolver) and s.k == 6 and s.type() == _abi.SOLVER_SSTEP_CG
+    import pytest
+    with pytest.raises(ValueError):
+        H.SolverFactory.make_solver(H.SolverFactory.parse_solver("async"), _abi.default_params())
 
 
 def test_params_default_matches_reference_defaults():
