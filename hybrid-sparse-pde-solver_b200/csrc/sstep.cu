@@ -260,6 +260,7 @@ SolveResult sstep_solve(Ctx& ctx, hamlss_mat* A, const double* b, double* x, con
     const double lam_max = std::max(hi, lam_min * 2.0);
     // Y = [r, B_0 .. B_{k-1}] as columns of ld entries; Ap for the fallback step
     const long long ld = ((long long)n + 31) / 32 * 32;
+    if (ld > INT_MAX) fail(HAMLSS_ERR_SIZE, "s-step basis larger than 2^31 rows");
     ws.basis.ensure((size_t)ld * (size_t)(k + 1));
     double* Y = ws.basis.p;
     double* r = Y;
@@ -327,7 +328,6 @@ SolveResult sstep_solve(Ctx& ctx, hamlss_mat* A, const double* b, double* x, con
         HAMLSS_CUDA(cudaMemcpyAsync(G.data(), Gd, sizeof(double) * G.size(), cudaMemcpyDeviceToHost, st));
         HAMLSS_CUDA(cudaStreamSynchronize(st));
     };
-    if ((long long)ld > INT_MAX) fail(HAMLSS_ERR_SIZE, "s-step basis larger than 2^31 rows");
     while (total < p.max_iter && rel > p.tol) {
         int kb = k;
         build(kb);
