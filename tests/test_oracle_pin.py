@@ -341,3 +341,17 @@ def test_kat_pipelined_fgmres(orc):
     assert np.linalg.norm(x_std - x_pip) / np.linalg.norm(x_std) < 1e-5
     C = P.convection_diffusion_2d(10, 0.1, 5.0, 0.0)
     assert orc.solve(5, 2, *C, np.ones(100), params=p)[0] == 1
+
+
+def test_oracle_pipelined_lucky_breakdown_equals_reference(orc, ref):
+    # b along an eigenvector: h_10 = 0 exactly; the pipelined cycle leaves before rotating
+    # that column and restarts once (pipelined_fgmres_solver.cpp:117-123)
+    A = (np.arange(5, dtype=np.int32), np.arange(4, dtype=np.int32), np.array([2.0, 3.0, 5.0, 7.0]))
+    b = np.array([2.0, 0.0, 0.0, 0.0])
+    p = default_params(tol=1e-10, max_iter=50, restart_size=4, drop_tol=0.0)
+    o, r = orc.solve(5, 0, *A, b, params=p), ref.solve(5, 0, *A, b, params=p)
+    assert (o[2].converged, o[2].iterations, o[2].restarts) == (r[2].converged, r[2].iterations,
+                                                                 r[2].restarts) == (1, 1, 1)
+    assert np.array_equal(o[1], r[1])
+    s = orc.solve(1, 0, *A, b, params=p)[2]
+    assert (s.iterations, s.restarts) == (1, 0)
