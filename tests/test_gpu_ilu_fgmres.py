@@ -106,6 +106,16 @@ def test_ilut_factor_and_apply_bitwise(orc, name, A, dt, fp):
     assert rc == 0 and np.array_equal(I.apply(r), z)
 
 
+def test_ilut_edge_cases_bitwise(orc):
+    # an empty row, tiny diagonals the fill limit may drop, equal magnitudes (tie order)
+    from test_oracle_pin import ILUT_EDGE_SETTINGS, ilut_edge_cases
+    for name, A in ilut_edge_cases():
+        for dt, fp in ILUT_EDGE_SETTINGS:
+            M, I = ilut(A, dt, fp)
+            for g, w in zip(I.factor_csr(), orc.ilut(*A, dt, fp)):
+                assert np.array_equal(g, w), (name, dt, fp)
+
+
 def test_ilut_large_wavefront(orc):
     # 65k rows: thousands of rows in flight at once, each waiting on the rows it eliminates
     bx, by = P.convdiff_wind(256, 30.0)

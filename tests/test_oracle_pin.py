@@ -355,3 +355,29 @@ def test_oracle_pipelined_lucky_breakdown_equals_reference(orc, ref):
     assert np.array_equal(o[1], r[1])
     s = orc.solve(1, 0, *A, b, params=p)[2]
     assert (s.iterations, s.restarts) == (1, 0)
+
+
+def ilut_edge_cases():
+    """ILUT corner cases: an empty row, tiny diagonals under large off-diagonals (the fill
+    limit can drop a diagonal, and later rows then skip that pivot), and equal magnitudes
+    (the heap select's tie order)."""
+    rng = np.random.default_rng(5)
+    n, r, c, v = 40, [], [], []
+    for i in range(n):
+        r.append(i); c.append(i); v.append(1e-3 if i % 3 == 0 else 4.0)
+        for j in rng.choice(n, 6, replace=False):
+            if j != i:
+                r.append(i); c.append(int(j)); v.append(float(rng.choice([-1.0, 1.0, 2.0])))
+    yield "empty_row", coo_csr(4, [0, 0, 1, 1, 3, 3], [0, 3, 0, 1, 1, 3], [4.0, 1.0, 1.0, 4.0, 2.0, 5.0])
+    yield "small_diag", coo_csr(n, r, c, v)
+    yield "poisson_ties", P.poisson_2d(12)
+
+
+ILUT_EDGE_SETTINGS = [(1e-4, 0), (1e3, 0), (1e-2, 2), (1e-8, 20), (0.5, 0)]
+
+
+@pytest.mark.parametrize("name,A", list(ilut_edge_cases()), ids=[c[0] for c in ilut_edge_cases()])
+def test_oracle_ilut_edge_cases_equal_reference(orc, ref, name, A):
+    for dt, fp in ILUT_EDGE_SETTINGS:
+        for x, y in zip(orc.ilut(*A, dt, fp), ref.ilut(*A, dt, fp)):
+            assert np.array_equal(x, y), (dt, fp)
