@@ -59,6 +59,34 @@ def main():
                                             s.initial_residual], np.float64)
         f, st = ref.features(rp, ci, v)
         out["features"], out["initial_state"] = f, np.int32(st)
+        # ILUT factors (ilu.cpp:94-220) at two settings
+        for tag, dt, fp in (("ilut_a", 1e-4, 0), ("ilut_b", 1e-3, 5)):
+            frp, fci, flu = ref.ilut(rp, ci, v, dt, fp)
+            out[f"{tag}_rp"], out[f"{tag}_ci"], out[f"{tag}_v"] = frp, fci, flu
+        # PipelinedFGMRESSolver with ILU(0) and with Jacobi
+        for prec, tag in ((2, "pfgmres_ilu"), (1, "pfgmres_jacobi")):
+            p = default_params(drop_tol=0.0, tol=1e-8, max_iter=1000, restart_size=20)
+            rc, x, s = ref.solve(5, prec, rp, ci, v, b, params=p)
+            out[f"{tag}_x"] = x
+            out[f"{tag}_stats"] = np.array([rc, s.iterations, s.final_residual, s.restarts,
+                                            s.flop_count, s.mem_bytes], np.float64)
+        # SStepCGSolver(k = 4) on the unit-diagonal scaling D^-1/2 A D^-1/2, and the
+        # spectral interval it uses
+        rows = np.repeat(np.arange(len(rp) - 1), np.diff(rp))
+        dsc = 1.0 / np.sqrt(np.abs(v[ci == rows]))
+        vs = v * dsc[rows] * dsc[ci]
+        out["unit_v"] = vs
+        out["spectral_interval"] = np.array(ref.spectral_interval(rp, ci, vs, 20))
+        p = default_params(tol=1e-8, max_iter=400, sstep_k=4)
+        rc, x, s = ref.solve(3, 1, rp, ci, vs, b, params=p)
+        out["sstep_x"] = x
+        out["sstep_stats"] = np.array([rc, s.iterations, s.final_residual, s.comm_bytes, s.sstep_k,
+                                       s.flop_count], np.float64)
+        # the adaptive ladder under the default drop_tol (ILUT in the MODERATE rung)
+        p = default_params(max_iter=5)
+        rc, x, s, log = ref.solve_adaptive(rp, ci, v, b, params=p)
+        out["ladder_x"] = x
+        out["ladder_stats"] = np.array([rc, s.iterations, s.state_used, len(log)], np.float64)
         np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
         print("wrote", name)
 

@@ -161,6 +161,24 @@ def test_oracle_matches_golden(orc, path):
         assert np.array_equal(x, g[f"{tag}_x"])
     f, st = orc.features(rp, ci, v)
     assert np.array_equal(f, g["features"]) and st == int(g["initial_state"])
+    for tag, dt, fp in (("ilut_a", 1e-4, 0), ("ilut_b", 1e-3, 5)):
+        for x, k in zip(orc.ilut(rp, ci, v, dt, fp), ("rp", "ci", "v")):
+            assert np.array_equal(x, g[f"{tag}_{k}"]), tag
+    for prec, tag in ((2, "pfgmres_ilu"), (1, "pfgmres_jacobi")):
+        p = default_params(drop_tol=0.0, tol=1e-8, max_iter=1000, restart_size=20)
+        rc, x, s = orc.solve(5, prec, rp, ci, v, b, params=p)
+        assert np.array_equal(x, g[f"{tag}_x"])
+        assert [rc, s.iterations, s.final_residual, s.restarts, s.flop_count, s.mem_bytes] == \
+               list(g[f"{tag}_stats"])
+    vs = g["unit_v"]
+    assert np.array_equal(np.array(orc.spectral_interval(rp, ci, vs, 20)), g["spectral_interval"])
+    rc, x, s = orc.solve(3, 1, rp, ci, vs, b, params=default_params(tol=1e-8, max_iter=400, sstep_k=4))
+    assert np.array_equal(x, g["sstep_x"], equal_nan=True)
+    assert [rc, s.iterations, s.comm_bytes, s.sstep_k, s.flop_count] == \
+           [g["sstep_stats"][k] for k in (0, 1, 3, 4, 5)]
+    rc, x, s, log, init = orc.solve_adaptive(rp, ci, v, b, params=default_params(max_iter=5))
+    assert np.array_equal(x, g["ladder_x"])
+    assert [rc, s.iterations, s.state_used, len(log)] == list(g["ladder_stats"])
 
 
 def test_generators_match_oracle(orc):
