@@ -137,7 +137,9 @@ def run_dataset(paths, params=None, verbose: bool = True) -> list:
 
     if isinstance(paths, (str, os.PathLike)) and os.path.isdir(paths):
         paths = MatrixMarketIO.list_mtx_files(paths)
-    p = params or default_params(tol=1e-8, max_iter=2000, drop_tol=0.0)
+    # examples/run_dataset.cpp:305-310: tol 1e-8, max_iter 5000, restart 60, stall window 20;
+    # drop_tol keeps its default (1e-4: the MODERATE rung's ILU is ILUT)
+    p = params or default_params(tol=1e-8, max_iter=5000, restart_size=60, stall_window=20)
     rows = []
     for path in paths:
         name = os.path.splitext(os.path.basename(path))[0]
