@@ -262,3 +262,27 @@ def test_blocked_coarse_lu_pivoting():
     d[np.repeat(np.arange(n), np.diff(rp)), ci] = v
     want = np.linalg.solve(d, r)
     assert np.max(np.abs(z - want)) <= 1e-10 * np.max(np.abs(want))
+
+
+AMG_VARIANTS = [dict(amg_levels=3), dict(amg_strong=0.5), dict(amg_strong=0.08),
+                dict(amg_smooth_pre=1, amg_smooth_post=3)]
+
+
+@pytest.mark.parametrize("over", AMG_VARIANTS,
+                         ids=[",".join(f"{k}={v}" for k, v in o.items()) for o in AMG_VARIANTS])
+def test_amg_parameters_bitwise_vs_oracle(orc, over):
+    # the factory's AMG parameters (solver_factory.cpp:80-88): levels, strength threshold,
+    # pre/post sweeps -- hierarchy bit for bit; the V-cycle bit for bit while the coarsest
+    # level is solved by the same elimination (up to 96 rows), else within rounding (above
+    # 96 rows the engine applies an explicit inverse as a GEMV)
+    A = P.varkappa_poisson_2d(28, 1.0, 13)
+    p = default_params(**over)
+    M = H.SolverFactory.make_precond(H.PREC_AMG, dev(A), p)
+    h = hierarchy(M)
+    assert_same_hierarchy(h, orc.amg_hierarchy(*A, params=p))
+    r = P.rhs(28 * 28, 3, -1.0, 1.0)
+    z, zo = M.apply(r), orc.precond_apply(3, *A, r, p)[1]
+    if h[-1]["A"][0] <= 96:
+        assert np.array_equal(z, zo)
+    else:
+        assert np.max(np.abs(z - zo)) <= 1e-10 * np.max(np.abs(zo))

@@ -399,3 +399,21 @@ def test_oracle_ilut_edge_cases_equal_reference(orc, ref, name, A):
     for dt, fp in ILUT_EDGE_SETTINGS:
         for x, y in zip(orc.ilut(*A, dt, fp), ref.ilut(*A, dt, fp)):
             assert np.array_equal(x, y), (dt, fp)
+
+
+AMG_VARIANTS = [dict(amg_levels=3), dict(amg_strong=0.5), dict(amg_strong=0.08),
+                dict(amg_smooth_pre=1, amg_smooth_post=3)]
+
+
+@pytest.mark.parametrize("over", AMG_VARIANTS, ids=[",".join(f"{k}={v}" for k, v in o.items()) for o in AMG_VARIANTS])
+def test_oracle_amg_parameters_equal_reference(orc, ref, over):
+    # the factory forwards amg_levels, amg_strong and the pre/post sweep counts
+    # (solver_factory.cpp:80-88): hierarchy and V-cycle bit for bit under each
+    A = P.varkappa_poisson_2d(28, 1.0, 13)
+    p = default_params(**over)
+    for l1, l2 in zip(orc.amg_hierarchy(*A, params=p), ref.amg_hierarchy(*A, params=p)):
+        for k in l1:
+            for a, b in zip(l1[k][2:], l2[k][2:]):
+                assert np.array_equal(a, b), k
+    r = P.rhs(28 * 28, 3, -1.0, 1.0)
+    assert np.array_equal(orc.precond_apply(3, *A, r, p)[1], ref.precond_apply(3, *A, r, p)[1])
