@@ -141,3 +141,25 @@ def test_ladder_through_ilut(ref):
            [(e.from_state, e.to_state, e.at_iteration) for e in log] == [(0, 1, 5), (1, 2, 5)]
     assert st.state_used == sr.state_used == 2
     assert abs(st.iterations - sr.iterations) <= 1
+
+
+def test_ladder_mode3_keeps_cg_on_a_nonmonotone_residual():
+    # variable-kappa Poisson (sigma 1.5): CG's recursive residual rises and falls, so the
+    # windowed stall rule of modes 1 / 2 may end CG+Jacobi early; mode 3 judges the CG rung
+    # by divergence and budget only and converges there
+    A = P.varkappa_poisson_2d(128, 1.5, 21)
+    n = 128 * 128
+    M = H.SparseMatrix(n, n, *A)
+    b = P.rhs(n, 4)
+    out = {}
+    for mode in (2, 3):
+        sel = H.AdaptiveSelector(default_params(tol=1e-8, max_iter=4000, drop_tol=0.0, ladder_mode=mode))
+        x = np.zeros(n)
+        st = H.SolverStats()
+        ok = sel.solve(M, b, x, st)
+        out[mode] = (ok, st.state_used, [(e.from_state, e.reason) for e in sel.escalation_log()])
+    ok3, state3, log3 = out[3]
+    assert ok3 and state3 == H.STATE_EASY and log3 == [], out
+    for frm, reason in out[2][2]:
+        if frm == H.STATE_EASY:
+            assert reason == 1, out                     # mode 2 left CG on the stall rule
