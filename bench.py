@@ -60,6 +60,10 @@ def parse():
                     choices=["auto", "cg_jacobi", "amg_fp64", "amg_mixed"])
     ap.add_argument("--n-side", type=int, default=N_SIDE)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-same-algorithm", action="store_true",
+                    help="skip the device vs reference AMG-PCG side measurement at 240^2")
+    ap.add_argument("--no-coarse512", action="store_true",
+                    help="skip the coarsest <= 512 (no stall cut) hierarchy side measurement")
     ap.add_argument("--cpu-sample-iters", type=int, default=40)
     ap.add_argument("--serving-requests", type=int, default=200,
                     help="requests in the serving stream (0 skips the serving measurement)")
@@ -180,20 +184,37 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def own_launches(solver, n_side, steps, profiled_ops):
-    """The engine's kernel launches in the timed region: the per-step count of the ncu
-    launch list (profiles/launch_count.json, library GEMMs excluded) times the steps, for the
-    workload it was counted on; else the engine profiler's operation count (a lower bound:
-    the profiler times outermost operations, and the AMG setup is one of them)."""
-    path = os.path.join(ROOT, "profiles", "launch_count.json")
-    key = f"{solver}_{n_side}"
+def launches_of_one_step(step):
+    """Kernel launches of one step, counted live by the CUDA activity profiler
+    (torch.profiler over CUPTI, which sees every kernel of the process): (engine kernels,
+    library kernels by name, e.g. cuBLAS GEMMs).  None when the profiler yields nothing."""
+    import torch
+    from torch.autograd import DeviceType
+    from torch.profiler import ProfilerActivity, profile
+
     try:
-        d = json.load(open(path)).get(key)
-        if d:
-            return int(d["own_kernels_per_step"]) * steps
-    except (ValueError, OSError, KeyError):
-        pass
-    return profiled_ops
+        torch.cuda.synchronize()
+        with profile(activities=[ProfilerActivity.CUDA]) as prof:
+            step()
+            torch.cuda.synchronize()
+        own, lib = 0, {}
+        for e in prof.events():
+            if e.device_type != DeviceType.CUDA:
+                continue
+            name = e.name
+            low = name.lower()
+            if low.startswith(("memcpy", "memset")):
+                continue
+            if "cutlass" in low or "gemm" in low or "cublas" in low:
+                lib[name] = lib.get(name, 0) + 1
+            else:
+                own += 1
+        if own == 0 and not lib:
+            return None
+        return own, lib
+    except Exception as exc:         # profiler unavailable: report the op count instead
+        log(f"launch count: activity profiler unavailable ({exc})")
+        return None
 
 
 def ncu_traffic(kernel_family):
@@ -260,6 +281,29 @@ def make_params(solver):
     p = H.SolverParams(tol=TOL, max_iter=1000, precision=prec, amg_omega=2.0 / 3.0,
                        amg_coarse_limit=512, amg_levels=25, amg_stall_ratio=STALL)
     return p, H.SOLVER_CG, H.PREC_AMG
+
+
+def workload_name(n_side, solver, hierarchy):
+    base = f"var-kappa Poisson {n_side}^2 5-point, sigma={SIGMA}, rtol {TOL}"
+    if solver == "cg_jacobi":
+        return base + ", PCG + Jacobi (FP64)"
+    prec = "FP32 V-cycle, FP64 refinement" if solver == "amg_mixed" else "FP64"
+    cut = ""
+    if hierarchy:
+        cut = (f", {hierarchy['levels']} levels, coarsest {hierarchy['coarsest_rows']} rows dense "
+               f"(hierarchy cut at the first level keeping > {int(STALL * 100)}% of its rows; "
+               f"<= 512 otherwise)")
+    return base + f", PCG + SA-AMG (theta 0.25, omega 2/3{cut}), {prec}"
+
+
+def amg_config(solver, hierarchy):
+    if solver == "cg_jacobi":
+        return None
+    out = {"theta": 0.25, "omega": 2.0 / 3.0, "coarse_limit": 512, "max_levels": 25,
+           "stall_ratio": STALL, "smooth_pre": 2, "smooth_post": 2}
+    if hierarchy:
+        out.update(hierarchy)
+    return out
 
 
 def run_ours(args, rank, world, local):
@@ -353,10 +397,16 @@ def run_ours(args, rank, world, local):
     total_launches = sum(f[1] for f in fams)
     max_ms = max_over_ranks(dev_ms, "cuda")
     value = replica_throughput(args.steps, world, max_ms)
+    # kernel launches of one more (identical) step, counted by the activity profiler
+    counted = launches_of_one_step(one_solve)
+    if counted is not None:
+        log(f"one step launches {counted[0]} engine kernels and "
+            f"{sum(counted[1].values())} library kernels")
 
     # ---- solve phase alone, hierarchy resident: mixed precision against all-FP64 on the
     #      same AMG hierarchy (the two arithmetic schemes compared on equal terms)
     solve_only = None
+    hierarchy = None
     if ptype == H.PREC_AMG:
         h = C.c_void_p()
         rc = L.hamlss_precond_setup(ctx.h, A.h, ptype, C.byref(params), C.byref(h), None)
@@ -364,6 +414,16 @@ def run_ours(args, rank, world, local):
             raise RuntimeError(L.hamlss_last_error())
         p64 = _abi.Params.from_buffer_copy(params)
         p64.precision = 0
+        nlev = C.c_int32()
+        L.hamlss_amg_num_levels(h, C.byref(nlev))
+        level_rows = []
+        for lv in range(nlev.value):
+            r_, c_, z_ = C.c_int32(), C.c_int32(), C.c_int32()
+            L.hamlss_amg_level_matrix(h, lv, 0, C.byref(r_), C.byref(c_), C.byref(z_),
+                                      None, None, None)
+            level_rows.append((r_.value, z_.value))
+        hierarchy = {"levels": nlev.value, "rows": [r for r, _ in level_rows],
+                     "nnz": [z for _, z in level_rows], "coarsest_rows": level_rows[-1][0]}
 
         def timed_solves(pp, k):
             its = []
@@ -468,15 +528,20 @@ def run_ours(args, rank, world, local):
         "ms_per_step": round(max_ms / args.steps, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if solver == "amg_mixed" else "f64",
         "data": "synthetic (seeded lognormal kappa, uniform rhs)",
-        "config": {"workload": f"var-kappa Poisson {args.n_side}^2 5-point, sigma={SIGMA}, "
-                               f"rtol {TOL}, PCG + {solver}",
+        "config": {"workload": workload_name(args.n_side, solver, hierarchy),
                    "n": n, "nnz": nnz, "solver": solver, "global_batch": world,
+                   "amg": amg_config(solver, hierarchy),
                    "l2": "inputs larger than L2 (no flush)", "parallelism": f"replicas x{world}"},
         "iterations": int(np.median(iters)), "true_residual_max": float(max(true_res)),
         "e2e": {"value": round(e2e_value, 4), "unit": "solves/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
         "roofline": roofline,
-        "gpu_launches": own_launches(solver, args.n_side, args.steps, int(total_launches)),
+        "gpu_launches": (counted[0] * args.steps) if counted else int(total_launches),
+        "gpu_launches_source": ("engine kernels of one step counted by the CUDA activity profiler "
+                                "(CUPTI) after the timed region, times the steps" if counted else
+                                "engine profiler's outermost operations (activity profiler "
+                                "unavailable)"),
+        "library_launches_per_step": counted[1] if counted else None,
         "profiled_operations": int(total_launches),
         "kernel_families": {f[0]: {"launches": f[1], "ms": round(f[2], 3),
                                    "GB/s": round(f[3] / max(f[2], 1e-9) / 1e6, 1)} for f in fams},
@@ -486,75 +551,202 @@ def run_ours(args, rank, world, local):
     return out, (rp, ci, v, b)
 
 
-def cpu_baseline(args, data, device_iters_fp64):
+REF_FIXTURE = os.path.join(ROOT, "tests", "golden", "ref_cg_jacobi_2048.json")
+# the largest grid side on which the reference's AMG can be set up: its smoothed
+# prolongation forms a dense n_fine x n_coarse buffer whose size overflows int at 256^2
+# (amg.cpp:113)
+REF_AMG_MAX_SIDE = 240
+
+
+def ref_full_solve():
+    """The reference's own complete CG+Jacobi solve of the 2048^2 benchmark system
+    (iterations, wall time, threads), recorded by tests/golden/make_ref_iterations.py."""
+    try:
+        with open(REF_FIXTURE) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return None
+
+
+def cpu_baseline(args, data):
+    """The reference's CG+Jacobi (its only path at this size) timed on a bounded sample of
+    iterations of the same system, scaled by the iteration count of the reference's own
+    complete solve (fixture written by the reference itself)."""
     rp, ci, v, b = data
+    full = ref_full_solve()
+    if args.n_side != 2048 or not full:
+        return None
     threads = cpu_threads()
     dt, it = reference_cpu_sample(rp, ci, v, b, args.cpu_sample_iters, threads)
     per_iter = dt / max(it, 1)
-    value = 1.0 / (per_iter * device_iters_fp64)
+    value = 1.0 / (per_iter * full["iterations"])
     return {"value": value, "unit": "solves/s", "cores": threads, "kind": "reference",
-            "sample": f"{it} CG+Jacobi iterations of the reference (release build, "
-                      f"{threads} OpenMP threads) on the same 2048^2 system, {dt:.1f} s; "
-                      f"solve time = per-iteration time x {device_iters_fp64} iterations "
-                      f"(the count FP64 CG+Jacobi needs for 1e-10 on this system)"}
+            "sample": f"{it} CG+Jacobi iterations of the reference (release build, {threads} "
+                      f"OpenMP threads) on the same 2048^2 system, {dt:.1f} s, scaled to the "
+                      f"{full['iterations']} iterations of the reference's own complete solve "
+                      f"of this system to 1e-10 ({full['wall_s']} s on {full['threads']} "
+                      f"threads, tests/golden/ref_cg_jacobi_2048.json); its AMG cannot be set "
+                      f"up at this size (amg.cpp:113)"}
 
 
-def fp64_cg_iterations(data):
-    """Iterations FP64 CG+Jacobi needs on the system (engine run, same algorithm)."""
+def same_algorithm_side(args, local, side=REF_AMG_MAX_SIDE):
+    """Device PCG + SA-AMG against the reference's CGSolver + AMGPreconditioner on the
+    largest grid the reference's AMG can set up: variable-kappa Poisson side^2 (sigma 1,
+    rhs U[-1, 1)), rtol 1e-10, the reference's own AMG defaults (theta 0.25, omega 0.67,
+    coarse limit 50, 10 levels, V(2, 2)), FP64 on both sides.  One complete solve each
+    (matrix in, preconditioner setup, solve, solution out); device: median of 5 through
+    the C ABI with host buffers; reference: all host threads."""
+    import ctypes as C
+
+    import hsps_b200 as H
+    import oracle
+    from hsps_b200 import _abi
+    from hsps_b200._abi import default_params
+
+    rp, ci, v, b = problem(side, 4242)
+    n, nnz = len(rp) - 1, len(v)
+    p = default_params(tol=TOL, max_iter=1000)
+    L = _abi.lib()
+    ctx = H.Context(local)
+
+    def device_once():
+        x = np.zeros(n)
+        t0 = time.perf_counter()
+        mh = C.c_void_p()
+        if L.hamlss_mat_upload(ctx.h, n, n, nnz, rp.ctypes.data, ci.ctypes.data, v.ctypes.data,
+                               H.HOST, C.byref(mh)):
+            raise RuntimeError(L.hamlss_last_error())
+        M = C.c_void_p()
+        if L.hamlss_precond_setup(ctx.h, mh, H.PREC_AMG, C.byref(p), C.byref(M), None):
+            raise RuntimeError(L.hamlss_last_error())
+        st = _abi.Stats()
+        rc = L.hamlss_solve(ctx.h, H.SOLVER_CG, mh, M, b.ctypes.data, x.ctypes.data, H.HOST,
+                            C.byref(p), C.byref(st))
+        dt = time.perf_counter() - t0
+        L.hamlss_precond_release(M)
+        L.hamlss_mat_release(mh)
+        if rc:
+            raise RuntimeError(L.hamlss_last_error())
+        return dt, st
+
+    device_once()
+    runs = [device_once() for _ in range(5)]
+    dev_s = float(np.median([r[0] for r in runs]))
+    dst = runs[-1][1]
+    threads = cpu_threads()
+    R = oracle.Reference(fast=True, threads=threads)
+    t0 = time.perf_counter()
+    rc, xr, sr = R.solve(H.SOLVER_CG, H.PREC_AMG, rp, ci, v, b, params=p)
+    ref_s = time.perf_counter() - t0
+    rr = b - oracle.Oracle().spmv(rp, ci, v, xr)
+    return {"problem": f"var-kappa Poisson {side}^2 (n {n}, nnz {nnz}), sigma 1, rtol 1e-10, "
+                       "PCG + SA-AMG with the reference's AMG defaults, FP64 both sides",
+            "device": {"solve_s": round(dev_s, 5), "solves_per_s": round(1.0 / dev_s, 2),
+                       "iterations": int(dst.iterations), "true_residual": float(dst.true_residual)},
+            "reference": {"solve_s": round(ref_s, 3), "solves_per_s": round(1.0 / ref_s, 4),
+                          "setup_s": round(sr.setup_time_s, 3), "iterations": int(sr.iterations),
+                          "true_residual": float(np.linalg.norm(rr) / np.linalg.norm(b)),
+                          "threads": threads},
+            "speedup": round(ref_s / dev_s, 1)}
+
+
+def coarse512_side(args, local, solver):
+    """The same 2048^2 solve with the hierarchy taken down to a dense coarsest level of at
+    most 512 rows (no stall cut), as the configuration states it: one complete solve
+    (setup + solve), its levels, coarsest size and iterations."""
     import ctypes as C
 
     import torch
 
     import hsps_b200 as H
+    from hsps_b200 import _abi
 
-    rp, ci, v, b = data
+    params, stype, ptype = make_params(solver)
+    if ptype != H.PREC_AMG:
+        return None
+    params.amg_stall_ratio = 0.0
+    rp, ci, v, b = problem(args.n_side, replica_seed(0))
     n = len(rp) - 1
-    A = H.SparseMatrix(n, n, rp, ci, v)
-    s, _ = H.SolverFactory.make("CG", "JACOBI", A, H.SolverParams(tol=TOL, max_iter=100000))
+    ctx = H.Context(local)
+    A = H.SparseMatrix(n, n, rp, ci, v, ctx)
+    L = _abi.lib()
     db = torch.from_numpy(b).cuda()
     dx = torch.zeros(n, dtype=torch.float64, device="cuda")
-    st = H.SolverStats()
-    s.solve(A, db, dx, st)
-    return st.iterations
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    h = C.c_void_p()
+    if L.hamlss_precond_setup(ctx.h, A.h, ptype, C.byref(params), C.byref(h), None):
+        raise RuntimeError(L.hamlss_last_error())
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    st = _abi.Stats()
+    rc = L.hamlss_solve(ctx.h, stype, A.h, h, C.c_void_p(db.data_ptr()), C.c_void_p(dx.data_ptr()),
+                        H.DEVICE, C.byref(params), C.byref(st))
+    torch.cuda.synchronize()
+    t2 = time.perf_counter()
+    nlev = C.c_int32()
+    L.hamlss_amg_num_levels(h, C.byref(nlev))
+    r_, c_, z_ = C.c_int32(), C.c_int32(), C.c_int32()
+    L.hamlss_amg_level_matrix(h, nlev.value - 1, 0, C.byref(r_), C.byref(c_), C.byref(z_),
+                              None, None, None)
+    L.hamlss_precond_release(h)
+    if rc:
+        raise RuntimeError(L.hamlss_last_error())
+    return {"hierarchy": "coarsest level <= 512 rows dense, no stall cut", "levels": nlev.value,
+            "coarsest_rows": r_.value, "setup_s": round(t1 - t0, 3), "solve_s": round(t2 - t1, 3),
+            "iterations": int(st.iterations), "true_residual": float(st.true_residual),
+            "solves_per_s": round(1.0 / (t2 - t0), 4)}
 
 
 def run_reference(args, rank, world):
+    """The reference's own CPU solver on the host cores, for this workload.  At 2048^2 its
+    AMG cannot be set up (amg.cpp:113) and its only path, CG+Jacobi, takes minutes per
+    complete solve, so K complete solves do not fit the arm: the arm reports that and
+    exits.  At sides the reference's AMG can set up (<= 240), each step is one complete
+    reference solve with CGSolver + AMGPreconditioner (same algorithm, the reference's
+    defaults)."""
     if rank != 0:
         return None
     import oracle
 
     if not oracle.reference_available(fast=True):
         return {"impl": "reference", "unavailable": "reference not built from source (oracle/_ref)"}
-    data = problem(args.n_side, 1000)
-    rp, ci, v, b = data
+    if args.n_side > REF_AMG_MAX_SIDE:
+        full = ref_full_solve()
+        cost = (f"{full['wall_s']:.0f} s per complete solve ({full['iterations']} iterations on "
+                f"{full['threads']} threads)") if full else "minutes per complete solve"
+        return {"impl": "reference",
+                "unavailable": f"the reference cannot set up its AMG above {REF_AMG_MAX_SIDE}^2 "
+                               f"(dense n_fine x n_coarse buffer, amg.cpp:113); its only path at "
+                               f"{args.n_side}^2, CGSolver + JacobiPreconditioner, takes {cost}, so "
+                               f"{args.warmup + args.steps} complete solves do not fit the arm's "
+                               f"time limit"}
+    from hsps_b200._abi import default_params
+
+    rp, ci, v, b = problem(args.n_side, 1000)
     threads = cpu_threads()
-    # iteration count of the full solve: CG+Jacobi to 1e-10 (the reference's own full-size
-    # path for this problem); sampled below at `cpu-sample-iters` iterations per step
-    n_full = int(os.environ.get("HAMLSS_REF_FULL_ITERS", "0")) or None
-    if n_full is None:
-        try:
-            n_full = fp64_cg_iterations(data)
-        except Exception:
-            n_full = 8210
+    R = oracle.Reference(fast=True, threads=threads)
+    p = default_params(tol=TOL, max_iter=1000)
     for _ in range(max(0, min(args.warmup, 1))):
-        reference_cpu_sample(rp, ci, v, b, 5, threads)
-    times = []
+        R.solve(0, 3, rp, ci, v, b, params=p)
+    t0 = time.perf_counter()
+    its = []
     for _ in range(args.steps):
-        dt, it = reference_cpu_sample(rp, ci, v, b, args.cpu_sample_iters, threads)
-        times.append(dt / max(it, 1))
-    per_iter = float(np.median(times))
-    value = 1.0 / (per_iter * n_full)
-    return {"impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s",
-            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": per_iter * n_full * 1e3, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+        rc, x, st = R.solve(0, 3, rp, ci, v, b, params=p)
+        its.append(st.iterations)
+    dt = time.perf_counter() - t0
+    value = args.steps / dt
+    return {"impl": "reference", "metric": METRIC.replace("2048^2", f"{args.n_side}^2"),
+            "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded)",
             "config": {"workload": f"var-kappa Poisson {args.n_side}^2 5-point, sigma={SIGMA}, "
-                                   f"rtol {TOL}, reference CGSolver + JacobiPreconditioner",
-                       "n": len(rp) - 1, "nnz": len(v)},
+                                   f"rtol {TOL}, reference CGSolver + AMGPreconditioner",
+                       "n": len(rp) - 1, "nnz": len(v), "iterations": int(np.median(its))},
             "cpu_baseline": {"value": value, "unit": "solves/s", "cores": threads,
                              "kind": "reference",
-                             "sample": f"{args.cpu_sample_iters} CG iterations per step, "
-                                       f"scaled to the {n_full} iterations of the full solve"},
+                             "sample": f"{args.steps} complete solves (setup + solve)"},
             "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
 
@@ -909,10 +1101,17 @@ def main():
     if out is None:
         return
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        iters_fp64 = out["iterations"] if out["config"]["solver"] == "cg_jacobi" else fp64_cg_iterations(data)
-        log(f"FP64 CG+Jacobi needs {iters_fp64} iterations; timing the reference sample")
-        out["cpu_baseline"] = cpu_baseline(args, data, iters_fp64)
+        log("timing the reference sample")
+        cb = cpu_baseline(args, data)
+        if cb:
+            out["cpu_baseline"] = cb
         log("cpu baseline done")
+    if rank == 0 and world == 1 and not args.no_same_algorithm:
+        log(f"same-algorithm side measurement at {REF_AMG_MAX_SIDE}^2 (device vs reference AMG-PCG)")
+        out["reference_same_algorithm"] = same_algorithm_side(args, local)
+    if rank == 0 and world == 1 and not args.no_coarse512:
+        log("coarsest <= 512 hierarchy side measurement")
+        out["hierarchy_coarse512"] = coarse512_side(args, local, out["config"]["solver"])
     if rank == 0 and world == 1 and args.serving_requests > 0:
         out["serving"] = run_serving(args, local)
     if rank == 0 and world == 1 and not args.no_configs:

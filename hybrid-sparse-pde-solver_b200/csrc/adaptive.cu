@@ -282,6 +282,7 @@ int extract_features(Ctx& ctx, hamlss_mat* A, double feat[24], int* initial_stat
     const int stride = std::max(1, n / sample_rows);
     const double mean = (double)nnz / n;
     int blocks = std::max(1, std::min(ceil_div(n, 256), ctx.sm_count * 8));
+    L.red_check(blocks, 3);
     k_features<<<blocks, 256, 0, st>>>(n, A->A.rp.p, A->A.ci.p, A->A.v.p, mean, stride,
                                        reinterpret_cast<Extrema*>(exbuf.p), L.red(), sums.p);
     HAMLSS_LAUNCH_CHECK();

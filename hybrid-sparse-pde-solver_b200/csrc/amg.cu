@@ -1043,6 +1043,11 @@ struct EpiSmooth {
     const T* dinv;
     T omega;
     HAMLSS_NO_LOAD
+    __device__ __forceinline__ void prefetch(int r0, int r1) const {
+        l2_prefetch_rows(b, r0, r1);
+        l2_prefetch_rows(x, r0, r1);
+        l2_prefetch_rows(dinv, r0, r1);
+    }
     template <int NV>
     __device__ __forceinline__ void operator()(int i, double ax, double (&)[NV]) const {
         if constexpr (sizeof(T) == 8) {
@@ -1059,6 +1064,7 @@ template <typename T>
 struct EpiSmoothDot {
     EpiSmooth<T> s;
     HAMLSS_NO_LOAD
+    __device__ __forceinline__ void prefetch(int r0, int r1) const { s.prefetch(r0, r1); }
     template <int NV>
     __device__ __forceinline__ void operator()(int i, double ax, double (&acc)[NV]) const {
         s(i, ax, acc);
@@ -1072,6 +1078,7 @@ struct EpiResid {
     const T* b;
     T* r;
     HAMLSS_NO_LOAD
+    __device__ __forceinline__ void prefetch(int r0, int r1) const { l2_prefetch_rows(b, r0, r1); }
     template <int NV>
     __device__ __forceinline__ void operator()(int i, double ax, double (&)[NV]) const {
         if constexpr (sizeof(T) == 8) r[i] = __dsub_rn((double)b[i], ax);
@@ -1117,6 +1124,7 @@ struct EpiProlongTo {
     const T* xin;
     T* xout;
     HAMLSS_NO_LOAD
+    __device__ __forceinline__ void prefetch(int r0, int r1) const { l2_prefetch_rows(xin, r0, r1); }
     template <int NV>
     __device__ __forceinline__ void operator()(int i, double ax, double (&)[NV]) const {
         if constexpr (sizeof(T) == 8) xout[i] = __dadd_rn((double)xin[i], ax);

@@ -100,6 +100,7 @@ void hamlss_params_default(hamlss_params* p) {
     p->jacobi_omega = 1.0;
     p->ladder_mode = 0;
     p->check_every = 8;
+    p->ir_update = 1e-2;
 }
 
 // ------------------------------------------------------------------------ context
@@ -192,6 +193,17 @@ int hamlss_profile_read(hamlss_ctx* ctx, int32_t cap, char* names, int32_t* laun
             if (total_bytes) total_bytes[c] = by[k];
         }
         *count = c;
+        return HAMLSS_OK;
+    });
+}
+
+int hamlss_energy_read(int device, double* joules) {
+    return guarded([&]() -> int {
+        if (!joules) return set_err(HAMLSS_ERR_INVALID, "null argument");
+        *joules = 0.0;
+        if (!nvml_energy_available(device))
+            return set_err(HAMLSS_ERR_NOT_READY, "NVML energy counter not available for this device");
+        *joules = nvml_energy_j(device);
         return HAMLSS_OK;
     });
 }
@@ -358,6 +370,8 @@ int hamlss_spmv(hamlss_ctx* ctx, const hamlss_mat* A, const double* x, double* y
                                            EpiStore<double>{dy});
         if (where == HAMLSS_HOST) ws.d[7].download(y, A->A.n, s);
         HAMLSS_CUDA(cudaStreamSynchronize(s));
+        if (lane_take_timeout(c.lane))
+            return set_err(HAMLSS_ERR_TIMEOUT, "an SpMV gave up waiting for its bulk copies");
         return HAMLSS_OK;
     });
 }
@@ -636,6 +650,8 @@ int hamlss_solve(hamlss_ctx* ctx, int solver, const hamlss_mat* A, const hamlss_
         HAMLSS_CUDA(cudaStreamSynchronize(s));
         if (r.status != HAMLSS_OK)
             return set_err(r.status, "non-finite values met during the solve");
+        if (lane_take_timeout(c.lane))
+            return set_err(HAMLSS_ERR_TIMEOUT, "an SpMV gave up waiting for its bulk copies");
         return HAMLSS_OK;
     });
 }

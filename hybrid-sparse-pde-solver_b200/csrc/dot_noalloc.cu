@@ -49,7 +49,8 @@ DeviceScratch g_dev[kMaxDevices];
 
 int fail(int code, const std::string& m) { return hamlss::set_last_error(code, m); }
 
-// Look up the scratch of the current device (once per device).
+// Look up the scratch of the current device (once per device; the address is kept for
+// the life of the process, so it goes stale if the process resets the device).
 int scratch_of_current_device(DeviceScratch** out) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);

@@ -20,11 +20,23 @@ void pool_keep_memory(int device) {
 }
 
 void lane_init(Lane& L, int sm_count) {
-    (void)sm_count;
     HAMLSS_CUDA(cudaStreamCreateWithFlags(&L.stream, cudaStreamNonBlocking));
-    L.partials.alloc(kPartialCap);
+    // every reducing launch has at most sm_count * kMaxBlocksPerSm blocks of at most
+    // kMaxRed sums each (red_check enforces it before the launch)
+    L.red_cap = (size_t)std::max(sm_count, 1) * kMaxBlocksPerSm * kMaxRed;
+    L.partials.alloc(L.red_cap);
+    L.err.alloc(1);
+    L.err.zero(L.stream);
     L.ticket.alloc(1);
     L.ticket.zero(L.stream);
+}
+
+bool lane_take_timeout(const Lane& L) {
+    int e = 0;
+    HAMLSS_CUDA(cudaMemcpyAsync(&e, L.err.p, sizeof(int), cudaMemcpyDeviceToHost, L.stream));
+    HAMLSS_CUDA(cudaStreamSynchronize(L.stream));
+    if (e) HAMLSS_CUDA(cudaMemsetAsync(L.err.p, 0, sizeof(int), L.stream));
+    return e != 0;
 }
 
 void lane_destroy(Lane& L) {
@@ -35,6 +47,7 @@ void lane_destroy(Lane& L) {
     }
     L.partials.release();
     L.ticket.release();
+    L.err.release();
 }
 
 namespace {

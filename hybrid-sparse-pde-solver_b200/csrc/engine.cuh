@@ -6,6 +6,7 @@
 
 #include "common.cuh"
 #include "spmv.cuh"
+#include "spmv_stream.cuh"
 
 namespace hamlss {
 
@@ -38,7 +39,23 @@ struct Profiler {
         marks.push_back(Mark{name, bytes, (size_t)slot});
         next = slot + 2;
     }
+    // Position of the next mark: a solver notes it around each iteration it issues, so it
+    // can find that iteration's launches once it knows where the device stopped.
+    size_t pos() const { return marks.size(); }
+    // Marks [from, to) are launches that their gate turned into no-ops (issued ahead of
+    // the device's stop test): they moved no bytes, and are reported as "gated".
+    void gated(size_t from, size_t to) {
+        for (size_t k = from; k < to && k < marks.size(); ++k) {
+            marks[k].name = "gated";
+            marks[k].bytes = 0.0;
+        }
+    }
 };
+
+inline size_t prof_pos(const Profiler* p) { return p ? p->pos() : 0; }
+inline void prof_gated(Profiler* p, size_t from, size_t to) {
+    if (p && from < to) p->gated(from, to);
+}
 
 // A stream plus the scratch its reductions use.  Kernels on one lane run in order, so
 // one reducer (partials + ticket) per lane is enough.
@@ -46,8 +63,15 @@ struct Lane {
     cudaStream_t stream = nullptr;
     DBuf<double> partials;
     DBuf<unsigned> ticket;
+    size_t red_cap = 0;       // entries of `partials`
+    DBuf<int> err;            // set by a bulk-copy SpMV whose wait ran out (zero otherwise)
     Profiler* prof = nullptr;
     Reducer red() const { return Reducer{partials.p, ticket.p}; }
+    // a grid of `blocks` blocks, each storing `nred` partial sums, must fit `partials`
+    void red_check(int blocks, int nred) const {
+        if ((size_t)blocks * (size_t)(nred > 0 ? nred : 1) > red_cap)
+            fail(HAMLSS_ERR_INVALID, "reduction grid exceeds the lane's partial-sum buffer");
+    }
 };
 
 // Only the outermost scope on a lane is recorded: a setup phase that launches many
@@ -91,10 +115,12 @@ int occupancy_blocks(K kernel, int threads, size_t dyn_smem = 0) {
 
 constexpr int kMaxBlocksPerSm = 8;
 constexpr int kMaxRed = 72;   // widest reduction (multi-dot of an FGMRES basis + 2)
-constexpr int kPartialCap = 148 * kMaxBlocksPerSm * kMaxRed;
 
 void lane_init(Lane& L, int sm_count);
 void lane_destroy(Lane& L);
+// Whether a bulk-copy SpMV on the lane gave up waiting for its copies since the last call
+// (it then read the matrix from global memory, so its results stand); clears the word.
+bool lane_take_timeout(const Lane& L);
 
 // Device view of a CSR matrix.
 template <typename T>
@@ -137,11 +163,65 @@ int spmv_group_size(const Csr<T>& A) {
     return 8;
 }
 
+// Lanes per row of the bulk-copy kernel (spmv_stream.cuh), or 0 for the plain kernel.  A
+// tile of 256 / G rows should fit one stage (1536 entries), so G grows with the average
+// row length; FP64 keeps G = 1 (each row summed in column order, bit-exact) and so takes
+// only the short-row operators.  Small operators (< 32768 rows) stay on the plain kernel.
+template <typename T>
+int stream_group(const Csr<T>& A) {
+    if (A.n < 32768) return 0;
+    const double avg = (double)A.nnz / A.n;
+    if (avg <= 5.5) return 1;
+    if (sizeof(T) == 8) return 0;
+    if (avg <= 11.0) return 2;
+    if (avg <= 22.0) return 4;
+    if (avg <= 44.0) return 8;
+    return 0;
+}
+
+// Max co-resident CTAs of a bulk-copy SpMV instantiation (its dynamic shared memory
+// raised above the 48 KB default once).
+template <typename K>
+int stream_per_sm(K kernel, size_t smem) {
+    HAMLSS_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    return std::min(occupancy_blocks(kernel, kStreamThreads, smem), kMaxBlocksPerSm);
+}
+
+template <typename T, int NRED, typename XOp, typename Epi, typename Fin, int G>
+void launch_spmv_stream(int sm_count, const Lane& L, const Csr<T>& A, const XOp& xop, const Epi& epi,
+                        const Fin& fin, const int* gate) {
+    auto kern = k_spmv_stream<T, NRED, XOp, Epi, Fin, G>;
+    constexpr size_t smem = StreamShape<T>::smem_bytes;
+    static const int per_sm = stream_per_sm(kern, smem);
+    const int tiles = ceil_div(A.n, kStreamThreads / G);
+    const int blocks = std::max(1, std::min(tiles, sm_count * per_sm));
+    if (NRED > 0) L.red_check(blocks, NRED);
+    kern<<<blocks, kStreamThreads, smem, L.stream>>>(A.n, A.rp, A.ci, A.v, xop, epi, L.red(), fin, gate,
+                                                     L.err.p);
+    HAMLSS_LAUNCH_CHECK();
+}
+
 template <typename T, int NRED, typename XOp, typename Epi, typename Fin = NoFin>
 void launch_spmv(int sm_count, const Lane& L, const Csr<T>& A, const XOp& xop, const Epi& epi,
                  const Fin& fin = Fin{}, const int* gate = nullptr, const char* name = "spmv",
                  double vec_bytes = -1.0) {
     ProfScope ps(L, name, csr_bytes(A) + (vec_bytes >= 0 ? vec_bytes : 2.0 * sizeof(T) * A.n));
+    switch (stream_group(A)) {
+        case 1: return launch_spmv_stream<T, NRED, XOp, Epi, Fin, 1>(sm_count, L, A, xop, epi, fin, gate);
+        case 2:
+            if constexpr (sizeof(T) == 4)
+                return launch_spmv_stream<T, NRED, XOp, Epi, Fin, 2>(sm_count, L, A, xop, epi, fin, gate);
+            break;
+        case 4:
+            if constexpr (sizeof(T) == 4)
+                return launch_spmv_stream<T, NRED, XOp, Epi, Fin, 4>(sm_count, L, A, xop, epi, fin, gate);
+            break;
+        case 8:
+            if constexpr (sizeof(T) == 4)
+                return launch_spmv_stream<T, NRED, XOp, Epi, Fin, 8>(sm_count, L, A, xop, epi, fin, gate);
+            break;
+        default: break;
+    }
     auto kern = k_spmv<T, NRED, XOp, Epi, Fin>;
     // thread-safe one-time initialisation (contexts may be driven from several threads)
     static const int per_sm = std::min(occupancy_blocks(kern, kSpmvThreads), kMaxBlocksPerSm);
@@ -149,6 +229,7 @@ void launch_spmv(int sm_count, const Lane& L, const Csr<T>& A, const XOp& xop, c
     const int rows_per_warp = gsz > 1 ? 32 / gsz : 32;
     const int nwork = ceil_div(A.n, rows_per_warp);
     int blocks = std::max(1, std::min(ceil_div(nwork, kSpmvWarps), sm_count * per_sm));
+    if (NRED > 0) L.red_check(blocks, NRED);
     kern<<<blocks, kSpmvThreads, 0, L.stream>>>(A.n, A.rp, A.ci, A.v, xop, epi, L.red(), fin, gate, gsz);
     HAMLSS_LAUNCH_CHECK();
 }
@@ -158,6 +239,7 @@ void launch_vec(int sm_count, const Lane& L, int n, const Body& body, const Fin&
                 const int* gate = nullptr, const char* name = "vec", double bytes = 0.0) {
     ProfScope ps(L, name, bytes);
     int blocks = std::max(1, std::min(ceil_div(n, 256), sm_count * kMaxBlocksPerSm));
+    if (NRED > 0) L.red_check(blocks, NRED);
     k_vec<NRED, Body, Fin><<<blocks, 256, 0, L.stream>>>(n, body, L.red(), fin, gate);
     HAMLSS_LAUNCH_CHECK();
 }

@@ -11,11 +11,13 @@
 //                                         tests |g_{j+1}| < tol ||b|| (fgmres_solver.cpp:126-148)
 //   v_{j+1} = w / ||w||
 // The cycle ends with the triangular solve for y (:57-66) and x += Z y, both on the
-// device; the host polls once per restart cycle.  Classical Gram-Schmidt applied twice
+// device; the host polls between groups of inner steps (sized by the decay of the
+// residual estimate) and at the end of each cycle.  Classical Gram-Schmidt applied twice
 // replaces the reference's modified Gram-Schmidt (:122-125): same subspace, three passes
 // over V instead of 2(j+1) dependent dot/axpy pairs.
 #include <cmath>
 #include <cstring>
+#include <vector>
 
 #include "krylov.cuh"
 
@@ -242,6 +244,7 @@ void launch_mdot_t(Ctx& ctx, int mode, int n, int nv, const double* V, long long
                    const double* hprev, GmState* s, const GmArrays& a, int j, const int* gate) {
     const Lane& L = ctx.lane;
     int blocks = std::max(1, std::min(ceil_div(n, 256), ctx.sm_count * 4));
+    L.red_check(blocks, mode == 2 ? 1 : NV);
     ProfScope ps(L, "gmres_mdot", 8.0 * n * (nv + (mode == 0 ? 1 : 2)));
     if (mode == 0)
         k_mdot<NV, 0, FinH1<NV>><<<blocks, 256, 0, L.stream>>>(n, nv, V, ld, w, hprev, L.red(),
@@ -321,36 +324,83 @@ SolveResult fgmres_solve(Ctx& ctx, hamlss_mat* A, Prec* M, const double* b, doub
         return res;
     }
     int total = 0, cycles = 0;
+    int sub = std::max(1, std::min(m, 8));       // inner steps issued before the first poll
+    // Launch positions of each inner step in the engine profiler: its start, its last
+    // launch (v_{j+1} = w / ||w||) and its end.
+    struct StepMarks { size_t start, next_v, end; };
+    std::vector<StepMarks> steps;
     while (total < max_iter) {
         const int cm = std::min(m, max_iter - total);
         HAMLSS_CUDA(cudaMemsetAsync(&s->halt, 0, sizeof(int), st));
         HAMLSS_CUDA(cudaMemcpyAsync(&s->iter_base, &total, sizeof(int), cudaMemcpyHostToDevice, st));
         launch_spmv<double, 1>(sm, L, A->A.f64(), XVec<double>{x}, EpiRes{b, r}, FinCycleStart{s, a},
                                nullptr, "gmres_residual", 24.0 * n);
+        const size_t v0_mark = prof_pos(L.prof);
         launch_vec<0>(sm, L, n, BodyScaleV0{r, V, s, 0.0}, NoFin{}, &s->halt, "vec", 16.0 * n);
-        for (int j = 0; j < cm; ++j) {
-            double* vj = V + ld * j;
-            double* zj = Z + ld * j;
-            if (flex) M->apply(ctx, L, vj, zj, &s->halt);
-            launch_spmv<double, 0>(sm, L, A->A.f64(), XVec<double>{zj}, EpiStore<double>{w}, NoFin{},
-                                   &s->halt, "spmv");
-            launch_mdot(ctx, 0, n, j + 1, V, ld, w, nullptr, s, a, j, &s->halt);
-            launch_mdot(ctx, 1, n, j + 1, V, ld, w, a.h1, s, a, j, &s->halt);
-            launch_mdot(ctx, 2, n, j + 1, V, ld, w, a.h2, s, a, j, &s->halt);
-            launch_vec<0>(sm, L, n, BodyNextV{w, V + ld * (j + 1), s, 0.0}, NoFin{}, &s->halt, "vec",
-                          16.0 * n);
+        steps.clear();
+        // Inner steps go out in groups; the host polls between groups and stops issuing
+        // once the device's test has ended the cycle.  The group size follows the decay of
+        // |g_{j+1}| (monotone in GMRES) since the previous poll.
+        int j = 0, poll_j = 0;
+        double poll_res = -1.0;
+        bool halted = false;
+        while (j < cm && !halted) {
+            const int jend = std::min(cm, j + sub);
+            for (; j < jend; ++j) {
+                StepMarks sm_;
+                sm_.start = prof_pos(L.prof);
+                double* vj = V + ld * j;
+                double* zj = Z + ld * j;
+                if (flex) M->apply(ctx, L, vj, zj, &s->halt);
+                launch_spmv<double, 0>(sm, L, A->A.f64(), XVec<double>{zj}, EpiStore<double>{w}, NoFin{},
+                                       &s->halt, "spmv");
+                launch_mdot(ctx, 0, n, j + 1, V, ld, w, nullptr, s, a, j, &s->halt);
+                launch_mdot(ctx, 1, n, j + 1, V, ld, w, a.h1, s, a, j, &s->halt);
+                launch_mdot(ctx, 2, n, j + 1, V, ld, w, a.h2, s, a, j, &s->halt);
+                sm_.next_v = prof_pos(L.prof);
+                launch_vec<0>(sm, L, n, BodyNextV{w, V + ld * (j + 1), s, 0.0}, NoFin{}, &s->halt, "vec",
+                              16.0 * n);
+                sm_.end = prof_pos(L.prof);
+                steps.push_back(sm_);
+            }
+            if (j >= cm) break;                    // the cycle's own poll follows
+            poll(h);
+            halted = h.halt != 0;
+            if (!halted && h.bnorm > 0.0) {
+                const double res = h.res;
+                int grow = std::min(2 * sub, m);
+                if (poll_res > res && res > 0.0 && h.jcount > poll_j) {
+                    const double rate = std::log(res / poll_res) / (h.jcount - poll_j);
+                    const double need = std::ceil(std::log(h.tol_abs / res) / rate);
+                    if (need >= 0.0 && need < grow) grow = std::max(1, (int)need);
+                }
+                sub = grow;
+                poll_j = h.jcount;
+                poll_res = res;
+            }
         }
         {
             ProfScope ps(L, "gmres_small", 0.0);
             k_backsolve<<<1, 32, 0, st>>>(s, a);
             HAMLSS_LAUNCH_CHECK();
         }
+        const size_t upd_mark = prof_pos(L.prof);
         {
             ProfScope ps(L, "gmres_update", 8.0 * n * (2 + cm));
             k_update_x<<<std::max(1, std::min(ceil_div(n, 256), sm * 8)), 256, 0, st>>>(n, x, Z, ld, s, a.y);
             HAMLSS_LAUNCH_CHECK();
         }
         poll(h);
+        if (L.prof && h.halt) {
+            // launches the gate skipped: after a stop at cycle start, every inner step;
+            // after a stop in step jcount - 1, that step's v_{j+1} and the later steps
+            const size_t end = steps.empty() ? v0_mark + 1 : steps.back().end;
+            const size_t from = h.jcount == 0 ? v0_mark
+                              : (size_t)h.jcount <= steps.size() ? steps[h.jcount - 1].next_v : end;
+            prof_gated(L.prof, from, end);
+        }
+        if (L.prof && upd_mark < L.prof->pos())       // x += Z y over the steps taken
+            L.prof->marks[upd_mark].bytes = h.jcount ? 8.0 * n * (2 + h.jcount) : 0.0;
         if (h.status == ST_NONFINITE) { res.status = HAMLSS_ERR_NONFINITE; break; }
         total += h.jcount;
         ++cycles;

@@ -49,6 +49,14 @@ SolveResult sstep_solve(Ctx& ctx, hamlss_mat* A, const double* b, double* x,
 // uniform vector, Gershgorin bounds of the tridiagonal.
 void spectral_interval(Ctx& ctx, hamlss_mat* A, int steps, double* lo, double* hi);
 
+// Mixed-precision PCG with reliable updates: FP32 iteration (values, vectors, M^-1),
+// FP64 dot products and scalars, the residual replaced by the true FP64 one whenever the
+// recursive one fell by `delta` since the last replacement and to confirm the stop test.
+// x (FP64, device) is the initial guess and the result; *n_updates counts the updates.
+SolveResult cg_reliable_solve(Ctx& ctx, hamlss_mat* A, Prec* M, const double* b, double* x, double tol,
+                              int max_iter, int check_every, double delta, Workspace& ws,
+                              const LadderCfg* lad, int* n_updates);
+
 // Mixed precision: FP64 iterative refinement around an FP32 inner PCG / FGMRES.
 SolveResult mixed_solve(Ctx& ctx, int solver, hamlss_mat* A, Prec* M, const double* b,
                         double* x, const hamlss_params& p, Workspace& ws, int* outer_iters,

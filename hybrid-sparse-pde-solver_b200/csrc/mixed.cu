@@ -1,4 +1,8 @@
-// mixed.cu -- FP32 inner solves inside an FP64 iterative-refinement loop.
+// mixed.cu -- mixed-precision solves.
+//
+// PCG: by default the reliable-update PCG of cg.cu (FP32 iteration, residual refreshed in
+// FP64; ir_update > 0).  With ir_update = 0, and for FGMRES, FP32 inner solves inside an
+// FP64 iterative-refinement loop:
 //
 //   repeat:  r = b - A x            FP64 values, FP64 vectors (true residual)
 //            stop when ||r|| / ||b|| < tol
@@ -24,6 +28,7 @@ struct EpiRes64 {
     const double* b;
     double* r;
     HAMLSS_NO_LOAD
+    __device__ __forceinline__ void prefetch(int r0, int r1) const { l2_prefetch_rows(b, r0, r1); }
     template <int NV>
     __device__ __forceinline__ void operator()(int i, double ax, double (&acc)[NV]) const {
         double bi = b[i];
@@ -100,6 +105,14 @@ SolveResult mixed_solve(Ctx& ctx, int solver, hamlss_mat* A, Prec* M, const doub
         ad.kind = M ? M->kind : HAMLSS_PREC_NONE;
         *outer_iters = 1;
         return fgmres_solve(ctx, A, M ? &ad : nullptr, b, x, p.tol, p.max_iter, p.restart_size, ws, lad);
+    }
+    if (p.ir_update > 0.0) {
+        // reliable updates: one FP32 PCG whose residual is refreshed in FP64 (cg.cu)
+        int updates = 0;
+        SolveResult r = cg_reliable_solve(ctx, A, M, b, x, p.tol, p.max_iter, p.check_every,
+                                          std::min(p.ir_update, 0.5), ws, lad, &updates);
+        *outer_iters = updates;
+        return r;
     }
     // buffers: FP64 residual in d[5]; FP32 rhs / correction in f[5], f[6]; scalars in small
     ws.d[5].ensure(n);

@@ -122,7 +122,7 @@ bool spd_like(int n, const int32_t* rp, const int32_t* ci, const double* v) {
 
 bool same_batch_key(const hamlss_params& a, const hamlss_params& b) {
     return a.tol == b.tol && a.max_iter == b.max_iter && a.ir_max_outer == b.ir_max_outer &&
-           a.ir_inner_tol == b.ir_inner_tol &&
+           a.ir_inner_tol == b.ir_inner_tol && a.ir_update == b.ir_update &&
            std::min(a.restart_size, kBatchMaxRestart) == std::min(b.restart_size, kBatchMaxRestart);
 }
 

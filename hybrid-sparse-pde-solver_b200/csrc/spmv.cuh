@@ -57,6 +57,24 @@ __device__ __forceinline__ double lane_row_sum(int row, const int* __restrict__ 
     return sum;
 }
 
+// L2 prefetch of [p, p + bytes) by one thread (cp.async.bulk.prefetch.L2), trimmed to
+// the whole 16-byte granules inside the range so it never touches memory outside it.
+// Functors of the bulk-copy SpMV (spmv_stream.cuh) call it from prefetch(r0, r1) for the
+// vector slices a row tile will read.
+__device__ __forceinline__ void l2_prefetch(const void* p, size_t bytes) {
+    uintptr_t a = reinterpret_cast<uintptr_t>(p);
+    uintptr_t lo = (a + 15) & ~(uintptr_t)15, hi = (a + bytes) & ~(uintptr_t)15;
+    while (hi > lo) {
+        const uintptr_t chunk = (hi - lo) > (1u << 20) ? (1u << 20) : (hi - lo);
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(lo), "r"((unsigned)chunk) : "memory");
+        lo += chunk;
+    }
+}
+template <typename T>
+__device__ __forceinline__ void l2_prefetch_rows(const T* v, int r0, int r1) {
+    if (v && r1 > r0) l2_prefetch(v + r0, (size_t)(r1 - r0) * sizeof(T));
+}
+
 struct NoFin {
     template <int NV>
     __device__ void operator()(const double (&)[NV]) const {}

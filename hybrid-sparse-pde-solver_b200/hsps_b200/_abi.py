@@ -70,6 +70,7 @@ class Params(C.Structure):
         ("ladder_mode", C.c_int32),
         ("check_every", C.c_int32),
         ("amg_stall_ratio", C.c_double),
+        ("ir_update", C.c_double),
     ]
 
 
@@ -82,7 +83,7 @@ def default_params(**over) -> Params:
         sstep_cond_tol=1e12, async_enabled=0, async_max_stale=3, fill_per_row=0,
         block_size=1, record_hw_energy=0, precision=FP64, ir_inner_tol=1e-5,
         ir_max_outer=30, amg_omega=0.67, amg_coarse_limit=50, jacobi_omega=1.0,
-        ladder_mode=0, check_every=8, amg_stall_ratio=0.0,
+        ladder_mode=0, check_every=8, amg_stall_ratio=0.0, ir_update=1e-2,
     )
     for k, v in over.items():
         if not hasattr(p, k):
@@ -222,6 +223,7 @@ def _declare(L: C.CDLL) -> None:
         "hamlss_ctx_stream": (C.c_int, [P, pp]),
         "hamlss_profile_enable": (C.c_int, [P, C.c_int, I32]),
         "hamlss_profile_read": (C.c_int, [P, I32, V, V, V, V, pi]),
+        "hamlss_energy_read": (C.c_int, [C.c_int, pd]),
         "hamlss_mat_upload": (C.c_int, [P, I32, I32, I32, V, V, V, C.c_int, pp]),
         "hamlss_mat_update_values": (C.c_int, [P, V, C.c_int]),
         "hamlss_mat_info": (C.c_int, [P, pi, pi, pi]),

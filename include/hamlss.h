@@ -108,6 +108,10 @@ typedef struct hamlss_params {
     double  amg_stall_ratio;  /* 0: coarsen until amg_coarse_limit / amg_levels / no progress */
                               /* (reference); r in (0,1): also stop when n_c > r * n_f, the  */
                               /* coarsening having stalled, and solve that level densely     */
+    double  ir_update;        /* mixed-precision PCG: FP32 iteration whose residual is        */
+                              /* replaced by the true FP64 one when it fell by this factor   */
+                              /* since the last replacement (reliable update), 1e-2; 0: FP64 */
+                              /* refinement restarting an FP32 PCG (ir_inner_tol, _max_outer) */
 } hamlss_params;
 
 /* ----------------------------------------------------------------- statistics
@@ -177,6 +181,12 @@ int hamlss_profile_enable(hamlss_ctx* ctx, int enable, int32_t max_launches);
 int hamlss_profile_read(hamlss_ctx* ctx, int32_t cap, char* names, int32_t* launches,
                         double* total_ms, double* total_bytes, int32_t* count);
 
+/* Energy counter of CUDA device `device` (NVML's total energy since driver load, joules),
+ * matched to the CUDA ordinal by PCI bus id.  Replaces NVMLMonitor::read_energy_j
+ * (src/parallel/nvml_monitor.cpp:85-100).  Read only.  HAMLSS_ERR_NOT_READY when NVML or
+ * the counter is not available for the device. */
+int hamlss_energy_read(int device, double* joules);
+
 /* -------------------------------------------------------------------- matrix
  * Replaces hsps::SparseMatrix(rows, cols, row_ptr, col_idx, values)
  * (sparse_matrix.cpp:22-27): a deep copy into device memory.  The engine keeps the
@@ -212,7 +222,9 @@ int hamlss_scale(hamlss_ctx* ctx, int32_t n, double alpha, double* x);
  * The scratch (2048 partial sums, the result slot and a ticket: 16 KiB) is a fixed array
  * compiled into the library, which every GPU that loads the library holds until exit.
  * The first call on each device looks up that array's device address (make that first
- * call before any stream capture).  All calls on a device share the array: calls whose
+ * call before any stream capture) and keeps it for the life of the process: after
+ * cudaDeviceReset on a device the kept address is stale, so do not call this entry point
+ * on a device that the process has reset.  All calls on a device share the array: calls whose
  * work may overlap on the GPU (other streams, other host threads) race; serialise them.
  * A launch that would need more than 2048 partial sums (a GPU with more than 256 SMs) is
  * refused with HAMLSS_ERR_SIZE. */

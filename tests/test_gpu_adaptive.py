@@ -85,22 +85,25 @@ def test_ladder_matches_reference(ref, name, A):
 
 
 def test_ladder_device_stall_escalates_early():
-    # Pe = 300 conv-diff: CG+Jacobi stalls; ladder_mode 1 escalates before max_iter
-    bx, by = P.convdiff_wind(40, 300.0)
-    A = P.convection_diffusion_2d(40, 1.0, bx, by)
-    n = 1600
+    # Poisson 64^2 starts in EASY (CG + Jacobi).  CG's recursive residual first rises: in
+    # FP64 on the host, rel(15) / rel(0) = 1.37 > 0.95, so with ladder_mode 1 the device's
+    # windowed stall test must end the EASY attempt after about 15 iterations -- far
+    # before its budget (0.4 max_iter) and max_iter
+    A = P.poisson_2d(64)
+    n = 4096
     b = P.rhs(n, 4)
     M = dev(A)
     p = default_params(tol=1e-8, max_iter=400, restart_size=30, drop_tol=0.0, ladder_mode=1)
     sel = H.AdaptiveSelector(p)
     f, s0 = sel.extract_features(M)
+    assert s0 == H.STATE_EASY
     x = np.zeros(n)
     st = H.SolverStats()
     sel.solve(M, b, x, st)
     log = sel.escalation_log()
-    if log:
-        assert all(e.reason in (1, 2, 3) for e in log)
-        assert log[0].at_iteration < p.max_iter
+    assert log, "the device stall test never fired"
+    assert log[0].from_state == H.STATE_EASY and log[0].reason == 1, log[0]
+    assert log[0].at_iteration <= 20 < p.max_iter * 4 // 10
 
 
 def test_ladder_easy_poisson_no_escalation():
@@ -160,6 +163,8 @@ def test_ladder_mode3_keeps_cg_on_a_nonmonotone_residual():
         out[mode] = (ok, st.state_used, [(e.from_state, e.reason) for e in sel.escalation_log()])
     ok3, state3, log3 = out[3]
     assert ok3 and state3 == H.STATE_EASY and log3 == [], out
-    for frm, reason in out[2][2]:
-        if frm == H.STATE_EASY:
-            assert reason == 1, out                     # mode 2 left CG on the stall rule
+    # mode 2 leaves CG on the stall rule: in FP64 on the host CG's residual grows to
+    # 5.5 x its first value by iteration 15 (ratio 5.5 >> 0.95, below the divergence
+    # factor 10), so the windowed test fires there
+    easy = [reason for frm, reason in out[2][2] if frm == H.STATE_EASY]
+    assert easy == [1], out

@@ -111,7 +111,10 @@ def test_write_read_round_trip(tmp_path):
     assert open(g).read().startswith("%%MatrixMarket matrix array real general\n% solution\n4 1\n")
 
 
-DATA = "/root/reference/data"
+# the project checkout: HSPS_REFERENCE, else a `reference` directory beside this repository
+DATA = os.path.join(os.environ.get("HSPS_REFERENCE") or
+                    os.path.join(os.path.dirname(os.path.dirname(os.path.dirname(
+                        os.path.abspath(__file__)))), "reference"), "data")
 
 
 @pytest.mark.skipif(not os.path.isdir(DATA), reason="project data directory not present")
