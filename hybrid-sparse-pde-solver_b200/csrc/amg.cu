@@ -728,7 +728,19 @@ __global__ void k_spgemm_dense(const int* __restrict__ rows, int nrows, int bcol
 // Row i of C = A B for the listed rows, one block per row, with a dense accumulator over the
 // row's column window [lo_i, lo_i + span_i) (the span of the selected rows of B, at most
 // W columns): the arithmetic and output order of k_spgemm_dense, for right operands with
-// more columns than fit in shared memory.  Shared memory: W doubles + W flag bytes.
+// more columns than fit in shared memory.
+// The left entries are added one at a time with a block barrier between them (so every
+// column sums in left-row order), which makes each step's loads the critical path: the
+// block first stages the row's (a_t, row bounds of B) for up to kWinLeft entries in shared
+// memory, and every thread keeps its first product of the next kWinAhead steps in flight
+// in registers, so a step costs a barrier and the adds rather than a chain of dependent
+// global loads.  Shared memory: W doubles + W flag bytes (rounded up to 16) + kWinLeft
+// staged entries of 16 bytes.
+constexpr int kWinLeft = 512;
+constexpr int kWinAhead = 4;
+
+inline size_t window_smem(int W) { return ((9 * (size_t)std::max(W, 1) + 15) & ~(size_t)15) + 16 * (size_t)kWinLeft; }
+
 template <bool FILL>
 __global__ void k_spgemm_window(const int* __restrict__ rows, int nrows, int W,
                                 const int* __restrict__ wlo, const int* __restrict__ wspan,
@@ -738,9 +750,14 @@ __global__ void k_spgemm_window(const int* __restrict__ rows, int nrows, int W,
                                 int* ccnt, const int* __restrict__ crp, int* cci, double* cv) {
     extern __shared__ double acc[];
     unsigned char* hit = reinterpret_cast<unsigned char*>(acc + W);
+    double* sa = reinterpret_cast<double*>(reinterpret_cast<unsigned char*>(acc) +
+                                           ((9 * (size_t)W + 15) & ~(size_t)15));
+    int* sb0 = reinterpret_cast<int*>(sa + kWinLeft);
+    int* sb1 = sb0 + kWinLeft;
     __shared__ int s_warp[kRowBlock / 32];
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    for (int c = threadIdx.x; c < W; c += blockDim.x) {
+    const int tid = threadIdx.x, bdim = blockDim.x;
+    const int lane = tid & 31, wid = tid >> 5, nw = bdim >> 5;
+    for (int c = tid; c < W; c += bdim) {
         acc[c] = 0.0;
         hit[c] = 0;
     }
@@ -749,19 +766,67 @@ __global__ void k_spgemm_window(const int* __restrict__ rows, int nrows, int W,
         const int i = rows[r];
         const int s = arp[i], k = arp[i + 1] - s;
         const int lo = wlo[i], span = wspan[i];
-        for (int t = 0; t < k; ++t) {
+        const int kk = min(k, kWinLeft);
+        for (int t = tid; t < kk; t += bdim) {
             const int j = aci[s + t];
-            const double a = av[s + t];
-            const int e1 = brp[j + 1];
-            for (int e = brp[j] + threadIdx.x; e < e1; e += blockDim.x) {
-                const int c = bci[e] - lo;
-                acc[c] = __dadd_rn(acc[c], __dmul_rn(a, bv[e]));
-                hit[c] = 1;
-            }
-            __syncthreads();
+            sa[t] = av[s + t];
+            sb0[t] = brp[j];
+            sb1[t] = brp[j + 1];
         }
-        const int chunk = (span + blockDim.x - 1) / blockDim.x;
-        const int c0 = min(span, (int)threadIdx.x * chunk), c1 = min(span, c0 + chunk);
+        __syncthreads();
+        // first product of staged step t for this thread: column (window-relative) and value
+        int pc[kWinAhead];
+        double pv[kWinAhead];
+#pragma unroll
+        for (int q = 0; q < kWinAhead; ++q) {
+            pc[q] = -1;
+            pv[q] = 0.0;
+            if (q < kk) {
+                const int e = sb0[q] + tid;
+                if (e < sb1[q]) { pc[q] = bci[e] - lo; pv[q] = bv[e]; }
+            }
+        }
+        for (int t0 = 0; t0 < k; t0 += kWinAhead) {
+#pragma unroll
+            for (int q = 0; q < kWinAhead; ++q) {
+                const int t = t0 + q;
+                if (t < k) {
+                    double a;
+                    int b0, b1, e;
+                    if (t < kk) {
+                        a = sa[t];
+                        b0 = sb0[t];
+                        b1 = sb1[t];
+                        if (pc[q] >= 0) {
+                            acc[pc[q]] = __dadd_rn(acc[pc[q]], __dmul_rn(a, pv[q]));
+                            hit[pc[q]] = 1;
+                        }
+                        e = b0 + tid + bdim;          // the staged first product is done
+                    } else {
+                        const int j = aci[s + t];
+                        a = av[s + t];
+                        b0 = brp[j];
+                        b1 = brp[j + 1];
+                        e = b0 + tid;
+                    }
+                    for (; e < b1; e += bdim) {
+                        const int c = bci[e] - lo;
+                        acc[c] = __dadd_rn(acc[c], __dmul_rn(a, bv[e]));
+                        hit[c] = 1;
+                    }
+                    // refill slot q with step t + kWinAhead
+                    const int tn = t + kWinAhead;
+                    pc[q] = -1;
+                    if (tn < kk) {
+                        const int en = sb0[tn] + tid;
+                        if (en < sb1[tn]) { pc[q] = bci[en] - lo; pv[q] = bv[en]; }
+                    }
+                    __syncthreads();
+                }
+            }
+        }
+        const int chunk = (span + bdim - 1) / bdim;
+        const int c0 = min(span, tid * chunk), c1 = min(span, c0 + chunk);
         int mine = 0;
         for (int c = c0; c < c1; ++c) mine += (hit[c] && fabs(acc[c]) > kEps * kEps) ? 1 : 0;
         int incl = mine;
@@ -777,7 +842,7 @@ __global__ void k_spgemm_window(const int* __restrict__ rows, int nrows, int W,
             total += s_warp[w];
         }
         before += incl - mine;
-        if (ccnt && threadIdx.x == 0) ccnt[i] = total;
+        if (ccnt && tid == 0) ccnt[i] = total;
         if (FILL) {
             int o = crp[i] + before;
             for (int c = c0; c < c1; ++c)
@@ -1432,7 +1497,8 @@ int long_rows(Ctx& ctx, int n, const int* rp, DBuf<int>& list, size_t* smem) {
 // dynamic shared-memory limit is raised once, to the largest any launch of it asks for
 // (kMaxRowSmem), and never lowered: contexts on other threads launch it concurrently.
 constexpr size_t kMaxRowSmem = 20 * (size_t)kSortMax;   // hash table of kSortMax slots
-static_assert(kMaxRowSmem >= 9 * (size_t)kDenseCols && kMaxRowSmem >= 16 * (size_t)kSortMax &&
+static_assert(kMaxRowSmem >= 9 * (size_t)kDenseCols + 16 + 16 * (size_t)kWinLeft &&
+                  kMaxRowSmem >= 16 * (size_t)kSortMax &&
                   kMaxRowSmem >= 12 * (size_t)kWarpHeads * kMergeWarps,
               "row kernels' shared memory");
 
@@ -1545,7 +1611,7 @@ void spgemm(Ctx& ctx, const Csr<double>& A, const Csr<double>& B, DCsr& C) {
     HAMLSS_CUDA(cudaStreamSynchronize(s));
     const int nlong = hm[0], ndense = hm[2], nwarp = hm[3], nwin = hm[5];
     const int* winlist = list.p + 3LL * A.n;
-    const size_t winsmem = 9 * (size_t)std::max(hm[6], 1);   // window accumulator + hit flags
+    const size_t winsmem = window_smem(hm[6]);   // window accumulator + hit flags + left row
     int KH = 32;
     while (KH < hm[4]) KH <<= 1;
     const size_t wsmem = sizeof(int) * 3 * (size_t)KH * kMergeWarps;

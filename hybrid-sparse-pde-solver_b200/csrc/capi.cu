@@ -129,7 +129,6 @@ int hamlss_ctx_destroy(hamlss_ctx* ctx) {
     return guarded([&]() -> int {
         if (!ctx) return HAMLSS_OK;
         cudaSetDevice(ctx->c.device);
-        blas_destroy(ctx->c.blas);
         lane_destroy(ctx->c.lane);
         for (auto e : ctx->c.prof.ev) cudaEventDestroy(e);
         if (ctx->c.ev0) cudaEventDestroy(ctx->c.ev0);

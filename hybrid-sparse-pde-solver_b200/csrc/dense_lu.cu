@@ -6,8 +6,8 @@
 // become dense, and when the hierarchy is cut where coarsening stalls the coarsest level
 // can hold thousands of rows.  Blocked for the GPU (row-major n x n, nb = 64), first
 // without interchanges -- diagonal block factored in shared memory, the inverses of its
-// two triangles formed by one block (64 x 64 each), L21 = A21 U11^-1 and U12 = L11^-1 A12
-// as DGEMMs, A22 by DGEMM, no grid-wide synchronisation -- and, if a pivot falls below
+// two triangles formed by the same kernel (64 x 64 each), L21 = A21 U11^-1 and
+// U12 = L11^-1 A12 as DGEMMs, A22 by DGEMM, no grid-wide synchronisation -- and, if a pivot falls below
 // 1e-10 of the largest entry, again with partial pivoting as the reference does:
 //   panel     columns [k0, k0+nb): one cooperative kernel over all SMs, one column at a
 //             time -- pivot search (largest |a_ij|, first index on ties, like the
@@ -15,13 +15,12 @@
 //             rank-1 update of the panel's remaining columns; two grid barriers a column
 //   swaps     the panel's row interchanges applied to every other column
 //   U12       L11^-1 A12, one thread per column (unit lower triangular solve)
-//   trailing  A22 -= L21 U12, a library DGEMM (cuBLAS)
+//   trailing  A22 -= L21 U12, a DGEMM on the FP64 tensor cores (k_dgemm below)
 // The inverse solves A X = I: X = P I, then L Y = X and U X = Y, blocked the same way
 // (each 64-row block multiplied by its diagonal block's inverse, DGEMM update of the
 // rest): every step is a GEMM, where column-per-thread triangular solves were a long
 // dependent chain per launch.
 #include <cooperative_groups.h>
-#include <cublas_v2.h>
 
 #include <algorithm>
 #include <cstdio>
@@ -162,38 +161,6 @@ k_lu_panel(int n, int k0, int kb, double* M, int* piv, double* cand_v, int* cand
     }
 }
 
-// ------------------------------------------------------------ without pivoting
-// Diagonal block A11 (rows / columns [k0, k0+kb)) factored in shared memory by one block:
-// l = a_rj * (1/a_jj), a_rc -= l * a_jc.  *tiny is set when a pivot's magnitude falls
-// below `floor` (the caller then redoes the whole factorisation with partial pivoting).
-__global__ void k_lu_diag_nopiv(int n, int k0, int kb, double* M, double floor, int* tiny) {
-    __shared__ double a[kNb][kNb + 1];
-    for (int t = threadIdx.x; t < kb * kb; t += blockDim.x) {
-        const int r = t / kb, c = t - r * kb;
-        a[r][c] = M[(size_t)(k0 + r) * n + k0 + c];
-    }
-    __syncthreads();
-    for (int j = 0; j < kb; ++j) {
-        const double d = a[j][j];
-        if (threadIdx.x == 0 && !(fabs(d) > floor)) *tiny = 1;
-        const double inv = (d != 0.0) ? 1.0 / d : 0.0;
-        __syncthreads();
-        for (int t = threadIdx.x; t < (kb - j - 1) * (kb - j); t += blockDim.x) {
-            const int r = j + 1 + t / (kb - j), c = j + t % (kb - j);
-            const double l = __dmul_rn(a[r][j], inv);
-            if (c == j) continue;
-            a[r][c] = __dsub_rn(a[r][c], __dmul_rn(l, a[j][c]));
-        }
-        __syncthreads();
-        for (int r = j + 1 + threadIdx.x; r < kb; r += blockDim.x) a[r][j] = __dmul_rn(a[r][j], inv);
-        __syncthreads();
-    }
-    for (int t = threadIdx.x; t < kb * kb; t += blockDim.x) {
-        const int r = t / kb, c = t - r * kb;
-        M[(size_t)(k0 + r) * n + k0 + c] = a[r][c];
-    }
-}
-
 __global__ void k_abs_max(long long count, const double* __restrict__ a, unsigned long long* out) {
     double m = 0.0;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < count;
@@ -239,40 +206,100 @@ __global__ void k_trsm_lower_unit(int n, int k0, int kb, const double* __restric
     }
 }
 
-// Inverses of the factors of diagonal block b (k0 = b * kNb): Li = L11^-1 (unit lower) and
-// Ui = U11^-1 (upper), kb x kb row-major with ld kNb at inv + 2 * b * kNb * kNb; blockIdx.y
-// 0 forms Li, 1 forms Ui.  Thread c solves column c (substitution in the factor's row
-// order); the block is in shared memory.
+// Inverses of the factors of a kb x kb diagonal block held in shared memory `a` (L unit
+// lower below the diagonal, U on and above it): thread c < kb of the first 64 solves
+// column c of Li = L^-1, thread c of the next 64 column c of Ui = U^-1 (substitution in
+// the factor's row order), both into shared memory (the own column, so no thread waits
+// on another), then written to Li / Ui (row-major, ld kNb).
+__device__ void block_inverses_smem(int kb, const double (*a)[kNb + 1], double (*li)[kNb + 1],
+                                    double (*ui)[kNb + 1], double* Li, double* Ui) {
+    const int t = threadIdx.x;
+    if (t < kNb) {
+        const int c = t;
+        if (c < kb)
+            for (int r = 0; r < kb; ++r) {              // L x = e_c
+                double acc = (r == c) ? 1.0 : 0.0;
+                if (r > c)
+                    for (int q = c; q < r; ++q) acc = __dsub_rn(acc, __dmul_rn(a[r][q], li[q][c]));
+                li[r][c] = r < c ? 0.0 : acc;
+            }
+    } else if (t < 2 * kNb) {
+        const int c = t - kNb;
+        if (c < kb)
+            for (int r = kb - 1; r >= 0; --r) {         // U x = e_c
+                double acc = (r == c) ? 1.0 : 0.0;
+                if (r <= c) {
+                    for (int q = r + 1; q <= c; ++q) acc = __dsub_rn(acc, __dmul_rn(a[r][q], ui[q][c]));
+                    acc = acc / a[r][r];
+                }
+                ui[r][c] = r > c ? 0.0 : acc;
+            }
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < kb * kb; e += blockDim.x) {
+        const int r = e / kb, c = e - r * kb;
+        Li[r * kNb + c] = li[r][c];
+        Ui[r * kNb + c] = ui[r][c];
+    }
+}
+
+constexpr size_t kDiagSmem = 3 * sizeof(double) * kNb * (kNb + 1);
+
+// Inverses of the factors of diagonal block b0 + blockIdx.x (k0 = b * kNb): Li = L11^-1
+// and Ui = U11^-1 at inv + 2 * b * kNb * kNb.  Dynamic shared memory: kDiagSmem.
 __global__ void k_block_inverses(int n, int b0, const double* __restrict__ M, double* inv) {
-    __shared__ double a[kNb][kNb + 1];
+    extern __shared__ double dsm[];
+    auto a = reinterpret_cast<double (*)[kNb + 1]>(dsm);
+    auto li = a + kNb;
+    auto ui = li + kNb;
     const int b = b0 + blockIdx.x;
     const int k0 = b * kNb, kb = min(kNb, n - k0);
-    double* Li = inv + 2LL * b * kNb * kNb;
-    double* Ui = Li + kNb * kNb;
     for (int t = threadIdx.x; t < kb * kb; t += blockDim.x) {
         const int r = t / kb, c = t - r * kb;
         a[r][c] = M[(size_t)(k0 + r) * n + k0 + c];
     }
     __syncthreads();
-    const int c = threadIdx.x;
-    if (c < kb && blockIdx.y == 0) {
-        for (int r = 0; r < kb; ++r) {              // L x = e_c
-            double acc = (r == c) ? 1.0 : 0.0;
-            if (r > c)
-                for (int q = c; q < r; ++q) acc = __dsub_rn(acc, __dmul_rn(a[r][q], Li[q * kNb + c]));
-            Li[r * kNb + c] = r < c ? 0.0 : acc;
-        }
+    double* Li = inv + 2LL * b * kNb * kNb;
+    block_inverses_smem(kb, a, li, ui, Li, Li + kNb * kNb);
+}
+
+// ------------------------------------------------------------ without pivoting
+// The no-interchange step for diagonal block k0 in one kernel: factor A11 = L11 U11 in
+// shared memory (the arithmetic of the column-by-column elimination: l = a_rj * (1/a_jj),
+// a_rc -= l * a_jc, then the column scaled), flag a pivot below `floor`, write the factors
+// back, and form Li, Ui (block_inverses_smem).  256 threads as 16 x 16 over the trailing
+// rows and columns, one barrier per column.  Dynamic shared memory: kDiagSmem.
+__global__ void __launch_bounds__(256) k_lu_diag_inv(int n, int k0, int kb, double* M, double floor,
+                                                     int* tiny, double* inv) {
+    extern __shared__ double dsm[];
+    auto a = reinterpret_cast<double (*)[kNb + 1]>(dsm);
+    auto li = a + kNb;
+    auto ui = li + kNb;
+    for (int t = threadIdx.x; t < kb * kb; t += blockDim.x) {
+        const int r = t / kb, c = t - r * kb;
+        a[r][c] = M[(size_t)(k0 + r) * n + k0 + c];
     }
-    if (c < kb && blockIdx.y == 1) {
-        for (int r = kb - 1; r >= 0; --r) {         // U x = e_c
-            double acc = (r == c) ? 1.0 : 0.0;
-            if (r <= c) {
-                for (int q = r + 1; q <= c; ++q) acc = __dsub_rn(acc, __dmul_rn(a[r][q], Ui[q * kNb + c]));
-                acc = acc / a[r][r];
-            }
-            Ui[r * kNb + c] = r > c ? 0.0 : acc;
+    __syncthreads();
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    for (int j = 0; j < kb; ++j) {
+        const double d = a[j][j];
+        if (threadIdx.x == 0 && !(fabs(d) > floor)) *tiny = 1;
+        const double inv_d = (d != 0.0) ? 1.0 / d : 0.0;
+        for (int r = j + 1 + ty; r < kb; r += 16) {
+            const double l = __dmul_rn(a[r][j], inv_d);
+            for (int c = j + 1 + tx; c < kb; c += 16) a[r][c] = __dsub_rn(a[r][c], __dmul_rn(l, a[j][c]));
         }
+        __syncthreads();
+        // column j is read by nobody in step j + 1 (it touches columns > j + 1 and row j + 1)
+        for (int r = j + 1 + threadIdx.x; r < kb; r += blockDim.x) a[r][j] = __dmul_rn(a[r][j], inv_d);
     }
+    __syncthreads();
+    for (int t = threadIdx.x; t < kb * kb; t += blockDim.x) {
+        const int r = t / kb, c = t - r * kb;
+        M[(size_t)(k0 + r) * n + k0 + c] = a[r][c];
+    }
+    double* Li = inv + 2LL * (k0 / kNb) * kNb * kNb;
+    block_inverses_smem(kb, a, li, ui, Li, Li + kNb * kNb);
 }
 
 // dst (rows x cols, ld ldd) = src (ld lds), row-major.
@@ -300,25 +327,126 @@ __global__ void k_perm_identity(int n, const int* __restrict__ piv, double* X) {
     }
 }
 
-void cublas_check(cublasStatus_t s, const char* what) {
-    if (s != CUBLAS_STATUS_SUCCESS) fail(HAMLSS_ERR_CUDA, std::string("cuBLAS ") + what + " failed");
+// ------------------------------------------------------------------------ DGEMM
+// C (m x p, ldc) = alpha * A (m x k, lda) * B (k x p, ldb) + beta * C, all row-major FP64,
+// on the FP64 tensor cores (mma.sync m8n8k4 .f64 -- the FP64 matrix path of sm_100a;
+// tcgen05 has no FP64 kind).  A CTA computes a 128 x 64 tile with 8 warps of 32 x 32
+// (4 x 4 MMA tiles each); K advances in steps of 16 staged in shared memory, the next
+// step's tile loaded into registers while the current one is multiplied.  Row strides
+// of the staged tiles (20 and 68 doubles) keep each half-warp's fragment loads on distinct
+// banks.  Edges are zero-filled, so any m, p, k works.
+constexpr int kGBM = 128, kGBN = 64, kGBK = 16, kGThreads = 256;
+constexpr int kGAS = kGBK + 4;       // A tile row stride (doubles)
+constexpr int kGBS = kGBN + 4;       // B tile row stride
+
+__device__ __forceinline__ void dmma_8x8x4(double (&d)[2], double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(d[0]), "+d"(d[1]) : "d"(a), "d"(b));
+}
+
+__global__ void __launch_bounds__(kGThreads) k_dgemm(int m, int p, int k, double alpha,
+                                                     const double* __restrict__ A, int lda,
+                                                     const double* __restrict__ B, int ldb, double beta,
+                                                     double* __restrict__ C, int ldc) {
+    __shared__ double As[kGBM * kGAS];
+    __shared__ double Bs[kGBK * kGBS];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int wm = warp >> 1, wn = warp & 1;                 // 4 x 2 warps of 32 x 32
+    const int bm = blockIdx.y * kGBM, bn = blockIdx.x * kGBN;
+    const int fr = lane >> 2, fk = lane & 3;                 // fragment row / k (A), k / col (B)
+    double acc[4][4][2];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+    double ra[(kGBM * kGBK) / kGThreads], rb[(kGBK * kGBN) / kGThreads];
+    auto load = [&](int k0) {
+#pragma unroll
+        for (int q = 0; q < (kGBM * kGBK) / kGThreads; ++q) {
+            const int e = tid + kGThreads * q, r = e / kGBK, c = e % kGBK;
+            const int gr = bm + r, gc = k0 + c;
+            ra[q] = (gr < m && gc < k) ? A[(size_t)gr * lda + gc] : 0.0;
+        }
+#pragma unroll
+        for (int q = 0; q < (kGBK * kGBN) / kGThreads; ++q) {
+            const int e = tid + kGThreads * q, r = e / kGBN, c = e % kGBN;
+            const int gr = k0 + r, gc = bn + c;
+            rb[q] = (gr < k && gc < p) ? B[(size_t)gr * ldb + gc] : 0.0;
+        }
+    };
+    auto store = [&]() {
+#pragma unroll
+        for (int q = 0; q < (kGBM * kGBK) / kGThreads; ++q) {
+            const int e = tid + kGThreads * q;
+            As[(e / kGBK) * kGAS + e % kGBK] = ra[q];
+        }
+#pragma unroll
+        for (int q = 0; q < (kGBK * kGBN) / kGThreads; ++q) {
+            const int e = tid + kGThreads * q;
+            Bs[(e / kGBN) * kGBS + e % kGBN] = rb[q];
+        }
+    };
+    const int nk = (k + kGBK - 1) / kGBK;
+    if (nk > 0) {
+        load(0);
+        store();
+    }
+    __syncthreads();
+    for (int kt = 0; kt < nk; ++kt) {
+        if (kt + 1 < nk) load((kt + 1) * kGBK);
+#pragma unroll
+        for (int ks = 0; ks < kGBK; ks += 4) {
+            double af[4], bf[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) af[i] = As[(wm * 32 + i * 8 + fr) * kGAS + ks + fk];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) bf[j] = Bs[(ks + fk) * kGBS + wn * 32 + j * 8 + fr];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) dmma_8x8x4(acc[i][j], af[i], bf[j]);
+        }
+        __syncthreads();
+        if (kt + 1 < nk) {
+            store();
+            __syncthreads();
+        }
+    }
+    // accumulator element h of tile (i, j): row fr, column 2 * fk + h of the 8 x 8 tile
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int r = bm + wm * 32 + i * 8 + fr, c = bn + wn * 32 + j * 8 + 2 * fk + h;
+                if (r < m && c < p) {
+                    double* cp = C + (size_t)r * ldc + c;
+                    const double v = alpha * acc[i][j][h];
+                    *cp = beta != 0.0 ? v + beta * *cp : v;
+                }
+            }
+}
+
+void dgemm(Ctx& ctx, int m, int p, int k, double alpha, const double* A, int lda, const double* B, int ldb,
+           double beta, double* C, int ldc) {
+    if (m <= 0 || p <= 0) return;
+    const dim3 grid(ceil_div(p, kGBN), ceil_div(m, kGBM));
+    k_dgemm<<<grid, kGThreads, 0, ctx.lane.stream>>>(m, p, k, alpha, A, lda, B, ldb, beta, C, ldc);
+    HAMLSS_LAUNCH_CHECK();
 }
 
 // Row-major C (m x p, ld n) -= A (m x k, ld n) * B (k x p, ld n).
-void gemm_sub(cublasHandle_t h, int n, int m, int p, int k, const double* A, const double* B, double* C) {
+void gemm_sub(Ctx& ctx, int n, int m, int p, int k, const double* A, const double* B, double* C) {
     if (m <= 0 || p <= 0 || k <= 0) return;
-    const double minus1 = -1.0, one = 1.0;
-    cublas_check(cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, p, m, k, &minus1, B, n, A, n, &one, C, n),
-                 "dgemm");
+    dgemm(ctx, m, p, k, -1.0, A, n, B, n, 1.0, C, n);
 }
 
 // Row-major C (m x p, ldc) = A (m x k, lda) * B (k x p, ldb).
-void gemm_set(cublasHandle_t h, int m, int p, int k, const double* A, int lda, const double* B, int ldb,
+void gemm_set(Ctx& ctx, int m, int p, int k, const double* A, int lda, const double* B, int ldb,
               double* C, int ldc) {
     if (m <= 0 || p <= 0 || k <= 0) return;
-    const double one = 1.0, zero = 0.0;
-    cublas_check(cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, p, m, k, &one, B, ldb, A, lda, &zero, C, ldc),
-                 "dgemm");
+    dgemm(ctx, m, p, k, 1.0, A, lda, B, ldb, 0.0, C, ldc);
 }
 
 int copy_grid(Ctx& ctx, long long count) {
@@ -334,29 +462,16 @@ __global__ void k_iota(int n, int* piv) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) piv[i] = i;
 }
 
-cublasHandle_t blas_of(Ctx& ctx) {
-    if (!ctx.blas) {
-        cublasHandle_t h = nullptr;
-        cublas_check(cublasCreate(&h), "create");
-        ctx.blas = h;
-    }
-    cublasHandle_t h = static_cast<cublasHandle_t>(ctx.blas);
-    cublas_check(cublasSetStream(h, ctx.lane.stream), "set stream");
-    cublas_check(cublasSetMathMode(h, CUBLAS_DEFAULT_MATH), "math mode");
-    return h;
-}
-
 // Blocked LU without row interchanges; false when a pivot falls below `floor`.
 // L21 = A21 U11^-1 and U12 = L11^-1 A12 are GEMMs with the diagonal block's inverses
 // (k_block_inverses) through the scratch T (n x kNb doubles).
-bool factor_nopivot(Ctx& ctx, cublasHandle_t h, int n, double* M, double floor, double* inv, double* T) {
+bool factor_nopivot(Ctx& ctx, int n, double* M, double floor, double* inv, double* T) {
     cudaStream_t s = ctx.lane.stream;
     DBuf<int> tiny(1);
     tiny.zero(s);
     for (int k0 = 0; k0 < n; k0 += kNb) {
         const int kb = std::min(kNb, n - k0);
-        k_lu_diag_nopiv<<<1, 256, 0, s>>>(n, k0, kb, M, floor, tiny.p);
-        k_block_inverses<<<dim3(1, 2), kNb, 0, s>>>(n, k0 / kNb, M, inv);
+        k_lu_diag_inv<<<1, 256, kDiagSmem, s>>>(n, k0, kb, M, floor, tiny.p, inv);
         HAMLSS_LAUNCH_CHECK();
         const int rest = n - k0 - kb;
         if (rest > 0) {
@@ -364,13 +479,13 @@ bool factor_nopivot(Ctx& ctx, cublasHandle_t h, int n, double* M, double floor, 
             const double* Ui = Li + kNb * kNb;
             double* A21 = M + (size_t)(k0 + kb) * n + k0;
             double* A12 = M + (size_t)k0 * n + k0 + kb;
-            gemm_set(h, rest, kb, kb, A21, n, Ui, kNb, T, kNb);
+            gemm_set(ctx, rest, kb, kb, A21, n, Ui, kNb, T, kNb);
             k_copy_block<<<copy_grid(ctx, (long long)rest * kb), 256, 0, s>>>(rest, kb, T, kNb, A21, n);
             HAMLSS_LAUNCH_CHECK();
-            gemm_set(h, kb, rest, kb, Li, kNb, A12, n, T, rest);
+            gemm_set(ctx, kb, rest, kb, Li, kNb, A12, n, T, rest);
             k_copy_block<<<copy_grid(ctx, (long long)rest * kb), 256, 0, s>>>(kb, rest, T, rest, A12, n);
             HAMLSS_LAUNCH_CHECK();
-            gemm_sub(h, n, rest, rest, kb, A21, A12, M + (size_t)(k0 + kb) * n + k0 + kb);
+            gemm_sub(ctx, n, rest, rest, kb, A21, A12, M + (size_t)(k0 + kb) * n + k0 + kb);
         }
     }
     int t = 0;
@@ -380,7 +495,7 @@ bool factor_nopivot(Ctx& ctx, cublasHandle_t h, int n, double* M, double floor, 
 }
 
 // Blocked LU with partial pivoting (cooperative panels).
-void factor_pivot(Ctx& ctx, cublasHandle_t h, int n, double* M, int* piv) {
+void factor_pivot(Ctx& ctx, int n, double* M, int* piv) {
     cudaStream_t s = ctx.lane.stream;
     DBuf<double> cand_v(ctx.sm_count);
     DBuf<int> cand_i(ctx.sm_count), singular(1);
@@ -404,7 +519,7 @@ void factor_pivot(Ctx& ctx, cublasHandle_t h, int n, double* M, int* piv) {
         if (rest > 0) {
             k_trsm_lower_unit<<<col_grid(ctx, rest), 128, 0, s>>>(n, k0, kb, M, n, M, n, k0 + kb, n);
             HAMLSS_LAUNCH_CHECK();
-            gemm_sub(h, n, rest, rest, kb, M + (size_t)(k0 + kb) * n + k0, M + (size_t)k0 * n + k0 + kb,
+            gemm_sub(ctx, n, rest, rest, kb, M + (size_t)(k0 + kb) * n + k0, M + (size_t)k0 * n + k0 + kb,
                      M + (size_t)(k0 + kb) * n + k0 + kb);
         }
     }
@@ -414,13 +529,70 @@ void factor_pivot(Ctx& ctx, cublasHandle_t h, int n, double* M, int* piv) {
     if (sing) fail(HAMLSS_ERR_ZERO_PIVOT, "coarsest AMG level is singular (zero pivot in its dense LU)");
 }
 
+// ---------------------------------------------------------------- Gram matrix
+constexpr int kGramRows = 128;
+constexpr int kGramMaxC = 33;
+
+// pair index q -> (a, b), a <= b, pairs listed row by row of the upper triangle
+__device__ void gram_pair(int c, int q, int* a, int* b) {
+    int r = 0;
+    while (q >= c - r) { q -= c - r; ++r; }
+    *a = r;
+    *b = r + q;
+}
+
+__global__ void __launch_bounds__(256) k_gram_partial(int n, int c, const double* __restrict__ Y,
+                                                      long long ld, double* part) {
+    __shared__ double tile[kGramRows][kGramMaxC + 1];
+    const int np = c * (c + 1) / 2;
+    int pa[3], pb[3];
+    double acc[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int u = 0; u < 3; ++u) {
+        const int q = threadIdx.x + 256 * u;
+        pa[u] = pb[u] = 0;
+        if (q < np) gram_pair(c, q, &pa[u], &pb[u]);
+    }
+    for (int r0 = blockIdx.x * kGramRows; r0 < n; r0 += gridDim.x * kGramRows) {
+        for (int e = threadIdx.x; e < kGramRows * c; e += blockDim.x) {
+            const int j = e / kGramRows, r = e - j * kGramRows;
+            tile[r][j] = (r0 + r < n) ? Y[(size_t)j * ld + r0 + r] : 0.0;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int u = 0; u < 3; ++u)
+            if (threadIdx.x + 256 * u < np)
+                for (int r = 0; r < kGramRows; ++r) acc[u] += tile[r][pa[u]] * tile[r][pb[u]];
+        __syncthreads();
+    }
+#pragma unroll
+    for (int u = 0; u < 3; ++u) {
+        const int q = threadIdx.x + 256 * u;
+        if (q < np) part[(size_t)blockIdx.x * np + q] = acc[u];
+    }
+}
+
+// G[a][b] = G[b][a] = the blocks' partial sums of pair (a, b), added in block order
+__global__ void k_gram_reduce(int c, int nblocks, const double* __restrict__ part, double* G) {
+    const int np = c * (c + 1) / 2;
+    for (int q = threadIdx.x; q < np; q += blockDim.x) {
+        double s = 0.0;
+        for (int b = 0; b < nblocks; ++b) s += part[(size_t)b * np + q];
+        int a, bb;
+        gram_pair(c, q, &a, &bb);
+        G[a * c + bb] = s;
+        G[bb * c + a] = s;
+    }
+}
+
 }  // namespace
 
 void dense_lu_inverse(Ctx& ctx, int n, double* M, double* Minv, int* piv) {
     cudaStream_t s = ctx.lane.stream;
     if (n <= 0) return;
-    cublasHandle_t h = blas_of(ctx);
     const int cg_ = col_grid(ctx, n);
+    HAMLSS_CUDA(cudaFuncSetAttribute(k_lu_diag_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDiagSmem));
+    HAMLSS_CUDA(cudaFuncSetAttribute(k_block_inverses, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDiagSmem));
     const size_t bytes = sizeof(double) * (size_t)n * n;
     // First without interchanges (the coarse operators here are symmetric positive definite
     // or close to diagonally dominant, where that is stable); if a pivot falls below
@@ -438,13 +610,13 @@ void dense_lu_inverse(Ctx& ctx, int n, double* M, double* Minv, int* piv) {
     std::memcpy(&big, &bits, sizeof big);
     const int nblk = (n + kNb - 1) / kNb;
     DBuf<double> inv(2LL * nblk * kNb * kNb), T((size_t)n * kNb);
-    if (factor_nopivot(ctx, h, n, M, 1e-10 * big, inv.p, T.p)) {
+    if (factor_nopivot(ctx, n, M, 1e-10 * big, inv.p, T.p)) {
         k_iota<<<cg_, 128, 0, s>>>(n, piv);
         HAMLSS_LAUNCH_CHECK();
     } else {
         HAMLSS_CUDA(cudaMemcpyAsync(M, Minv, bytes, cudaMemcpyDeviceToDevice, s));
-        factor_pivot(ctx, h, n, M, piv);
-        k_block_inverses<<<dim3(nblk, 2), kNb, 0, s>>>(n, 0, M, inv.p);
+        factor_pivot(ctx, n, M, piv);
+        k_block_inverses<<<nblk, 2 * kNb, kDiagSmem, s>>>(n, 0, M, inv.p);
         HAMLSS_LAUNCH_CHECK();
     }
     // X = P I; L Y = X (forward, unit lower); U X = Y (backward).  The diagonal blocks are
@@ -455,29 +627,34 @@ void dense_lu_inverse(Ctx& ctx, int n, double* M, double* Minv, int* piv) {
     for (int k0 = 0; k0 < n; k0 += kNb) {
         const int kb = std::min(kNb, n - k0);
         const double* Li = inv.p + 2LL * (k0 / kNb) * kNb * kNb;
-        gemm_set(h, kb, n, kb, Li, kNb, Minv + (size_t)k0 * n, n, W.p, n);
+        gemm_set(ctx, kb, n, kb, Li, kNb, Minv + (size_t)k0 * n, n, W.p, n);
         k_copy_block<<<copy_grid(ctx, (long long)kb * n), 256, 0, s>>>(kb, n, W.p, n, Minv + (size_t)k0 * n, n);
         HAMLSS_LAUNCH_CHECK();
         const int rest = n - k0 - kb;
-        gemm_sub(h, n, rest, n, kb, M + (size_t)(k0 + kb) * n + k0, Minv + (size_t)k0 * n,
+        gemm_sub(ctx, n, rest, n, kb, M + (size_t)(k0 + kb) * n + k0, Minv + (size_t)k0 * n,
                  Minv + (size_t)(k0 + kb) * n);
     }
     const int last = ((n - 1) / kNb) * kNb;
     for (int k0 = last; k0 >= 0; k0 -= kNb) {
         const int kb = std::min(kNb, n - k0);
         const double* Ui = inv.p + 2LL * (k0 / kNb) * kNb * kNb + kNb * kNb;
-        gemm_set(h, kb, n, kb, Ui, kNb, Minv + (size_t)k0 * n, n, W.p, n);
+        gemm_set(ctx, kb, n, kb, Ui, kNb, Minv + (size_t)k0 * n, n, W.p, n);
         k_copy_block<<<copy_grid(ctx, (long long)kb * n), 256, 0, s>>>(kb, n, W.p, n, Minv + (size_t)k0 * n, n);
         HAMLSS_LAUNCH_CHECK();
-        gemm_sub(h, n, k0, n, kb, M + k0, Minv + (size_t)k0 * n, Minv);
+        gemm_sub(ctx, n, k0, n, kb, M + k0, Minv + (size_t)k0 * n, Minv);
     }
     HAMLSS_CUDA(cudaStreamSynchronize(s));
 }
 
-void* blas_stream_handle(Ctx& ctx) { return blas_of(ctx); }
+int gram_partials(Ctx& ctx, int c) { return ctx.sm_count * 4 * (c * (c + 1) / 2); }
 
-void blas_destroy(void* h) {
-    if (h) cublasDestroy(static_cast<cublasHandle_t>(h));
+void gram_matrix(Ctx& ctx, int n, int c, const double* Y, long long ld, double* G, double* part) {
+    if (c < 1 || c > kGramMaxC) fail(HAMLSS_ERR_INVALID, "Gram matrix of more than 33 columns");
+    const int blocks = std::max(1, std::min(ceil_div(n, kGramRows), ctx.sm_count * 4));
+    k_gram_partial<<<blocks, 256, 0, ctx.lane.stream>>>(n, c, Y, ld, part);
+    HAMLSS_LAUNCH_CHECK();
+    k_gram_reduce<<<1, 256, 0, ctx.lane.stream>>>(c, blocks, part, G);
+    HAMLSS_LAUNCH_CHECK();
 }
 
 }  // namespace hamlss

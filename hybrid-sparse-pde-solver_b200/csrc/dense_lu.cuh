@@ -11,10 +11,11 @@ namespace hamlss {
 // Synchronises the context stream.
 void dense_lu_inverse(Ctx& ctx, int n, double* M, double* Minv, int* piv);
 
-// Release a context's cuBLAS handle (Ctx::blas).
-void blas_destroy(void* handle);
-// The context's cuBLAS handle (a cublasHandle_t, created on first use), bound to the
-// context's stream.
-void* blas_stream_handle(Ctx& ctx);
+// Gram matrix G = Y^T Y ((c x c, row-major, device) of the c columns of Y (column j at
+// Y + j * ld, n entries each), c <= 33: block partial sums over row tiles in shared
+// memory, then one ordered reduction over the blocks (deterministic).  `part` holds
+// sm_count * 4 * c * (c + 1) / 2 doubles.
+void gram_matrix(Ctx& ctx, int n, int c, const double* Y, long long ld, double* G, double* part);
+int gram_partials(Ctx& ctx, int c);
 
 }  // namespace hamlss

@@ -97,7 +97,6 @@ struct Ctx {
     Profiler prof;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     HBuf<char> host_poll;      // pinned landing zone for polled device state
-    void* blas = nullptr;      // cuBLAS handle, created on first use (dense coarse LU)
     // SpGEMM capacity slots (AMG setup), grown on demand and kept: setups of similar
     // matrices then allocate nothing large (fresh pool memory of GBs maps slowly)
     DBuf<int> gemm_ci;

@@ -12,7 +12,11 @@
 //               does not, at most kMaxBypass times; 1 fewest nonzeros first -- the least
 //               work first, which keeps the median latency down under steady load but
 //               leaves the largest requests to the end of a burst -- where a request passed
-//               kMaxAgeBypass times leads and is passed by nobody.
+//               kMaxAgeBypass times leads and is passed by nobody.  In both orders at most
+//               max_large requests of large_rows rows or more run at once (default 1):
+//               under processor sharing a large solve next to three others runs several
+//               times slower and sets the tail latency, while the requests that pass the
+//               waiting large one are short.
 //   solve lanes `slots` worker threads, each with its own engine context (its own CUDA
 //               stream), take admitted requests and run the adaptive ladder on them; their
 //               kernels overlap on the device.
@@ -138,6 +142,7 @@ struct hamlss_server {
     int64_t next_id = 1;
     int64_t admitted = 0, peak_admitted = 0;
     int running = 0, peak_running = 0;
+    int running_large = 0;              // admitted requests with n >= cfg.large_rows
     bool stop = false;
     std::vector<hamlss_ctx*> ctxs;
     std::vector<std::thread> threads;
@@ -147,6 +152,12 @@ struct hamlss_server {
     std::vector<double> latencies;
     double t_first = -1.0, t_last = 0.0;
 
+    bool is_large(const Request* r) const { return r->n >= cfg.large_rows; }
+    // a large request waits while max_large of them run (others may pass it meanwhile)
+    bool large_blocked(const Request* r) const {
+        return cfg.max_large > 0 && is_large(r) && running_large >= cfg.max_large;
+    }
+
     // ---- queue selection (mu held)
     Request* pick(std::deque<Request*>& q) {
         if (cfg.order == 1 && !q.empty()) {
@@ -154,7 +165,7 @@ struct hamlss_server {
             // the lanes are busy); a request passed kMaxAgeBypass times goes first, and while
             // it does not fit nobody passes it
             Request* h = q.front();
-            if (h->bypassed >= kMaxAgeBypass) {
+            if (h->bypassed >= kMaxAgeBypass && !large_blocked(h)) {
                 if (admitted + h->footprint > cfg.hbm_budget_bytes) return nullptr;
                 q.pop_front();
                 admit(h);
@@ -162,7 +173,7 @@ struct hamlss_server {
             }
             long best = -1;
             for (size_t i = 0; i < q.size(); ++i)
-                if (admitted + q[i]->footprint <= cfg.hbm_budget_bytes &&
+                if (admitted + q[i]->footprint <= cfg.hbm_budget_bytes && !large_blocked(q[i]) &&
                     (best < 0 || q[i]->nnz < q[(size_t)best]->nnz))
                     best = (long)i;
             if (best < 0) return nullptr;
@@ -172,19 +183,23 @@ struct hamlss_server {
             admit(r);
             return r;
         }
+        Request* head = nullptr;          // the first request not held by max_large
         for (size_t i = 0; i < q.size(); ++i) {
             Request* r = q[i];
+            if (large_blocked(r)) continue;
             if (admitted + r->footprint <= cfg.hbm_budget_bytes) {
-                if (i > 0) ++q.front()->bypassed;
+                if (head) ++head->bypassed;
                 q.erase(q.begin() + (long)i);
                 admit(r);
                 return r;
             }
-            if (i == 0 && r->bypassed >= kMaxBypass) return nullptr;  // head waits, nobody passes
+            if (!head && r->bypassed >= kMaxBypass) return nullptr;  // head waits, nobody passes
+            if (!head) head = r;
         }
         return nullptr;
     }
     void admit(Request* r) {
+        if (is_large(r)) ++running_large;
         admitted += r->footprint;
         peak_admitted = std::max(peak_admitted, admitted);
         r->state = St::Running;
@@ -192,6 +207,7 @@ struct hamlss_server {
         peak_running = std::max(peak_running, running);
     }
     void retire(Request* r, bool requeue) {
+        if (is_large(r)) --running_large;
         admitted -= r->footprint;
         --running;
         if (requeue) {
@@ -398,6 +414,8 @@ void hamlss_server_config_default(hamlss_server_config* c) {
     c->batch_max_rows = 16384;
     c->batch_max_count = 2048;
     c->order = 0;
+    c->large_rows = 1 << 20;
+    c->max_large = 1;
 }
 
 int hamlss_server_create(const hamlss_server_config* config, hamlss_server** out) {
@@ -408,6 +426,8 @@ int hamlss_server_create(const hamlss_server_config* config, hamlss_server** out
     else hamlss_server_config_default(&c);
     if (c.slots < 1 || c.slots > 64) return fail(HAMLSS_ERR_INVALID, "slots must be in [1, 64]");
     if (c.order != 0 && c.order != 1) return fail(HAMLSS_ERR_INVALID, "order must be 0 or 1");
+    if (c.large_rows < 1 || c.max_large < 0)
+        return fail(HAMLSS_ERR_INVALID, "large_rows >= 1 and max_large >= 0");
     if (c.hbm_budget_bytes <= 0) return fail(HAMLSS_ERR_INVALID, "hbm_budget_bytes must be > 0");
     if (c.batch_max_rows < 0 || (c.batch_max_rows > 0 && c.batch_max_count < 1))
         return fail(HAMLSS_ERR_INVALID, "batch_max_rows >= 0 and batch_max_count >= 1");

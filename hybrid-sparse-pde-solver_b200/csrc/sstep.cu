@@ -23,8 +23,6 @@
 #include <cstring>
 #include <vector>
 
-#include <cublas_v2.h>
-
 #include "dense_lu.cuh"
 #include "krylov.cuh"
 
@@ -181,10 +179,6 @@ k_sstep_update(int n, int k, double* x, const double* __restrict__ B, long long 
     }
 }
 
-void cublas_ok(cublasStatus_t s) {
-    if (s != CUBLAS_STATUS_SUCCESS) fail(HAMLSS_ERR_CUDA, "cuBLAS DGEMM (s-step Gram matrix) failed");
-}
-
 // chebyshev_shifts (sstep_cg_solver.cpp:26-37)
 std::vector<double> chebyshev_shifts(double lo, double hi, int k) {
     std::vector<double> t(k);
@@ -305,6 +299,7 @@ SolveResult sstep_solve(Ctx& ctx, hamlss_mat* A, const double* b, double* x, con
     long long flops = 0, bytes = 0;
     int total = 0;
     std::vector<double> G;
+    DBuf<double> gram_part;
     auto build = [&](int kb) {
         // build_basis (sstep_cg_solver.cpp:44-66)
         const std::vector<double> th = chebyshev_shifts(lam_min, lam_max, kb);
@@ -316,13 +311,11 @@ SolveResult sstep_solve(Ctx& ctx, hamlss_mat* A, const double* b, double* x, con
                                    "sstep_basis", 24.0 * n);
             launch_vec<0>(sm, L, n, BodyScaleDev{Bcol(j), s, 0.0}, NoFin{}, nullptr, "vec", 16.0 * n);
         }
-        // gram_matrix (:71-80) and rhs_ls[i] = r . B[i] (:228-230): one (kb+1)^2 DGEMM
+        // gram_matrix (:71-80) and rhs_ls[i] = r . B[i] (:228-230): one (kb+1)^2 Gram matrix
         {
             ProfScope ps(L, "sstep_gram", 8.0 * (double)n * (kb + 1));
-            cublasHandle_t hb = static_cast<cublasHandle_t>(blas_stream_handle(ctx));
-            const double one = 1.0, zero = 0.0;
-            cublas_ok(cublasDgemm(hb, CUBLAS_OP_T, CUBLAS_OP_N, kb + 1, kb + 1, n, &one, Y, (int)ld, Y,
-                                  (int)ld, &zero, Gd, kb + 1));
+            gram_part.ensure((size_t)gram_partials(ctx, kb + 1));
+            gram_matrix(ctx, n, kb + 1, Y, (long long)ld, Gd, gram_part.p);
         }
         G.assign((size_t)(kb + 1) * (kb + 1), 0.0);
         HAMLSS_CUDA(cudaMemcpyAsync(G.data(), Gd, sizeof(double) * G.size(), cudaMemcpyDeviceToHost, st));

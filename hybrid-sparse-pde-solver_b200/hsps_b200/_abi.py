@@ -161,6 +161,8 @@ class ServerConfig(C.Structure):
         ("batch_max_rows", C.c_int32),
         ("batch_max_count", C.c_int32),
         ("order", C.c_int32),
+        ("large_rows", C.c_int32),
+        ("max_large", C.c_int32),
     ]
 
 

@@ -354,6 +354,10 @@ typedef struct hamlss_server_config {
     int32_t order;             /* solve-lane queue: 0 arrival order (a fitting request may  */
                                /* pass a head that does not fit, at most 8 times) (0); 1    */
                                /* fewest nonzeros first, a request passed 32 times leads    */
+    int32_t large_rows;        /* requests with n >= large_rows are "large" (1048576)       */
+    int32_t max_large;         /* large requests running at once; 0: no bound (1).  Others  */
+                               /* pass a large head that waits for this bound, so one large */
+                               /* solve at a time keeps its speed while small ones flow      */
 } hamlss_server_config;
 
 typedef struct hamlss_server_report {
