@@ -204,13 +204,82 @@ __device__ double p_value(int i, int c, int s, int e, const int* __restrict__ ci
     return val;
 }
 
+// Rows of at most kLongRow entries, one warp per row (lane a holds entry a).  Candidate
+// agg(i) first, then the off-diagonal entries' aggregates at their first occurrence
+// (__match_any_sync); each candidate's value is formed by its lane walking the row's
+// entries in order through shuffles, with p_value's operations: val = [c == agg(i)], then
+// val -= (omega / a_ii) * a_ij for every off-diagonal j of aggregate c, in row order.
+// Survivors (|val| > 1e-14) are written in column order (rank = survivors with a smaller
+// column).  Same entries, values and order as the thread-per-row kernel below.
+template <bool FILL>
+__global__ void k_smooth_p_warp(int n, const int* __restrict__ rp, const int* __restrict__ ci,
+                                const double* __restrict__ v, const int* __restrict__ agg, double omega,
+                                int* pcnt, const int* __restrict__ prp, int* pci, double* pv) {
+    const int lane = threadIdx.x & 31;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += nwarps) {
+        const int s = rp[i], len = rp[i + 1] - s;
+        if (len > kLongRow) continue;                    // the block or thread kernels take it
+        const bool have = lane < len;
+        const int j = have ? ci[s + lane] : -1;
+        const double va = have ? v[s + lane] : 0.0;
+        const bool diag = have && j == i;
+        const unsigned dmask = __ballot_sync(0xffffffffu, diag);
+        double id = 0.0;
+        if (dmask) {
+            const double dv = __shfl_sync(0xffffffffu, va, __ffs(dmask) - 1);
+            id = (fabs(dv) > kEps) ? omega / dv : 0.0;
+        }
+        const bool raw = fabs(id) < kEps;
+        const int ai = agg[i];
+        const int c = (have && !diag) ? agg[j] : -1;     // this entry's aggregate
+        const unsigned same = __match_any_sync(0xffffffffu, c);
+        const bool cand = !raw && c >= 0 && c != ai && (__ffs(same) - 1) == lane;
+        double val = 0.0, val0 = 1.0;                    // own candidate / agg(i)
+        if (!raw) {
+            for (int l = 0; l < len; ++l) {
+                const int cl = __shfl_sync(0xffffffffu, c, l);
+                const double vl = __shfl_sync(0xffffffffu, va, l);
+                if (cl < 0) continue;
+                if (cand && cl == c) val = __dsub_rn(val, __dmul_rn(id, vl));
+                if (cl == ai) val0 = __dsub_rn(val0, __dmul_rn(id, vl));
+            }
+        }
+        const bool keep = cand && fabs(val) > 1e-14;
+        const bool keep0 = fabs(val0) > 1e-14;
+        const unsigned kmask = __ballot_sync(0xffffffffu, keep);
+        if (!FILL) {
+            if (lane == 0) pcnt[i] = __popc(kmask) + (keep0 ? 1 : 0);
+            continue;
+        }
+        // ranks by column among the survivors
+        const int myc = keep ? c : INT_MAX;
+        int rank = (keep0 && ai < myc) ? 1 : 0, rank0 = 0;
+        for (int l = 0; l < 32; ++l) {
+            const int cl = __shfl_sync(0xffffffffu, myc, l);
+            if (cl < myc) ++rank;
+            if (cl < ai) ++rank0;
+        }
+        const int o = prp[i];
+        if (keep) {
+            pci[o + rank] = c;
+            pv[o + rank] = val;
+        }
+        if (keep0 && lane == 0) {
+            pci[o + rank0] = ai;
+            pv[o + rank0] = val0;
+        }
+    }
+}
+
+// Rows the warp and block kernels leave (kSortMax entries or more), one thread per row.
 template <bool FILL>
 __global__ void k_smooth_p(int n, const int* __restrict__ rp, const int* __restrict__ ci,
                            const double* __restrict__ v, const int* __restrict__ agg, double omega,
                            int* pcnt, const int* __restrict__ prp, int* pci, double* pv) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const int s = rp[i], e = rp[i + 1];
-        if (smooth_row_on_block(e - s)) continue;       // k_smooth_p_rows takes it
+        if (e - s <= kLongRow || smooth_row_on_block(e - s)) continue;   // warp / block kernels
         double id = 0.0;
         for (int k = s; k < e; ++k)
             if (ci[k] == i) { id = (fabs(v[k]) > kEps) ? omega / v[k] : 0.0; break; }
@@ -1549,6 +1618,8 @@ void smooth_prolongation(Ctx& ctx, const Csr<double>& A, const DBuf<int>& agg, i
     DBuf<int> cnt(n), list;
     size_t smem = 0;                                // keys + values of the longest row
     const int nlong = long_rows(ctx, n, A.rp, list, &smem);
+    const int gw = std::max(1, std::min(ceil_div(n, 8), ctx.sm_count * 8));      // 8 warps a block
+    k_smooth_p_warp<false><<<gw, 256, 0, s>>>(n, A.rp, A.ci, A.v, agg.p, omega, cnt.p, nullptr, nullptr, nullptr);
     k_smooth_p<false><<<g, 256, 0, s>>>(n, A.rp, A.ci, A.v, agg.p, omega, cnt.p, nullptr, nullptr, nullptr);
     HAMLSS_LAUNCH_CHECK();
     if (nlong) {
@@ -1558,6 +1629,7 @@ void smooth_prolongation(Ctx& ctx, const Csr<double>& A, const DBuf<int>& agg, i
         HAMLSS_LAUNCH_CHECK();
     }
     build_csr_counts(ctx, P, n, nc, cnt);
+    k_smooth_p_warp<true><<<gw, 256, 0, s>>>(n, A.rp, A.ci, A.v, agg.p, omega, nullptr, P.rp.p, P.ci.p, P.v.p);
     k_smooth_p<true><<<g, 256, 0, s>>>(n, A.rp, A.ci, A.v, agg.p, omega, nullptr, P.rp.p, P.ci.p, P.v.p);
     HAMLSS_LAUNCH_CHECK();
     if (nlong) {
