@@ -12,8 +12,10 @@ namespace hamlss {
 void dense_lu_inverse(Ctx& ctx, int n, double* M, double* Minv, int* piv);
 
 // Gram matrix G = Y^T Y ((c x c, row-major, device) of the c columns of Y (column j at
-// Y + j * ld, n entries each), c <= 33: block partial sums over row tiles in shared
-// memory, then one ordered reduction over the blocks (deterministic).  `part` holds
+// Y + j * ld, n entries each), c <= 33: for n <= 32768 one thread per entry summing in
+// row order (the reference's sequential dot product, bit for bit); above, block partial
+// sums over row tiles in shared memory, then one ordered reduction over the blocks
+// (deterministic).  `part` holds
 // sm_count * 4 * c * (c + 1) / 2 doubles.
 void gram_matrix(Ctx& ctx, int n, int c, const double* Y, long long ld, double* G, double* part);
 int gram_partials(Ctx& ctx, int c);

@@ -175,7 +175,16 @@ int stream_group(const Csr<T>& A) {
     if (avg <= 11.0) return 2;
     if (avg <= 22.0) return 4;
     if (avg <= 44.0) return 8;
+    if (avg <= 88.0) return 16;
+    if (avg <= 176.0) return 32;
     return 0;
+}
+
+// FP32 operators with rows longer than the bulk-copy kernel stages (or too few rows for
+// it) and at least 48 entries a row on average: a warp per row (k_spmv_long).
+template <typename T>
+bool long_rows_warp(const Csr<T>& A) {
+    return sizeof(T) == 4 && A.n > 0 && (double)A.nnz / A.n >= 48.0;
 }
 
 // Max co-resident CTAs of a bulk-copy SpMV instantiation (its dynamic shared memory
@@ -219,7 +228,26 @@ void launch_spmv(int sm_count, const Lane& L, const Csr<T>& A, const XOp& xop, c
             if constexpr (sizeof(T) == 4)
                 return launch_spmv_stream<T, NRED, XOp, Epi, Fin, 8>(sm_count, L, A, xop, epi, fin, gate);
             break;
+        case 16:
+            if constexpr (sizeof(T) == 4)
+                return launch_spmv_stream<T, NRED, XOp, Epi, Fin, 16>(sm_count, L, A, xop, epi, fin, gate);
+            break;
+        case 32:
+            if constexpr (sizeof(T) == 4)
+                return launch_spmv_stream<T, NRED, XOp, Epi, Fin, 32>(sm_count, L, A, xop, epi, fin, gate);
+            break;
         default: break;
+    }
+    if constexpr (sizeof(T) == 4) {
+        if (long_rows_warp(A)) {
+            auto kl = k_spmv_long<T, NRED, XOp, Epi, Fin, 32>;
+            static const int per_sm_l = std::min(occupancy_blocks(kl, 256), kMaxBlocksPerSm);
+            const int blocks = std::max(1, std::min(ceil_div(A.n, 8), sm_count * per_sm_l));
+            if (NRED > 0) L.red_check(blocks, NRED);
+            kl<<<blocks, 256, 0, L.stream>>>(A.n, A.rp, A.ci, A.v, xop, epi, L.red(), fin, gate);
+            HAMLSS_LAUNCH_CHECK();
+            return;
+        }
     }
     auto kern = k_spmv<T, NRED, XOp, Epi, Fin>;
     // thread-safe one-time initialisation (contexts may be driven from several threads)

@@ -126,6 +126,56 @@ k_spmv(int n, const int* __restrict__ rp, const int* __restrict__ ci, const T* _
     }
 }
 
+// FP32 operators with long rows (the dense-ish coarse AMG levels, hundreds of entries a
+// row): G lanes per row (G = 32: a warp), each lane keeping four entries' loads in flight
+// (entries k, k + G, k + 2G, k + 3G) into four partial sums, combined by shuffles.  No
+// bit-exactness requirement applies to FP32 operands, so the order is free.
+template <typename T, int NRED, typename XOp, typename Epi, typename Fin, int G>
+__global__ void __launch_bounds__(256)
+k_spmv_long(int n, const int* __restrict__ rp, const int* __restrict__ ci, const T* __restrict__ v,
+            XOp xop, Epi epi, Reducer red, Fin fin, const int* gate) {
+    __shared__ double rsh[8 * (NRED > 0 ? NRED : 1)];
+    if (gate && *(volatile const int*)gate) return;
+    XOp xop_l = xop;
+    Epi epi_l = epi;
+    xop_l.load();
+    epi_l.load();
+    const int lane = threadIdx.x & 31, sub = lane / G, gl = lane - sub * G;
+    constexpr int kRows = 32 / G;                  // rows per warp
+    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    double acc[NRED > 0 ? NRED : 1];
+#pragma unroll
+    for (int k = 0; k < (NRED > 0 ? NRED : 1); ++k) acc[k] = 0.0;
+    for (int base = gw * kRows; base < n; base += nw * kRows) {
+        const int row = base + sub;
+        double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+        if (row < n) {
+            const int rs = __ldg(&rp[row]), re = __ldg(&rp[row + 1]);
+            int k = rs + gl;
+            for (; k + 3 * G < re; k += 4 * G) {
+                const T a0 = __ldg(&v[k]), a1 = __ldg(&v[k + G]), a2 = __ldg(&v[k + 2 * G]),
+                        a3 = __ldg(&v[k + 3 * G]);
+                const int c0 = __ldg(&ci[k]), c1 = __ldg(&ci[k + G]), c2 = __ldg(&ci[k + 2 * G]),
+                          c3 = __ldg(&ci[k + 3 * G]);
+                s0 += (double)a0 * xop_l(c0);
+                s1 += (double)a1 * xop_l(c1);
+                s2 += (double)a2 * xop_l(c2);
+                s3 += (double)a3 * xop_l(c3);
+            }
+            for (; k < re; k += G) s0 += (double)__ldg(&v[k]) * xop_l(__ldg(&ci[k]));
+        }
+        double sum = (s0 + s1) + (s2 + s3);
+#pragma unroll
+        for (int o = G >> 1; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+        if (row < n && gl == 0) epi_l(row, sum, acc);
+    }
+    if constexpr (NRED > 0) {
+        double tot[NRED];
+        if (grid_reduce<NRED>(red, acc, rsh, tot)) fin(tot);
+    }
+}
+
 // Elementwise kernel with the same reduction / finalize machinery (no matrix).
 template <int NRED, typename Body, typename Fin>
 __global__ void __launch_bounds__(256)

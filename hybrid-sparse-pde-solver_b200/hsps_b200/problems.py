@@ -130,6 +130,42 @@ def rhs(n_rows: int, seed: int, lo: float = 0.0, hi: float = 1.0) -> np.ndarray:
     return uniform(seed, n_rows, lo, hi, offset=1 << 40)
 
 
+def serving_specs(count: int, seed: int, n_lo: float = 1e3, n_hi: float = 4.2e6,
+                  rate: float = 0.0):
+    """The requests of serving_stream(...) as specs (kind, side, parameter, seed, arrival_s),
+    without building them: build_request(spec) makes (rp, ci, v, b, arrival_s, kind) when it
+    is needed, so long streams of large systems need not be held in memory at once."""
+    u = uniform(seed, 6 * count).reshape(count, 6)
+    t = 0.0
+    out = []
+    for k in range(count):
+        n = math.exp(math.log(n_lo) + u[k, 0] * (math.log(n_hi) - math.log(n_lo)))
+        side = max(8, int(round(math.sqrt(n))))
+        rseed = seed * 1_000_003 + k
+        if u[k, 1] < 0.5:
+            spec = ("varkappa", side, 1.5 * u[k, 2], rseed)
+        elif u[k, 1] < 0.85:
+            spec = ("convdiff", side, math.exp(u[k, 3] * math.log(1000.0)), rseed)
+        else:
+            spec = ("helmholtz", side, 0.1 + 9.9 * u[k, 4], rseed)
+        if rate > 0:
+            t += -math.log1p(-u[k, 5]) / rate
+        out.append(spec + (t,))
+    return out
+
+
+def build_request(spec):
+    """(rp, ci, v, b, arrival_s, kind) of a serving_specs entry."""
+    kind, side, par, rseed, t = spec
+    if kind == "varkappa":
+        A = varkappa_poisson_2d(side, par, rseed)
+    elif kind == "convdiff":
+        A = convection_diffusion_2d(side, 1.0, *convdiff_wind(side, par))
+    else:
+        A = helmholtz_2d(side, par)
+    return (*A, rhs(side * side, rseed), t, kind)
+
+
 def serving_stream(count: int, seed: int, n_lo: float = 1e3, n_hi: float = 4.2e6,
                    rate: float = 0.0):
     """A serving workload: `count` requests (rp, ci, v, b, arrival_s, kind).
@@ -139,21 +175,4 @@ def serving_stream(count: int, seed: int, n_lo: float = 1e3, n_hi: float = 4.2e6
     convection-diffusion (cell Peclet log-uniform in [1, 1000]) and 15% shifted Helmholtz
     (c uniform in [0.1, 10]); rhs uniform [0, 1).  Arrivals form a Poisson process of
     `rate` requests/s (exponential gaps); rate 0 puts every arrival at t = 0."""
-    u = uniform(seed, 6 * count).reshape(count, 6)
-    t = 0.0
-    out = []
-    for k in range(count):
-        n = math.exp(math.log(n_lo) + u[k, 0] * (math.log(n_hi) - math.log(n_lo)))
-        side = max(8, int(round(math.sqrt(n))))
-        rseed = seed * 1_000_003 + k
-        if u[k, 1] < 0.5:
-            A, kind = varkappa_poisson_2d(side, 1.5 * u[k, 2], rseed), "varkappa"
-        elif u[k, 1] < 0.85:
-            pe = math.exp(u[k, 3] * math.log(1000.0))
-            A, kind = convection_diffusion_2d(side, 1.0, *convdiff_wind(side, pe)), "convdiff"
-        else:
-            A, kind = helmholtz_2d(side, 0.1 + 9.9 * u[k, 4]), "helmholtz"
-        if rate > 0:
-            t += -math.log1p(-u[k, 5]) / rate
-        out.append((*A, rhs(side * side, rseed), t, kind))
-    return out
+    return [build_request(sp) for sp in serving_specs(count, seed, n_lo, n_hi, rate)]
