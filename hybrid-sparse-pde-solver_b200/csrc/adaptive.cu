@@ -148,11 +148,14 @@ struct LzState {
 struct EpiLz {
     const double* q;
     double* Aq;
+    double* terms;     // set: store the terms for an in-order sum (k_lz_seq_sum)
     HAMLSS_NO_LOAD
     template <int NV>
     __device__ __forceinline__ void operator()(int i, double ax, double (&acc)[NV]) const {
         Aq[i] = ax;
-        acc[0] += q[i] * ax;
+        const double t = __dmul_rn(q[i], ax);
+        if (terms) terms[i] = t;
+        else acc[0] += t;
     }
 };
 
@@ -169,14 +172,30 @@ struct BodyLzUpd {
     const double* qp;
     const LzState* s;
     double a, b;
+    double* terms;
     __device__ __forceinline__ void load() { a = s->alpha[s->na - 1]; b = s->beta_prev; }
     template <int NV>
     __device__ __forceinline__ void operator()(int i, double (&acc)[NV]) const {
-        double t = Aq[i] - (a * q[i] + b * qp[i]);
+        const double t = __dsub_rn(Aq[i], __dadd_rn(__dmul_rn(a, q[i]), __dmul_rn(b, qp[i])));
         Aq[i] = t;
-        acc[0] += t * t;
+        const double tt = __dmul_rn(t, t);
+        if (terms) terms[i] = tt;
+        else acc[0] += tt;
     }
 };
+
+// Systems of at most kLzSeqRows rows: the stored terms added in row order by one thread
+// (the reference's sequential dot / norm), then the finaliser.
+constexpr int kLzSeqRows = 1 << 15;
+
+template <typename Fin>
+__global__ void k_lz_seq_sum(int n, const double* __restrict__ terms, Fin fin, const int* gate) {
+    if (threadIdx.x != 0 || blockIdx.x != 0 || *(volatile const int*)gate) return;
+    double acc = 0.0;
+    for (int i = 0; i < n; ++i) acc = __dadd_rn(acc, terms[i]);
+    const double t[1] = {acc};
+    fin(t);
+}
 
 struct FinBeta {
     LzState* s;
@@ -234,11 +253,29 @@ void lanczos_bounds(Ctx& ctx, hamlss_mat* A, int K, double* tmin_out, double* tm
     LzState* lz = reinterpret_cast<LzState*>(lzb.p);
     HAMLSS_CUDA(cudaMemsetAsync(lz, 0, sizeof(LzState), st));
     launch_vec<0>(ctx.sm_count, L, n, BodyInit{q, qp, 1.0 / std::sqrt((double)n)});
+    DBuf<double> term_buf;
+    double* terms = nullptr;
+    if (n <= kLzSeqRows) {
+        term_buf.ensure((size_t)std::max(n, 1));
+        terms = term_buf.p;
+    }
+    // with terms, the launches' own grid sums are unused (NoFin) and k_lz_seq_sum finishes
     for (int j = 0; j < K; ++j) {
-        launch_spmv<double, 1>(ctx.sm_count, L, A->A.f64(), XVec<double>{q}, EpiLz{q, Aq}, FinAlpha{lz},
-                               &lz->halt, "features_spmv", 24.0 * n);
-        launch_vec<1>(ctx.sm_count, L, n, BodyLzUpd{Aq, q, qp, lz, 0.0, 0.0}, FinBeta{lz}, &lz->halt,
-                      "features", 32.0 * n);
+        if (terms) {
+            launch_spmv<double, 1>(ctx.sm_count, L, A->A.f64(), XVec<double>{q}, EpiLz{q, Aq, terms}, NoFin{},
+                                   &lz->halt, "features_spmv", 24.0 * n);
+            k_lz_seq_sum<<<1, 32, 0, st>>>(n, terms, FinAlpha{lz}, &lz->halt);
+            HAMLSS_LAUNCH_CHECK();
+            launch_vec<1>(ctx.sm_count, L, n, BodyLzUpd{Aq, q, qp, lz, 0.0, 0.0, terms}, NoFin{}, &lz->halt,
+                          "features", 32.0 * n);
+            k_lz_seq_sum<<<1, 32, 0, st>>>(n, terms, FinBeta{lz}, &lz->halt);
+            HAMLSS_LAUNCH_CHECK();
+        } else {
+            launch_spmv<double, 1>(ctx.sm_count, L, A->A.f64(), XVec<double>{q}, EpiLz{q, Aq, nullptr},
+                                   FinAlpha{lz}, &lz->halt, "features_spmv", 24.0 * n);
+            launch_vec<1>(ctx.sm_count, L, n, BodyLzUpd{Aq, q, qp, lz, 0.0, 0.0, nullptr}, FinBeta{lz},
+                          &lz->halt, "features", 32.0 * n);
+        }
         launch_vec<0>(ctx.sm_count, L, n, BodyLzShift{q, qp, Aq, lz, 0.0}, NoFin{}, &lz->halt,
                       "features", 32.0 * n);
     }

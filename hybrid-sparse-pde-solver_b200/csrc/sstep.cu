@@ -41,11 +41,20 @@ struct SsState {
     double bb;                       // ||b||^2
 };
 
+// Every reduction below either accumulates into the launch's grid reduction or, when
+// `terms` is set (systems of at most kSeqRows rows), stores its per-row terms
+// (terms[i], terms[n + i]) for k_seq_sum to add in row order -- the reference's
+// single-thread summation, bit for bit: the s-step update amplifies last-bit differences.
 struct BodyBB {
     const double* b;
+    double* terms;
     HAMLSS_NO_LOAD
     template <int NV>
-    __device__ __forceinline__ void operator()(int i, double (&acc)[NV]) const { acc[0] += b[i] * b[i]; }
+    __device__ __forceinline__ void operator()(int i, double (&acc)[NV]) const {
+        const double t = __dmul_rn(b[i], b[i]);
+        if (terms) terms[i] = t;
+        else acc[0] += t;
+    }
 };
 
 struct FinBB {
@@ -60,12 +69,15 @@ struct EpiNewton {
     const double* prev;
     double* out;
     double mtheta;
+    double* terms;
     HAMLSS_NO_LOAD
     template <int NV>
     __device__ __forceinline__ void operator()(int i, double ax, double (&acc)[NV]) const {
         const double v = __dadd_rn(ax, __dmul_rn(mtheta, prev[i]));
         out[i] = v;
-        acc[0] += v * v;
+        const double t = __dmul_rn(v, v);
+        if (terms) terms[i] = t;
+        else acc[0] += t;
     }
 };
 
@@ -110,12 +122,15 @@ struct BodyCopy {
 struct EpiResid {
     const double* b;
     double* r;
+    double* terms;
     HAMLSS_NO_LOAD
     template <int NV>
     __device__ __forceinline__ void operator()(int i, double ax, double (&acc)[NV]) const {
         const double ri = __dsub_rn(b[i], ax);
         r[i] = ri;
-        acc[0] += ri * ri;
+        const double t = __dmul_rn(ri, ri);
+        if (terms) terms[i] = t;
+        else acc[0] += t;
     }
 };
 
@@ -129,13 +144,21 @@ struct FinRR {
 struct EpiAp {
     const double* r;
     double* ap;
+    double* terms;
+    int n;
     HAMLSS_NO_LOAD
     template <int NV>
     __device__ __forceinline__ void operator()(int i, double ax, double (&acc)[NV]) const {
         ap[i] = ax;
         const double ri = r[i];
-        acc[0] += ri * ri;
-        acc[1] += ri * ax;
+        const double t0 = __dmul_rn(ri, ri), t1 = __dmul_rn(ri, ax);
+        if (terms) {
+            terms[i] = t0;
+            terms[n + i] = t1;
+        } else {
+            acc[0] += t0;
+            acc[1] += t1;
+        }
     }
 };
 
@@ -154,6 +177,7 @@ struct BodySteep {
     double* r;
     const double* ap;
     double alpha;
+    double* terms;
     HAMLSS_NO_LOAD
     template <int NV>
     __device__ __forceinline__ void operator()(int i, double (&acc)[NV]) const {
@@ -161,9 +185,31 @@ struct BodySteep {
         x[i] = __dadd_rn(x[i], __dmul_rn(alpha, ri));
         const double rn = __dadd_rn(ri, __dmul_rn(-alpha, ap[i]));
         r[i] = rn;
-        acc[0] += rn * rn;
+        const double t = __dmul_rn(rn, rn);
+        if (terms) terms[i] = t;
+        else acc[0] += t;
     }
 };
+
+// The stored terms of NV reductions added in row order by one thread each (separate
+// adds from 0.0), then handed to the reduction's finaliser.
+constexpr int kSeqRows = 1 << 15;
+
+template <int NV, typename Fin>
+__global__ void k_seq_sum(int n, const double* __restrict__ terms, Fin fin) {
+    __shared__ double tot[NV];
+    if (threadIdx.x < NV) {
+        double acc = 0.0;
+        for (int i = 0; i < n; ++i) acc = __dadd_rn(acc, terms[(size_t)threadIdx.x * n + i]);
+        tot[threadIdx.x] = acc;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t[NV];
+        for (int k = 0; k < NV; ++k) t[k] = tot[k];
+        fin(t);
+    }
+}
 
 struct Coeffs {
     double y[kMaxS];
@@ -274,9 +320,23 @@ SolveResult sstep_solve(Ctx& ctx, hamlss_mat* A, const double* b, double* x, con
     const long long spmv_b = ((long long)n + 1 + nz) * 4 + nz * 8 + (long long)n * 16;
     // r = b - A x, ||b|| (sstep_cg_solver.cpp:186-195)
     SsState h{};
-    launch_spmv<double, 1>(sm, L, A->A.f64(), XVec<double>{x}, EpiResid{b, r}, FinRR{s}, nullptr,
+    // small systems: every reduction in row order (k_seq_sum), as the reference sums
+    DBuf<double> term_buf;
+    double* terms = nullptr;
+    if (n <= kSeqRows) {
+        term_buf.ensure(2 * (size_t)std::max(n, 1));
+        terms = term_buf.p;
+    }
+    auto seq1 = [&](auto fin) {
+        if (!terms) return;
+        k_seq_sum<1><<<1, 32, 0, st>>>(n, terms, fin);
+        HAMLSS_LAUNCH_CHECK();
+    };
+    launch_spmv<double, 1>(sm, L, A->A.f64(), XVec<double>{x}, EpiResid{b, r, terms}, FinRR{s}, nullptr,
                            "sstep_residual", 24.0 * n);
-    launch_vec<1>(sm, L, n, BodyBB{b}, FinBB{s}, nullptr, "vec", 8.0 * n);
+    seq1(FinRR{s});
+    launch_vec<1>(sm, L, n, BodyBB{b, terms}, FinBB{s}, nullptr, "vec", 8.0 * n);
+    seq1(FinBB{s});
     poll(h);
     const double r0 = std::sqrt(h.rr);
     const double bnorm = std::sqrt(h.bb);
@@ -307,8 +367,9 @@ SolveResult sstep_solve(Ctx& ctx, hamlss_mat* A, const double* b, double* x, con
         else launch_vec<0>(sm, L, n, BodyCopy{r, Bcol(0)}, NoFin{}, nullptr, "vec", 16.0 * n);
         for (int j = 1; j < kb; ++j) {
             launch_spmv<double, 1>(sm, L, A->A.f64(), XVec<double>{Bcol(j - 1)},
-                                   EpiNewton{Bcol(j - 1), Bcol(j), -th[j - 1]}, FinNorm2{s}, nullptr,
+                                   EpiNewton{Bcol(j - 1), Bcol(j), -th[j - 1], terms}, FinNorm2{s}, nullptr,
                                    "sstep_basis", 24.0 * n);
+            seq1(FinNorm2{s});
             launch_vec<0>(sm, L, n, BodyScaleDev{Bcol(j), s, 0.0}, NoFin{}, nullptr, "vec", 16.0 * n);
         }
         // gram_matrix (:71-80) and rhs_ls[i] = r . B[i] (:228-230): one (kb+1)^2 Gram matrix
@@ -347,13 +408,18 @@ SolveResult sstep_solve(Ctx& ctx, hamlss_mat* A, const double* b, double* x, con
         std::vector<double> y;
         if (!cholesky_solve(Gk, kb, rhs, kb, y)) {
             // one steepest-descent step (sstep_cg_solver.cpp:236-250)
-            launch_spmv<double, 2>(sm, L, A->A.f64(), XVec<double>{r}, EpiAp{r, ap}, FinRrRap{s}, nullptr,
-                                   "sstep_fallback", 32.0 * n);
+            launch_spmv<double, 2>(sm, L, A->A.f64(), XVec<double>{r}, EpiAp{r, ap, terms, n}, FinRrRap{s},
+                                   nullptr, "sstep_fallback", 32.0 * n);
+            if (terms) {
+                k_seq_sum<2><<<1, 32, 0, st>>>(n, terms, FinRrRap{s});
+                HAMLSS_LAUNCH_CHECK();
+            }
             poll(h);
             double rn2 = h.rr;
             if (std::fabs(h.rap) > kEps) {
                 const double alpha = h.rr / h.rap;
-                launch_vec<1>(sm, L, n, BodySteep{x, r, ap, alpha}, FinRR{s}, nullptr, "vec", 40.0 * n);
+                launch_vec<1>(sm, L, n, BodySteep{x, r, ap, alpha, terms}, FinRR{s}, nullptr, "vec", 40.0 * n);
+                seq1(FinRR{s});
                 poll(h);
                 rn2 = h.rr;
             }
@@ -374,8 +440,9 @@ SolveResult sstep_solve(Ctx& ctx, hamlss_mat* A, const double* b, double* x, con
             HAMLSS_LAUNCH_CHECK();
         }
         // exact residual every batch (:255-264)
-        launch_spmv<double, 1>(sm, L, A->A.f64(), XVec<double>{x}, EpiResid{b, r}, FinRR{s}, nullptr,
+        launch_spmv<double, 1>(sm, L, A->A.f64(), XVec<double>{x}, EpiResid{b, r, terms}, FinRR{s}, nullptr,
                                "sstep_residual", 24.0 * n);
+        seq1(FinRR{s});
         flops += spmv_f;
         bytes += spmv_b;
         poll(h);
