@@ -477,6 +477,20 @@ __device__ __forceinline__ int pow2_at_least(int v) {
 
 // Rows [0, n) with kLongRow < len and len + 1 <= kSortMax, appended to `list`.
 // count[1] receives the longest listed row.
+// The same rows in three length buckets for the smoothed prolongation: len < 128 (sort of
+// <= 128 keys), < 512 and the rest; list + b * n holds bucket b, count[b] its size and
+// count[3 + b] its longest row.
+__global__ void k_long_rows3(int n, const int* __restrict__ rp, int* list, int* count) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int len = rp[i + 1] - rp[i];
+        if (smooth_row_on_block(len)) {
+            const int b = len < 128 ? 0 : len < 512 ? 1 : 2;
+            list[(size_t)b * n + atomicAdd(count + b, 1)] = i;
+            atomicMax(count + 3 + b, len);
+        }
+    }
+}
+
 __global__ void k_long_rows(int n, const int* __restrict__ rp, int* list, int* count) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const int len = rp[i + 1] - rp[i];
@@ -1717,6 +1731,16 @@ int warpwin_grid(Ctx& ctx, K kernel, size_t smem, int nrows) {
     return std::max(1, std::min(ceil_div(nrows, kWinWarps), ctx.sm_count * std::max(per, 1)));
 }
 
+// Grid of a block-per-row kernel launched with `threads` threads a block.
+template <typename K>
+int rows_grid(Ctx& ctx, K kernel, int threads, size_t smem, int nrows) {
+    static DeviceOnce raised;
+    raised(ctx.device, raise_row_kernel_limits);
+    int per = 0;
+    HAMLSS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, smem));
+    return std::max(1, std::min(nrows, ctx.sm_count * std::max(per, 1)));
+}
+
 template <typename K>
 int row_grid(Ctx& ctx, K kernel, size_t smem, int nrows) {
     static DeviceOnce raised;
@@ -1731,29 +1755,45 @@ void smooth_prolongation(Ctx& ctx, const Csr<double>& A, const DBuf<int>& agg, i
     const int n = A.n;
     cudaStream_t s = ctx.lane.stream;
     const int g = grid_for(ctx, n);
-    DBuf<int> cnt(n), list;
-    size_t smem = 0;                                // keys + values of the longest row
-    const int nlong = long_rows(ctx, n, A.rp, list, &smem);
+    DBuf<int> cnt(n), list(3LL * std::max(n, 1)), bk(6);
+    // rows longer than kLongRow by length bucket: a block of 64 / 128 / 256 threads a row
+    // (shorter rows sort fewer keys, so smaller blocks keep more rows in flight)
+    bk.zero(s);
+    if (n) k_long_rows3<<<g, 256, 0, s>>>(n, A.rp, list.p, bk.p);
+    HAMLSS_LAUNCH_CHECK();
+    int hb[6] = {0, 0, 0, 0, 0, 0};
+    bk.download(hb, 6, s);
+    HAMLSS_CUDA(cudaStreamSynchronize(s));
+    const int threads[3] = {64, 128, kRowBlock};
+    auto long_pass = [&](bool fill) {
+        for (int b = 0; b < 3; ++b) {
+            if (!hb[b]) continue;
+            int N = 1;
+            while (N < hb[3 + b] + 1) N <<= 1;
+            const size_t smem = 16 * (size_t)N;
+            const int* lst = list.p + (size_t)b * n;
+            if (fill) {
+                const int gb = rows_grid(ctx, k_smooth_p_rows<true>, threads[b], smem, hb[b]);
+                k_smooth_p_rows<true><<<gb, threads[b], smem, s>>>(lst, hb[b], A.rp, A.ci, A.v, agg.p, omega,
+                                                                   nullptr, P.rp.p, P.ci.p, P.v.p);
+            } else {
+                const int gb = rows_grid(ctx, k_smooth_p_rows<false>, threads[b], smem, hb[b]);
+                k_smooth_p_rows<false><<<gb, threads[b], smem, s>>>(lst, hb[b], A.rp, A.ci, A.v, agg.p, omega,
+                                                                    cnt.p, nullptr, nullptr, nullptr);
+            }
+            HAMLSS_LAUNCH_CHECK();
+        }
+    };
     const int gw = std::max(1, std::min(ceil_div(n, 8), ctx.sm_count * 8));      // 8 warps a block
     k_smooth_p_warp<false><<<gw, 256, 0, s>>>(n, A.rp, A.ci, A.v, agg.p, omega, cnt.p, nullptr, nullptr, nullptr);
     k_smooth_p<false><<<g, 256, 0, s>>>(n, A.rp, A.ci, A.v, agg.p, omega, cnt.p, nullptr, nullptr, nullptr);
     HAMLSS_LAUNCH_CHECK();
-    if (nlong) {
-        const int gb = row_grid(ctx, k_smooth_p_rows<false>, smem, nlong);
-        k_smooth_p_rows<false><<<gb, kRowBlock, smem, s>>>(list.p, nlong, A.rp, A.ci, A.v, agg.p, omega,
-                                                           cnt.p, nullptr, nullptr, nullptr);
-        HAMLSS_LAUNCH_CHECK();
-    }
+    long_pass(false);
     build_csr_counts(ctx, P, n, nc, cnt);
     k_smooth_p_warp<true><<<gw, 256, 0, s>>>(n, A.rp, A.ci, A.v, agg.p, omega, nullptr, P.rp.p, P.ci.p, P.v.p);
     k_smooth_p<true><<<g, 256, 0, s>>>(n, A.rp, A.ci, A.v, agg.p, omega, nullptr, P.rp.p, P.ci.p, P.v.p);
     HAMLSS_LAUNCH_CHECK();
-    if (nlong) {
-        const int gb = row_grid(ctx, k_smooth_p_rows<true>, smem, nlong);
-        k_smooth_p_rows<true><<<gb, kRowBlock, smem, s>>>(list.p, nlong, A.rp, A.ci, A.v, agg.p, omega,
-                                                          nullptr, P.rp.p, P.ci.p, P.v.p);
-        HAMLSS_LAUNCH_CHECK();
-    }
+    long_pass(true);
 }
 
 void transpose(Ctx& ctx, const DCsr& P, DCsr& R) {

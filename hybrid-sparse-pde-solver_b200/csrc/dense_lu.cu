@@ -330,26 +330,35 @@ __global__ void k_perm_identity(int n, const int* __restrict__ piv, double* X) {
 // ------------------------------------------------------------------------ DGEMM
 // C (m x p, ldc) = alpha * A (m x k, lda) * B (k x p, ldb) + beta * C, all row-major FP64,
 // on the FP64 tensor cores (mma.sync m8n8k4 .f64 -- the FP64 matrix path of sm_100a;
-// tcgen05 has no FP64 kind).  A CTA computes a 128 x 64 tile with 8 warps of 32 x 32
-// (4 x 4 MMA tiles each); K advances in steps of 16 staged in shared memory, the next
-// step's tile loaded into registers while the current one is multiplied.  Row strides
-// of the staged tiles (20 and 68 doubles) keep each half-warp's fragment loads on distinct
-// banks.  Edges are zero-filled, so any m, p, k works.
-constexpr int kGBM = 128, kGBN = 64, kGBK = 16, kGThreads = 256;
-constexpr int kGAS = kGBK + 4;       // A tile row stride (doubles)
-constexpr int kGBS = kGBN + 4;       // B tile row stride
+// tcgen05 has no FP64 kind).  Every GEMM of the blocked LU has k <= 64 (the block width),
+// so a CTA stages a whole 128 x 64 slice of A and 64 x 64 slice of B in shared memory with
+// one round of cp.async copies (edges zero-filled), then runs all 16 k-steps without a
+// barrier: 8 warps of 32 x 32 (4 x 4 MMA tiles each); C is read (beta != 0) and written
+// once, in the epilogue.  Larger k is taken in chunks of 64.  Row strides of the staged slices
+// (68 doubles) keep each half-warp's fragment loads on distinct banks.
+constexpr int kGBM = 128, kGBN = 64, kGBK = 64, kGThreads = 256;
+constexpr int kGAS = kGBK + 4;       // A slice row stride (doubles)
+constexpr int kGBS = kGBN + 4;       // B slice row stride
+constexpr size_t kGemmSmem = sizeof(double) * ((size_t)kGBM * kGAS + (size_t)kGBK * kGBS);
 
 __device__ __forceinline__ void dmma_8x8x4(double (&d)[2], double a, double b) {
     asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
                  : "+d"(d[0]), "+d"(d[1]) : "d"(a), "d"(b));
 }
 
+// 8-byte asynchronous copy global -> shared; src_bytes 0 fills the slot with zeros.
+__device__ __forceinline__ void cp_async8(double* dst, const double* src, int src_bytes) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;"
+                 ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src), "r"(src_bytes) : "memory");
+}
+
 __global__ void __launch_bounds__(kGThreads) k_dgemm(int m, int p, int k, double alpha,
                                                      const double* __restrict__ A, int lda,
                                                      const double* __restrict__ B, int ldb, double beta,
                                                      double* __restrict__ C, int ldc) {
-    __shared__ double As[kGBM * kGAS];
-    __shared__ double Bs[kGBK * kGBS];
+    extern __shared__ double gsm[];
+    double* As = gsm;
+    double* Bs = gsm + kGBM * kGAS;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int wm = warp >> 1, wn = warp & 1;                 // 4 x 2 warps of 32 x 32
     const int bm = blockIdx.y * kGBM, bn = blockIdx.x * kGBN;
@@ -359,42 +368,22 @@ __global__ void __launch_bounds__(kGThreads) k_dgemm(int m, int p, int k, double
     for (int i = 0; i < 4; ++i)
 #pragma unroll
         for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
-    double ra[(kGBM * kGBK) / kGThreads], rb[(kGBK * kGBN) / kGThreads];
-    auto load = [&](int k0) {
-#pragma unroll
-        for (int q = 0; q < (kGBM * kGBK) / kGThreads; ++q) {
-            const int e = tid + kGThreads * q, r = e / kGBK, c = e % kGBK;
-            const int gr = bm + r, gc = k0 + c;
-            ra[q] = (gr < m && gc < k) ? A[(size_t)gr * lda + gc] : 0.0;
+    for (int k0 = 0; k0 < k; k0 += kGBK) {
+        if (k0 > 0) __syncthreads();                         // the previous chunk is consumed
+        for (int e = tid; e < kGBM * kGBK; e += kGThreads) {
+            const int r = e / kGBK, c = e % kGBK, gr = bm + r, gc = k0 + c;
+            const bool in = gr < m && gc < k;
+            cp_async8(As + r * kGAS + c, in ? A + (size_t)gr * lda + gc : A, in ? 8 : 0);
         }
-#pragma unroll
-        for (int q = 0; q < (kGBK * kGBN) / kGThreads; ++q) {
-            const int e = tid + kGThreads * q, r = e / kGBN, c = e % kGBN;
-            const int gr = k0 + r, gc = bn + c;
-            rb[q] = (gr < k && gc < p) ? B[(size_t)gr * ldb + gc] : 0.0;
+        for (int e = tid; e < kGBK * kGBN; e += kGThreads) {
+            const int r = e / kGBN, c = e % kGBN, gr = k0 + r, gc = bn + c;
+            const bool in = gr < k && gc < p;
+            cp_async8(Bs + r * kGBS + c, in ? B + (size_t)gr * ldb + gc : B, in ? 8 : 0);
         }
-    };
-    auto store = [&]() {
-#pragma unroll
-        for (int q = 0; q < (kGBM * kGBK) / kGThreads; ++q) {
-            const int e = tid + kGThreads * q;
-            As[(e / kGBK) * kGAS + e % kGBK] = ra[q];
-        }
-#pragma unroll
-        for (int q = 0; q < (kGBK * kGBN) / kGThreads; ++q) {
-            const int e = tid + kGThreads * q;
-            Bs[(e / kGBN) * kGBS + e % kGBN] = rb[q];
-        }
-    };
-    const int nk = (k + kGBK - 1) / kGBK;
-    if (nk > 0) {
-        load(0);
-        store();
-    }
-    __syncthreads();
-    for (int kt = 0; kt < nk; ++kt) {
-        if (kt + 1 < nk) load((kt + 1) * kGBK);
-#pragma unroll
+        asm volatile("cp.async.commit_group;" ::: "memory");
+        asm volatile("cp.async.wait_group 0;" ::: "memory");
+        __syncthreads();
+#pragma unroll 4
         for (int ks = 0; ks < kGBK; ks += 4) {
             double af[4], bf[4];
 #pragma unroll
@@ -405,11 +394,6 @@ __global__ void __launch_bounds__(kGThreads) k_dgemm(int m, int p, int k, double
             for (int i = 0; i < 4; ++i)
 #pragma unroll
                 for (int j = 0; j < 4; ++j) dmma_8x8x4(acc[i][j], af[i], bf[j]);
-        }
-        __syncthreads();
-        if (kt + 1 < nk) {
-            store();
-            __syncthreads();
         }
     }
     // accumulator element h of tile (i, j): row fr, column 2 * fk + h of the 8 x 8 tile
@@ -431,8 +415,13 @@ __global__ void __launch_bounds__(kGThreads) k_dgemm(int m, int p, int k, double
 void dgemm(Ctx& ctx, int m, int p, int k, double alpha, const double* A, int lda, const double* B, int ldb,
            double beta, double* C, int ldc) {
     if (m <= 0 || p <= 0) return;
+    static DeviceOnce raised;
+    raised(ctx.device, [] {
+        HAMLSS_CUDA(cudaFuncSetAttribute(k_dgemm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmSmem));
+        return true;
+    });
     const dim3 grid(ceil_div(p, kGBN), ceil_div(m, kGBM));
-    k_dgemm<<<grid, kGThreads, 0, ctx.lane.stream>>>(m, p, k, alpha, A, lda, B, ldb, beta, C, ldc);
+    k_dgemm<<<grid, kGThreads, kGemmSmem, ctx.lane.stream>>>(m, p, k, alpha, A, lda, B, ldb, beta, C, ldc);
     HAMLSS_LAUNCH_CHECK();
 }
 
