@@ -599,7 +599,7 @@ constexpr int kDenseCols = 16384;       // columns a shared dense accumulator ma
 constexpr int kWarpHeads = 2048;        // merge heads a warp keeps in shared memory
 constexpr int kWarpMergeK = 512;        // long rows with at most this many left entries merge
 constexpr int kMergeWarps = 4;          // warps (rows) per block of k_spgemm_warp
-constexpr int kWarpWinMax = 2048;       // columns of a warp's private window (class 5)
+constexpr int kWarpWinMax = 4096;       // columns of a warp's private window (class 5)
 constexpr int kWarpWinMinProducts = 64; // fewer products: the thread merge is cheaper
 constexpr int kWinWarps = 8;            // warps (rows) per block of k_spgemm_warpwin
 
@@ -960,10 +960,11 @@ __global__ void k_spgemm_window(const int* __restrict__ rows, int nrows, int W,
 // arithmetic and output order of k_spgemm_window without its block barriers.  The left
 // entries are taken one at a time (a __syncwarp between them, so each column sums in
 // left-row order from 0.0 with separate multiply and add); lane q of a group of 32 steps
-// holds step q's (a, B row bounds) for the warp, and each lane's first product of the next
-// step is loaded before the current step is added.  Rows finish by a ballot-compacted scan
-// of the window in column order (survivors |v| > eps^2), which also clears it.
-// Shared memory: kWinWarps * (W doubles + W flag bytes), W a multiple of 16.
+// holds step q's (a, B row bounds) for the warp, each lane's first product of the next
+// step is loaded before the current step is added, and long B rows are read four entries
+// a lane at a time.  Rows finish by a ballot-compacted scan of the window in column order
+// (survivors |v| > eps^2: an untouched column holds 0.0 and never survives, so no touched
+// flags are kept), which also clears it.  Shared memory: (blockDim.x / 32) * W doubles.
 template <bool FILL>
 __global__ void __launch_bounds__(32 * kWinWarps)
 k_spgemm_warpwin(const int* __restrict__ rows, int nrows, int W, const int* __restrict__ wlo,
@@ -972,16 +973,12 @@ k_spgemm_warpwin(const int* __restrict__ rows, int nrows, int W, const int* __re
                  const double* __restrict__ bv, int* ccnt, const int* __restrict__ crp, int* cci,
                  double* cv) {
     extern __shared__ double wwin[];
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, wpb = blockDim.x >> 5;
     double* acc = wwin + (size_t)wid * W;
-    unsigned char* hit = reinterpret_cast<unsigned char*>(wwin + (size_t)kWinWarps * W) + (size_t)wid * W;
-    for (int c = lane; c < W; c += 32) {
-        acc[c] = 0.0;
-        hit[c] = 0;
-    }
+    for (int c = lane; c < W; c += 32) acc[c] = 0.0;
     __syncwarp();
-    const int nw = gridDim.x * kWinWarps;
-    for (int r = blockIdx.x * kWinWarps + wid; r < nrows; r += nw) {
+    const int nw = gridDim.x * wpb;
+    for (int r = blockIdx.x * wpb + wid; r < nrows; r += nw) {
         const int i = rows[r];
         const int s = arp[i], k = arp[i + 1] - s;
         const int lo = wlo[i], span = wspan[i];
@@ -1010,14 +1007,19 @@ k_spgemm_warpwin(const int* __restrict__ rows, int nrows, int W, const int* __re
                 int nc = -1;
                 double nv = 0.0;
                 if (q + 1 < cnt && nb0 + lane < nb1) { nc = bci[nb0 + lane] - lo; nv = bv[nb0 + lane]; }
-                if (pc >= 0) {
-                    acc[pc] = __dadd_rn(acc[pc], __dmul_rn(a, pv));
-                    hit[pc] = 1;
+                if (pc >= 0) acc[pc] = __dadd_rn(acc[pc], __dmul_rn(a, pv));
+                int e = b0 + lane + 32;
+                for (; e + 96 < b1; e += 128) {
+                    const int c0 = bci[e] - lo, c1 = bci[e + 32] - lo, c2 = bci[e + 64] - lo, c3 = bci[e + 96] - lo;
+                    const double v0 = bv[e], v1 = bv[e + 32], v2 = bv[e + 64], v3 = bv[e + 96];
+                    acc[c0] = __dadd_rn(acc[c0], __dmul_rn(a, v0));
+                    acc[c1] = __dadd_rn(acc[c1], __dmul_rn(a, v1));
+                    acc[c2] = __dadd_rn(acc[c2], __dmul_rn(a, v2));
+                    acc[c3] = __dadd_rn(acc[c3], __dmul_rn(a, v3));
                 }
-                for (int e = b0 + lane + 32; e < b1; e += 32) {
+                for (; e < b1; e += 32) {
                     const int c = bci[e] - lo;
                     acc[c] = __dadd_rn(acc[c], __dmul_rn(a, bv[e]));
-                    hit[c] = 1;
                 }
                 __syncwarp();
                 pc = nc;
@@ -1028,7 +1030,7 @@ k_spgemm_warpwin(const int* __restrict__ rows, int nrows, int W, const int* __re
         const int o0 = o;
         for (int c0 = 0; c0 < span; c0 += 32) {
             const int c = c0 + lane;
-            const bool keep = c < span && hit[c] && fabs(acc[c]) > kEps * kEps;
+            const bool keep = c < span && fabs(acc[c]) > kEps * kEps;
             const unsigned m = __ballot_sync(0xffffffffu, keep);
             if (FILL && keep) {
                 const int pos = o + __popc(m & ((1u << lane) - 1u));
@@ -1036,10 +1038,7 @@ k_spgemm_warpwin(const int* __restrict__ rows, int nrows, int W, const int* __re
                 cv[pos] = acc[c];
             }
             o += __popc(m);
-            if (c < span) {
-                acc[c] = 0.0;
-                hit[c] = 0;
-            }
+            if (c < span) acc[c] = 0.0;
         }
         if (ccnt && lane == 0) ccnt[i] = o - o0;
         __syncwarp();
@@ -1683,7 +1682,7 @@ int long_rows(Ctx& ctx, int n, const int* rp, DBuf<int>& list, size_t* smem) {
 // dynamic shared-memory limit is raised once, to the largest any launch of it asks for
 // (kMaxRowSmem), and never lowered: contexts on other threads launch it concurrently.
 constexpr size_t kMaxRowSmem = 20 * (size_t)kSortMax;   // hash table of kSortMax slots
-static_assert(kMaxRowSmem >= 9 * (size_t)kWinWarps * kWarpWinMax &&
+static_assert(kMaxRowSmem >= 8 * (size_t)kWarpWinMax &&
                   kMaxRowSmem >= 9 * (size_t)kDenseCols + 16 + 16 * (size_t)kWinLeft &&
                   kMaxRowSmem >= 16 * (size_t)kSortMax &&
                   kMaxRowSmem >= 12 * (size_t)kWarpHeads * kMergeWarps,
@@ -1723,12 +1722,12 @@ int merge_grid(Ctx& ctx, K kernel, size_t smem, int nrows) {
 
 // Grid of k_spgemm_warpwin (kWinWarps rows per block).
 template <typename K>
-int warpwin_grid(Ctx& ctx, K kernel, size_t smem, int nrows) {
+int warpwin_grid(Ctx& ctx, K kernel, int warps, size_t smem, int nrows) {
     static DeviceOnce raised;
     raised(ctx.device, raise_row_kernel_limits);
     int per = 0;
-    HAMLSS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, 32 * kWinWarps, smem));
-    return std::max(1, std::min(ceil_div(nrows, kWinWarps), ctx.sm_count * std::max(per, 1)));
+    HAMLSS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, 32 * warps, smem));
+    return std::max(1, std::min(ceil_div(nrows, warps), ctx.sm_count * std::max(per, 1)));
 }
 
 // Grid of a block-per-row kernel launched with `threads` threads a block.
@@ -1840,7 +1839,9 @@ void spgemm(Ctx& ctx, const Csr<double>& A, const Csr<double>& B, DCsr& C) {
     const int nlong = hm[0], ndense = hm[2], nwarp = hm[3], nwin = hm[5], nwwin = hm[7];
     const int* wwlist = list.p + 4LL * A.n;
     const int WW = std::max(16, (hm[8] + 15) / 16 * 16);      // class-5 window, 16-aligned
-    const size_t wwsmem = (size_t)kWinWarps * WW * 9;
+    // warps a block: as many 8-byte windows as fit the row kernels' shared-memory limit
+    const int wwarps = std::max(1, std::min(kWinWarps, (int)(kMaxRowSmem / (8u * (unsigned)WW))));
+    const size_t wwsmem = (size_t)wwarps * WW * 8;
     const int* winlist = list.p + 3LL * A.n;
     const size_t winsmem = window_smem(hm[6]);   // window accumulator + hit flags + left row
     int KH = 32;
@@ -1899,8 +1900,8 @@ void spgemm(Ctx& ctx, const Csr<double>& A, const Csr<double>& B, DCsr& C) {
                 HAMLSS_LAUNCH_CHECK();
             }
             if (nwwin) {
-                const int gb = warpwin_grid(ctx, k_spgemm_warpwin<true>, wwsmem, nwwin);
-                k_spgemm_warpwin<true><<<gb, 32 * kWinWarps, wwsmem, s>>>(wwlist, nwwin, WW, wlo.p, wspan.p,
+                const int gb = warpwin_grid(ctx, k_spgemm_warpwin<true>, wwarps, wwsmem, nwwin);
+                k_spgemm_warpwin<true><<<gb, 32 * wwarps, wwsmem, s>>>(wwlist, nwwin, WW, wlo.p, wspan.p,
                                                                           A.rp, A.ci, A.v, B.rp, B.ci, B.v,
                                                                           cnt.p, off.p, wci.p, wv.p);
                 HAMLSS_LAUNCH_CHECK();
@@ -1942,8 +1943,8 @@ void spgemm(Ctx& ctx, const Csr<double>& A, const Csr<double>& B, DCsr& C) {
         HAMLSS_LAUNCH_CHECK();
     }
     if (nwwin) {
-        const int gb = warpwin_grid(ctx, k_spgemm_warpwin<false>, wwsmem, nwwin);
-        k_spgemm_warpwin<false><<<gb, 32 * kWinWarps, wwsmem, s>>>(wwlist, nwwin, WW, wlo.p, wspan.p, A.rp,
+        const int gb = warpwin_grid(ctx, k_spgemm_warpwin<false>, wwarps, wwsmem, nwwin);
+        k_spgemm_warpwin<false><<<gb, 32 * wwarps, wwsmem, s>>>(wwlist, nwwin, WW, wlo.p, wspan.p, A.rp,
                                                                    A.ci, A.v, B.rp, B.ci, B.v, cnt.p, nullptr,
                                                                    nullptr, nullptr);
         HAMLSS_LAUNCH_CHECK();
@@ -1978,8 +1979,8 @@ void spgemm(Ctx& ctx, const Csr<double>& A, const Csr<double>& B, DCsr& C) {
         HAMLSS_LAUNCH_CHECK();
     }
     if (nwwin) {
-        const int gb = warpwin_grid(ctx, k_spgemm_warpwin<true>, wwsmem, nwwin);
-        k_spgemm_warpwin<true><<<gb, 32 * kWinWarps, wwsmem, s>>>(wwlist, nwwin, WW, wlo.p, wspan.p, A.rp,
+        const int gb = warpwin_grid(ctx, k_spgemm_warpwin<true>, wwarps, wwsmem, nwwin);
+        k_spgemm_warpwin<true><<<gb, 32 * wwarps, wwsmem, s>>>(wwlist, nwwin, WW, wlo.p, wspan.p, A.rp,
                                                                   A.ci, A.v, B.rp, B.ci, B.v, nullptr, C.rp.p,
                                                                   C.ci.p, C.v.p);
         HAMLSS_LAUNCH_CHECK();
