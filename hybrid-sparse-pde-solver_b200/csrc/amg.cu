@@ -588,20 +588,15 @@ __global__ void k_smooth_p_rows(const int* __restrict__ rows, int nrows, const i
 // SpGEMM row classes: 0 thread-per-row merge (short rows, or rows too long for the rest),
 // 1 block-per-row hash accumulation, 2 block-per-row dense accumulation (the right operand
 // has at most kDenseCols columns), 3 warp-per-row merge (left rows of kHeads+1 to
-// kWarpHeads entries), 4 block-per-row dense accumulation over the row's column window,
-// 5 warp-per-row dense accumulation over a window of at most kWarpWinMax columns (rows of
-// at least kWarpWinMinProducts products).  count[0] / list: class-1 rows, count[1] the
-// widest class-1 table, count[2] / list + m: class-2 rows, count[3] / list + 2m: class-3
-// rows, count[4] their longest left row, count[5] / list + 3m: class-4 rows, count[6] their
-// widest window, count[7] / list + 4m: class-5 rows, count[8] their widest window.
+// kWarpHeads entries), 4 block-per-row dense accumulation over the row's column window.
+// count[0] / list: class-1 rows, count[1] the widest class-1 table, count[2] / list + m:
+// class-2 rows, count[3] / list + 2m: class-3 rows, count[4] their longest left row,
+// count[5] / list + 3m: class-4 rows, count[6] their widest window.
 constexpr int kHashMax = 4096;          // distinct output columns a shared table may hold
 constexpr int kDenseCols = 16384;       // columns a shared dense accumulator may hold
 constexpr int kWarpHeads = 2048;        // merge heads a warp keeps in shared memory
 constexpr int kWarpMergeK = 512;        // long rows with at most this many left entries merge
 constexpr int kMergeWarps = 4;          // warps (rows) per block of k_spgemm_warp
-constexpr int kWarpWinMax = 4096;       // columns of a warp's private window (class 5)
-constexpr int kWarpWinMinProducts = 64; // fewer products: the thread merge is cheaper
-constexpr int kWinWarps = 8;            // warps (rows) per block of k_spgemm_warpwin
 
 __global__ void k_spgemm_classify(int m, const int* __restrict__ arp, const int* __restrict__ aci,
                                   const int* __restrict__ brp, const int* __restrict__ bci, int bcols,
@@ -627,8 +622,7 @@ __global__ void k_spgemm_classify(int m, const int* __restrict__ arp, const int*
         // also scans only that window.  The warp merge pays per output column
         const bool dense_ok = bcols <= kDenseCols && h > kHashMax / 4;
         int c = 0;
-        if (span <= kWarpWinMax && u >= kWarpWinMinProducts) c = 5;
-        else if (lng && span <= kDenseCols && u >= 32LL * k && h > kHashMax / 4) c = 4;
+        if (lng && span <= kDenseCols && u >= 32LL * k && h > kHashMax / 4) c = 4;
         else if (lng && k <= kWarpMergeK) c = 3;
         else if (lng && dense_ok) c = 2;
         else if (lng && h <= kHashMax) c = 1;
@@ -645,11 +639,6 @@ __global__ void k_spgemm_classify(int m, const int* __restrict__ arp, const int*
         } else if (c == 4) {
             list[3LL * m + atomicAdd(count + 5, 1)] = i;
             atomicMax(count + 6, (int)span);
-            wlo[i] = lo;
-            wspan[i] = (int)span;
-        } else if (c == 5) {
-            list[4LL * m + atomicAdd(count + 7, 1)] = i;
-            atomicMax(count + 8, (int)span);
             wlo[i] = lo;
             wspan[i] = (int)span;
         }
@@ -952,96 +941,6 @@ __global__ void k_spgemm_window(const int* __restrict__ rows, int nrows, int W,
             hit[c] = 0;
         }
         __syncthreads();
-    }
-}
-
-// Row i of C = A B for the listed rows, one warp per row, each warp with a private dense
-// accumulator over the row's column window [lo_i, lo_i + span_i), span_i <= W: the
-// arithmetic and output order of k_spgemm_window without its block barriers.  The left
-// entries are taken one at a time (a __syncwarp between them, so each column sums in
-// left-row order from 0.0 with separate multiply and add); lane q of a group of 32 steps
-// holds step q's (a, B row bounds) for the warp, each lane's first product of the next
-// step is loaded before the current step is added, and long B rows are read four entries
-// a lane at a time.  Rows finish by a ballot-compacted scan of the window in column order
-// (survivors |v| > eps^2: an untouched column holds 0.0 and never survives, so no touched
-// flags are kept), which also clears it.  Shared memory: (blockDim.x / 32) * W doubles.
-template <bool FILL>
-__global__ void __launch_bounds__(32 * kWinWarps)
-k_spgemm_warpwin(const int* __restrict__ rows, int nrows, int W, const int* __restrict__ wlo,
-                 const int* __restrict__ wspan, const int* __restrict__ arp, const int* __restrict__ aci,
-                 const double* __restrict__ av, const int* __restrict__ brp, const int* __restrict__ bci,
-                 const double* __restrict__ bv, int* ccnt, const int* __restrict__ crp, int* cci,
-                 double* cv) {
-    extern __shared__ double wwin[];
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, wpb = blockDim.x >> 5;
-    double* acc = wwin + (size_t)wid * W;
-    for (int c = lane; c < W; c += 32) acc[c] = 0.0;
-    __syncwarp();
-    const int nw = gridDim.x * wpb;
-    for (int r = blockIdx.x * wpb + wid; r < nrows; r += nw) {
-        const int i = rows[r];
-        const int s = arp[i], k = arp[i + 1] - s;
-        const int lo = wlo[i], span = wspan[i];
-        for (int t0 = 0; t0 < k; t0 += 32) {
-            const int cnt = min(32, k - t0);
-            double aq = 0.0;
-            int b0q = 0, b1q = 0;
-            if (lane < cnt) {
-                const int j = aci[s + t0 + lane];
-                aq = av[s + t0 + lane];
-                b0q = brp[j];
-                b1q = brp[j + 1];
-            }
-            // this lane's first product of step 0 of the group
-            int pc = -1;
-            double pv = 0.0;
-            {
-                const int b0 = __shfl_sync(0xffffffffu, b0q, 0), b1 = __shfl_sync(0xffffffffu, b1q, 0);
-                if (b0 + lane < b1) { pc = bci[b0 + lane] - lo; pv = bv[b0 + lane]; }
-            }
-            for (int q = 0; q < cnt; ++q) {
-                const double a = __shfl_sync(0xffffffffu, aq, q);
-                const int b0 = __shfl_sync(0xffffffffu, b0q, q), b1 = __shfl_sync(0xffffffffu, b1q, q);
-                const int qn = min(q + 1, 31);
-                const int nb0 = __shfl_sync(0xffffffffu, b0q, qn), nb1 = __shfl_sync(0xffffffffu, b1q, qn);
-                int nc = -1;
-                double nv = 0.0;
-                if (q + 1 < cnt && nb0 + lane < nb1) { nc = bci[nb0 + lane] - lo; nv = bv[nb0 + lane]; }
-                if (pc >= 0) acc[pc] = __dadd_rn(acc[pc], __dmul_rn(a, pv));
-                int e = b0 + lane + 32;
-                for (; e + 96 < b1; e += 128) {
-                    const int c0 = bci[e] - lo, c1 = bci[e + 32] - lo, c2 = bci[e + 64] - lo, c3 = bci[e + 96] - lo;
-                    const double v0 = bv[e], v1 = bv[e + 32], v2 = bv[e + 64], v3 = bv[e + 96];
-                    acc[c0] = __dadd_rn(acc[c0], __dmul_rn(a, v0));
-                    acc[c1] = __dadd_rn(acc[c1], __dmul_rn(a, v1));
-                    acc[c2] = __dadd_rn(acc[c2], __dmul_rn(a, v2));
-                    acc[c3] = __dadd_rn(acc[c3], __dmul_rn(a, v3));
-                }
-                for (; e < b1; e += 32) {
-                    const int c = bci[e] - lo;
-                    acc[c] = __dadd_rn(acc[c], __dmul_rn(a, bv[e]));
-                }
-                __syncwarp();
-                pc = nc;
-                pv = nv;
-            }
-        }
-        int o = (FILL && crp) ? crp[i] : 0;
-        const int o0 = o;
-        for (int c0 = 0; c0 < span; c0 += 32) {
-            const int c = c0 + lane;
-            const bool keep = c < span && fabs(acc[c]) > kEps * kEps;
-            const unsigned m = __ballot_sync(0xffffffffu, keep);
-            if (FILL && keep) {
-                const int pos = o + __popc(m & ((1u << lane) - 1u));
-                cci[pos] = lo + c;
-                cv[pos] = acc[c];
-            }
-            o += __popc(m);
-            if (c < span) acc[c] = 0.0;
-        }
-        if (ccnt && lane == 0) ccnt[i] = o - o0;
-        __syncwarp();
     }
 }
 
@@ -1682,8 +1581,7 @@ int long_rows(Ctx& ctx, int n, const int* rp, DBuf<int>& list, size_t* smem) {
 // dynamic shared-memory limit is raised once, to the largest any launch of it asks for
 // (kMaxRowSmem), and never lowered: contexts on other threads launch it concurrently.
 constexpr size_t kMaxRowSmem = 20 * (size_t)kSortMax;   // hash table of kSortMax slots
-static_assert(kMaxRowSmem >= 8 * (size_t)kWarpWinMax &&
-                  kMaxRowSmem >= 9 * (size_t)kDenseCols + 16 + 16 * (size_t)kWinLeft &&
+static_assert(kMaxRowSmem >= 9 * (size_t)kDenseCols + 16 + 16 * (size_t)kWinLeft &&
                   kMaxRowSmem >= 16 * (size_t)kSortMax &&
                   kMaxRowSmem >= 12 * (size_t)kWarpHeads * kMergeWarps,
               "row kernels' shared memory");
@@ -1705,8 +1603,6 @@ bool raise_row_kernel_limits() {
     raise_smem_limit(k_spgemm_warp<true>);
     raise_smem_limit(k_spgemm_window<false>);
     raise_smem_limit(k_spgemm_window<true>);
-    raise_smem_limit(k_spgemm_warpwin<false>);
-    raise_smem_limit(k_spgemm_warpwin<true>);
     return true;
 }
 
@@ -1718,16 +1614,6 @@ int merge_grid(Ctx& ctx, K kernel, size_t smem, int nrows) {
     int per = 0;
     HAMLSS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, 32 * kMergeWarps, smem));
     return std::max(1, std::min(ceil_div(nrows, kMergeWarps), ctx.sm_count * std::max(per, 1)));
-}
-
-// Grid of k_spgemm_warpwin (kWinWarps rows per block).
-template <typename K>
-int warpwin_grid(Ctx& ctx, K kernel, int warps, size_t smem, int nrows) {
-    static DeviceOnce raised;
-    raised(ctx.device, raise_row_kernel_limits);
-    int per = 0;
-    HAMLSS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, 32 * warps, smem));
-    return std::max(1, std::min(ceil_div(nrows, warps), ctx.sm_count * std::max(per, 1)));
 }
 
 // Grid of a block-per-row kernel launched with `threads` threads a block.
@@ -1826,22 +1712,17 @@ void spgemm(Ctx& ctx, const Csr<double>& A, const Csr<double>& B, DCsr& C) {
     cudaStream_t s = ctx.lane.stream;
     const int g = grid_for(ctx, A.n);
     DBuf<int> heads(3LL * std::max(A.nnz, 1));
-    DBuf<int> cnt(std::max(A.n, 1)), cls(std::max(A.n, 1)), list(5LL * std::max(A.n, 1)), meta(9);
+    DBuf<int> cnt(std::max(A.n, 1)), cls(std::max(A.n, 1)), list(4LL * std::max(A.n, 1)), meta(7);
     DBuf<int> wlo(std::max(A.n, 1)), wspan(std::max(A.n, 1));
     meta.zero(s);
     if (A.n)
         k_spgemm_classify<<<g, 256, 0, s>>>(A.n, A.rp, A.ci, B.rp, B.ci, B.m, cls.p, list.p, meta.p, wlo.p,
                                             wspan.p);
     HAMLSS_LAUNCH_CHECK();
-    int hm[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-    meta.download(hm, 9, s);
+    int hm[7] = {0, 0, 0, 0, 0, 0, 0};
+    meta.download(hm, 7, s);
     HAMLSS_CUDA(cudaStreamSynchronize(s));
-    const int nlong = hm[0], ndense = hm[2], nwarp = hm[3], nwin = hm[5], nwwin = hm[7];
-    const int* wwlist = list.p + 4LL * A.n;
-    const int WW = std::max(16, (hm[8] + 15) / 16 * 16);      // class-5 window, 16-aligned
-    // warps a block: as many 8-byte windows as fit the row kernels' shared-memory limit
-    const int wwarps = std::max(1, std::min(kWinWarps, (int)(kMaxRowSmem / (8u * (unsigned)WW))));
-    const size_t wwsmem = (size_t)wwarps * WW * 8;
+    const int nlong = hm[0], ndense = hm[2], nwarp = hm[3], nwin = hm[5];
     const int* winlist = list.p + 3LL * A.n;
     const size_t winsmem = window_smem(hm[6]);   // window accumulator + hit flags + left row
     int KH = 32;
@@ -1899,13 +1780,6 @@ void spgemm(Ctx& ctx, const Csr<double>& A, const Csr<double>& B, DCsr& C) {
                                                                      cnt.p, off.p, wci.p, wv.p);
                 HAMLSS_LAUNCH_CHECK();
             }
-            if (nwwin) {
-                const int gb = warpwin_grid(ctx, k_spgemm_warpwin<true>, wwarps, wwsmem, nwwin);
-                k_spgemm_warpwin<true><<<gb, 32 * wwarps, wwsmem, s>>>(wwlist, nwwin, WW, wlo.p, wspan.p,
-                                                                          A.rp, A.ci, A.v, B.rp, B.ci, B.v,
-                                                                          cnt.p, off.p, wci.p, wv.p);
-                HAMLSS_LAUNCH_CHECK();
-            }
             build_csr_counts(ctx, C, A.n, B.m, cnt);
             if (A.n)
                 k_spgemm_compact<<<std::max(1, std::min(ceil_div(A.n, 8), ctx.sm_count * 16)), 256, 0, s>>>(
@@ -1942,13 +1816,6 @@ void spgemm(Ctx& ctx, const Csr<double>& A, const Csr<double>& B, DCsr& C) {
                                                               nullptr);
         HAMLSS_LAUNCH_CHECK();
     }
-    if (nwwin) {
-        const int gb = warpwin_grid(ctx, k_spgemm_warpwin<false>, wwarps, wwsmem, nwwin);
-        k_spgemm_warpwin<false><<<gb, 32 * wwarps, wwsmem, s>>>(wwlist, nwwin, WW, wlo.p, wspan.p, A.rp,
-                                                                   A.ci, A.v, B.rp, B.ci, B.v, cnt.p, nullptr,
-                                                                   nullptr, nullptr);
-        HAMLSS_LAUNCH_CHECK();
-    }
     build_csr_counts(ctx, C, A.n, B.m, cnt);
     k_spgemm<true><<<g, 256, 0, s>>>(A.n, A.rp, A.ci, A.v, B.rp, B.ci, B.v, nullptr, C.rp.p, C.ci.p,
                                      C.v.p, heads.p, cls.p);
@@ -1976,13 +1843,6 @@ void spgemm(Ctx& ctx, const Csr<double>& A, const Csr<double>& B, DCsr& C) {
         k_spgemm_window<true><<<gb, kRowBlock, winsmem, s>>>(winlist, nwin, hm[6], wlo.p, wspan.p, A.rp, A.ci,
                                                              A.v, B.rp, B.ci, B.v, nullptr, C.rp.p, C.ci.p,
                                                              C.v.p);
-        HAMLSS_LAUNCH_CHECK();
-    }
-    if (nwwin) {
-        const int gb = warpwin_grid(ctx, k_spgemm_warpwin<true>, wwarps, wwsmem, nwwin);
-        k_spgemm_warpwin<true><<<gb, 32 * wwarps, wwsmem, s>>>(wwlist, nwwin, WW, wlo.p, wspan.p, A.rp,
-                                                                  A.ci, A.v, B.rp, B.ci, B.v, nullptr, C.rp.p,
-                                                                  C.ci.p, C.v.p);
         HAMLSS_LAUNCH_CHECK();
     }
 }

@@ -384,7 +384,9 @@ SolveResult cg_impl(Ctx& ctx, hamlss_mat* A, Prec* M, const T* b, T* x, double t
         else if (h.iter > 0 && h.rel > 0.0 && h.r0 > 0.0 && h.bnorm > 0.0 && h.r0 / h.bnorm > h.rel)
             rate = std::log(h.rel / (h.r0 / h.bnorm)) / h.iter;
         if (rate < 0.0 && h.rel > tol) {
-            const double need = std::ceil(std::log(tol / h.rel) / rate);
+            // with a preconditioner a trip is costly next to a poll: aim a little short and
+            // let the next poll take the last trips (fewer trips issued past the stop)
+            const double need = std::ceil(std::log(tol / h.rel) / rate * (JAC ? 1.0 : 0.75));
             if (need < grow) grow = std::max(1, (int)need);
         }
         chunk = std::max(1, std::min(grow, max_iter - h.iter));
@@ -666,7 +668,9 @@ SolveResult cg_reliable_impl(Ctx& ctx, hamlss_mat* A, Prec* M, const double* b, 
         else if (h.iter > 0 && h.rel > 0.0 && h.r0 > 0.0 && h.bnorm > 0.0 && h.r0 / h.bnorm > h.rel)
             rate = std::log(h.rel / (h.r0 / h.bnorm)) / h.iter;
         if (rate < 0.0 && h.rel > tol) {
-            const double need = std::ceil(std::log(tol / h.rel) / rate);
+            // with a preconditioner a trip is costly next to a poll: aim a little short and
+            // let the next poll take the last trips (fewer trips issued past the stop)
+            const double need = std::ceil(std::log(tol / h.rel) / rate * (JAC ? 1.0 : 0.75));
             if (need < grow) grow = std::max(1, (int)need);
         }
         chunk = std::max(1, std::min(grow, max_iter - h.iter));

@@ -206,9 +206,9 @@ k_spmv_stream(int n, const int* __restrict__ rp, const int* __restrict__ ci, con
             const int re = landed ? srp[sub + 1] : __ldg(&rp[row + 1]);
             const int* sci = stage_ci<T>(smem, s);
             const T* sv = stage_v<T>(smem, s);
-            for (int k = rs + gl; k < re; k += G) {
-                T a;
-                int c;
+            // four entries at a time: their x gathers are issued together, then added in
+            // order (the row's summation order is unchanged)
+            auto entry = [&](int k, T& a, int& c) {
                 if (k < lim) {
                     a = sv[k - base];
                     c = sci[k - base];
@@ -216,6 +216,25 @@ k_spmv_stream(int n, const int* __restrict__ rp, const int* __restrict__ ci, con
                     a = __ldg(&v[k]);
                     c = __ldg(&ci[k]);
                 }
+            };
+            int k = rs + gl;
+            for (; k + 3 * G < re; k += 4 * G) {
+                T a0, a1, a2, a3;
+                int c0, c1, c2, c3;
+                entry(k, a0, c0);
+                entry(k + G, a1, c1);
+                entry(k + 2 * G, a2, c2);
+                entry(k + 3 * G, a3, c3);
+                const double x0 = xop_l(c0), x1 = xop_l(c1), x2 = xop_l(c2), x3 = xop_l(c3);
+                sum = mul_add<T>(sum, a0, x0);
+                sum = mul_add<T>(sum, a1, x1);
+                sum = mul_add<T>(sum, a2, x2);
+                sum = mul_add<T>(sum, a3, x3);
+            }
+            for (; k < re; k += G) {
+                T a;
+                int c;
+                entry(k, a, c);
                 sum = mul_add<T>(sum, a, xop_l(c));
             }
         }
