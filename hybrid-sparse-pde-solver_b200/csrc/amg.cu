@@ -591,7 +591,8 @@ __global__ void k_smooth_p_rows(const int* __restrict__ rows, int nrows, const i
 // kWarpHeads entries), 4 block-per-row dense accumulation over the row's column window.
 // count[0] / list: class-1 rows, count[1] the widest class-1 table, count[2] / list + m:
 // class-2 rows, count[3] / list + 2m: class-3 rows, count[4] their longest left row,
-// count[5] / list + 3m: class-4 rows, count[6] their widest window.
+// count[5 + b] / list + (3 + b) m: class-4 rows of window bucket b (span <= 4096, <= 8192,
+// <= kDenseCols), count[8 + b] the bucket's widest window.
 constexpr int kHashMax = 4096;          // distinct output columns a shared table may hold
 constexpr int kDenseCols = 16384;       // columns a shared dense accumulator may hold
 constexpr int kWarpHeads = 2048;        // merge heads a warp keeps in shared memory
@@ -637,8 +638,10 @@ __global__ void k_spgemm_classify(int m, const int* __restrict__ arp, const int*
             list[2LL * m + atomicAdd(count + 3, 1)] = i;
             atomicMax(count + 4, k);
         } else if (c == 4) {
-            list[3LL * m + atomicAdd(count + 5, 1)] = i;
-            atomicMax(count + 6, (int)span);
+            // by window width, so narrow windows take less shared memory a block
+            const int b = span <= 4096 ? 0 : span <= 8192 ? 1 : 2;
+            list[(3LL + b) * m + atomicAdd(count + 5 + b, 1)] = i;
+            atomicMax(count + 8 + b, (int)span);
             wlo[i] = lo;
             wspan[i] = (int)span;
         }
@@ -1712,19 +1715,37 @@ void spgemm(Ctx& ctx, const Csr<double>& A, const Csr<double>& B, DCsr& C) {
     cudaStream_t s = ctx.lane.stream;
     const int g = grid_for(ctx, A.n);
     DBuf<int> heads(3LL * std::max(A.nnz, 1));
-    DBuf<int> cnt(std::max(A.n, 1)), cls(std::max(A.n, 1)), list(4LL * std::max(A.n, 1)), meta(7);
+    DBuf<int> cnt(std::max(A.n, 1)), cls(std::max(A.n, 1)), list(6LL * std::max(A.n, 1)), meta(11);
     DBuf<int> wlo(std::max(A.n, 1)), wspan(std::max(A.n, 1));
     meta.zero(s);
     if (A.n)
         k_spgemm_classify<<<g, 256, 0, s>>>(A.n, A.rp, A.ci, B.rp, B.ci, B.m, cls.p, list.p, meta.p, wlo.p,
                                             wspan.p);
     HAMLSS_LAUNCH_CHECK();
-    int hm[7] = {0, 0, 0, 0, 0, 0, 0};
-    meta.download(hm, 7, s);
+    int hm[11] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    meta.download(hm, 11, s);
     HAMLSS_CUDA(cudaStreamSynchronize(s));
-    const int nlong = hm[0], ndense = hm[2], nwarp = hm[3], nwin = hm[5];
-    const int* winlist = list.p + 3LL * A.n;
-    const size_t winsmem = window_smem(hm[6]);   // window accumulator + hit flags + left row
+    const int nlong = hm[0], ndense = hm[2], nwarp = hm[3];
+    // class-4 windows by width bucket: each launch sizes its shared memory to its widest row
+    auto windows = [&](bool fill, int* ccnt, const int* crp, int* cci, double* cv) {
+        for (int b = 0; b < 3; ++b) {
+            const int nw = hm[5 + b];
+            if (!nw) continue;
+            const int W = hm[8 + b];
+            const size_t wsm = window_smem(W);       // window accumulator + hit flags + left row
+            const int* wl = list.p + (3LL + b) * A.n;
+            if (fill) {
+                const int gb = row_grid(ctx, k_spgemm_window<true>, wsm, nw);
+                k_spgemm_window<true><<<gb, kRowBlock, wsm, s>>>(wl, nw, W, wlo.p, wspan.p, A.rp, A.ci, A.v,
+                                                                 B.rp, B.ci, B.v, ccnt, crp, cci, cv);
+            } else {
+                const int gb = row_grid(ctx, k_spgemm_window<false>, wsm, nw);
+                k_spgemm_window<false><<<gb, kRowBlock, wsm, s>>>(wl, nw, W, wlo.p, wspan.p, A.rp, A.ci, A.v,
+                                                                  B.rp, B.ci, B.v, ccnt, crp, cci, cv);
+            }
+            HAMLSS_LAUNCH_CHECK();
+        }
+    };
     int KH = 32;
     while (KH < hm[4]) KH <<= 1;
     const size_t wsmem = sizeof(int) * 3 * (size_t)KH * kMergeWarps;
@@ -1773,13 +1794,7 @@ void spgemm(Ctx& ctx, const Csr<double>& A, const Csr<double>& B, DCsr& C) {
                                                                   B.ci, B.v, cnt.p, off.p, wci.p, wv.p);
                 HAMLSS_LAUNCH_CHECK();
             }
-            if (nwin) {
-                const int gb = row_grid(ctx, k_spgemm_window<true>, winsmem, nwin);
-                k_spgemm_window<true><<<gb, kRowBlock, winsmem, s>>>(winlist, nwin, hm[6], wlo.p, wspan.p,
-                                                                     A.rp, A.ci, A.v, B.rp, B.ci, B.v,
-                                                                     cnt.p, off.p, wci.p, wv.p);
-                HAMLSS_LAUNCH_CHECK();
-            }
+            windows(true, cnt.p, off.p, wci.p, wv.p);
             build_csr_counts(ctx, C, A.n, B.m, cnt);
             if (A.n)
                 k_spgemm_compact<<<std::max(1, std::min(ceil_div(A.n, 8), ctx.sm_count * 16)), 256, 0, s>>>(
@@ -1809,13 +1824,7 @@ void spgemm(Ctx& ctx, const Csr<double>& A, const Csr<double>& B, DCsr& C) {
                                                            B.v, cnt.p, nullptr, nullptr, nullptr);
         HAMLSS_LAUNCH_CHECK();
     }
-    if (nwin) {
-        const int gb = row_grid(ctx, k_spgemm_window<false>, winsmem, nwin);
-        k_spgemm_window<false><<<gb, kRowBlock, winsmem, s>>>(winlist, nwin, hm[6], wlo.p, wspan.p, A.rp, A.ci,
-                                                              A.v, B.rp, B.ci, B.v, cnt.p, nullptr, nullptr,
-                                                              nullptr);
-        HAMLSS_LAUNCH_CHECK();
-    }
+    windows(false, cnt.p, nullptr, nullptr, nullptr);
     build_csr_counts(ctx, C, A.n, B.m, cnt);
     k_spgemm<true><<<g, 256, 0, s>>>(A.n, A.rp, A.ci, A.v, B.rp, B.ci, B.v, nullptr, C.rp.p, C.ci.p,
                                      C.v.p, heads.p, cls.p);
@@ -1838,13 +1847,7 @@ void spgemm(Ctx& ctx, const Csr<double>& A, const Csr<double>& B, DCsr& C) {
                                                           B.v, nullptr, C.rp.p, C.ci.p, C.v.p);
         HAMLSS_LAUNCH_CHECK();
     }
-    if (nwin) {
-        const int gb = row_grid(ctx, k_spgemm_window<true>, winsmem, nwin);
-        k_spgemm_window<true><<<gb, kRowBlock, winsmem, s>>>(winlist, nwin, hm[6], wlo.p, wspan.p, A.rp, A.ci,
-                                                             A.v, B.rp, B.ci, B.v, nullptr, C.rp.p, C.ci.p,
-                                                             C.v.p);
-        HAMLSS_LAUNCH_CHECK();
-    }
+    windows(true, nullptr, C.rp.p, C.ci.p, C.v.p);
 }
 
 }  // namespace

@@ -330,96 +330,71 @@ __global__ void k_perm_identity(int n, const int* __restrict__ piv, double* X) {
 // ------------------------------------------------------------------------ DGEMM
 // C (m x p, ldc) = alpha * A (m x k, lda) * B (k x p, ldb) + beta * C, all row-major FP64,
 // on the FP64 tensor cores (mma.sync m8n8k4 .f64 -- the FP64 matrix path of sm_100a;
-// tcgen05 has no FP64 kind).  Every GEMM of the blocked LU has k <= 64 (the block width).
-// Persistent CTAs walk the 128 x 64 output tiles; a tile's whole 128 x 64 slice of A and
-// 64 x 64 slice of B arrive in shared memory by one round of cp.async copies (edges
-// zero-filled) into one of two buffers, so the next tile's slices load while the current
-// one is multiplied: 8 warps of 32 x 32 (4 x 4 MMA tiles each), 16 k-steps without a
-// barrier.  C is read (beta != 0) and written once per tile.  Larger k is taken in chunks
-// of 64 within a tile.  Row strides of the staged slices (68 doubles) keep each
-// half-warp's fragment loads on distinct banks.
-constexpr int kGBM = 128, kGBN = 64, kGBK = 64, kGThreads = 256;
-constexpr int kGAS = kGBK + 4;       // A slice row stride (doubles)
-constexpr int kGBS = kGBN + 4;       // B slice row stride
-constexpr size_t kGemmBuf = (size_t)kGBM * kGAS + (size_t)kGBK * kGBS;    // doubles per buffer
-constexpr size_t kGemmSmem = 2 * sizeof(double) * kGemmBuf;
+// tcgen05 has no FP64 kind).  A CTA computes a 128 x 64 tile with 8 warps of 32 x 32
+// (4 x 4 MMA tiles each); K advances in steps of 16 staged in shared memory, the next
+// step's tile loaded into registers while the current one is multiplied.  Row strides
+// of the staged tiles (20 and 68 doubles) keep each half-warp's fragment loads on distinct
+// banks.  Edges are zero-filled, so any m, p, k works.
+constexpr int kGBM = 128, kGBN = 64, kGBK = 16, kGThreads = 256;
+constexpr int kGAS = kGBK + 4;       // A tile row stride (doubles)
+constexpr int kGBS = kGBN + 4;       // B tile row stride
 
 __device__ __forceinline__ void dmma_8x8x4(double (&d)[2], double a, double b) {
     asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
                  : "+d"(d[0]), "+d"(d[1]) : "d"(a), "d"(b));
 }
 
-// 8-byte asynchronous copy global -> shared; src_bytes 0 fills the slot with zeros.
-__device__ __forceinline__ void cp_async8(double* dst, const double* src, int src_bytes) {
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;"
-                 ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src), "r"(src_bytes) : "memory");
-}
-
-// cp.async the A and B slices of output tile (bm, bn), k-chunk k0, into buffer `buf`.
-__device__ __forceinline__ void gemm_stage(double* buf, int m, int p, int k, int bm, int bn, int k0,
-                                           const double* __restrict__ A, int lda,
-                                           const double* __restrict__ B, int ldb) {
-    double* As = buf;
-    double* Bs = buf + kGBM * kGAS;
-    for (int e = threadIdx.x; e < kGBM * kGBK; e += kGThreads) {
-        const int r = e / kGBK, c = e % kGBK, gr = bm + r, gc = k0 + c;
-        const bool in = gr < m && gc < k;
-        cp_async8(As + r * kGAS + c, in ? A + (size_t)gr * lda + gc : A, in ? 8 : 0);
-    }
-    for (int e = threadIdx.x; e < kGBK * kGBN; e += kGThreads) {
-        const int r = e / kGBN, c = e % kGBN, gr = k0 + r, gc = bn + c;
-        const bool in = gr < k && gc < p;
-        cp_async8(Bs + r * kGBS + c, in ? B + (size_t)gr * ldb + gc : B, in ? 8 : 0);
-    }
-    asm volatile("cp.async.commit_group;" ::: "memory");
-}
-
 __global__ void __launch_bounds__(kGThreads) k_dgemm(int m, int p, int k, double alpha,
                                                      const double* __restrict__ A, int lda,
                                                      const double* __restrict__ B, int ldb, double beta,
                                                      double* __restrict__ C, int ldc) {
-    extern __shared__ double gsm[];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    __shared__ double As[kGBM * kGAS];
+    __shared__ double Bs[kGBK * kGBS];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int wm = warp >> 1, wn = warp & 1;                 // 4 x 2 warps of 32 x 32
+    const int bm = blockIdx.y * kGBM, bn = blockIdx.x * kGBN;
     const int fr = lane >> 2, fk = lane & 3;                 // fragment row / k (A), k / col (B)
-    const int tn = (p + kGBN - 1) / kGBN, tiles = ((m + kGBM - 1) / kGBM) * tn;
-    const int nk = (k + kGBK - 1) / kGBK;
-    // work items: (tile, k-chunk) in order; item w+1 is staged while item w is multiplied
-    const int mine = (int)blockIdx.x < tiles ? (tiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
-    const int items = mine * nk;
-    auto item_coords = [&](int w, int& bm, int& bn, int& k0) {
-        const int t = (int)blockIdx.x + (w / nk) * (int)gridDim.x;
-        bm = (t / tn) * kGBM;
-        bn = (t % tn) * kGBN;
-        k0 = (w % nk) * kGBK;
-    };
-    if (items > 0) {
-        int bm, bn, k0;
-        item_coords(0, bm, bn, k0);
-        gemm_stage(gsm, m, p, k, bm, bn, k0, A, lda, B, ldb);
-    }
     double acc[4][4][2];
-    for (int w = 0; w < items; ++w) {
-        int bm, bn, k0;
-        item_coords(w, bm, bn, k0);
-        if (k0 == 0) {
 #pragma unroll
-            for (int i = 0; i < 4; ++i)
+    for (int i = 0; i < 4; ++i)
 #pragma unroll
-                for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+        for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+    double ra[(kGBM * kGBK) / kGThreads], rb[(kGBK * kGBN) / kGThreads];
+    auto load = [&](int k0) {
+#pragma unroll
+        for (int q = 0; q < (kGBM * kGBK) / kGThreads; ++q) {
+            const int e = tid + kGThreads * q, r = e / kGBK, c = e % kGBK;
+            const int gr = bm + r, gc = k0 + c;
+            ra[q] = (gr < m && gc < k) ? A[(size_t)gr * lda + gc] : 0.0;
         }
-        if (w + 1 < items) {
-            int bm2, bn2, k02;
-            item_coords(w + 1, bm2, bn2, k02);
-            gemm_stage(gsm + ((w + 1) & 1) * kGemmBuf, m, p, k, bm2, bn2, k02, A, lda, B, ldb);
-            asm volatile("cp.async.wait_group 1;" ::: "memory");
-        } else {
-            asm volatile("cp.async.wait_group 0;" ::: "memory");
+#pragma unroll
+        for (int q = 0; q < (kGBK * kGBN) / kGThreads; ++q) {
+            const int e = tid + kGThreads * q, r = e / kGBN, c = e % kGBN;
+            const int gr = k0 + r, gc = bn + c;
+            rb[q] = (gr < k && gc < p) ? B[(size_t)gr * ldb + gc] : 0.0;
         }
-        __syncthreads();
-        const double* As = gsm + (w & 1) * kGemmBuf;
-        const double* Bs = As + kGBM * kGAS;
-#pragma unroll 4
+    };
+    auto store = [&]() {
+#pragma unroll
+        for (int q = 0; q < (kGBM * kGBK) / kGThreads; ++q) {
+            const int e = tid + kGThreads * q;
+            As[(e / kGBK) * kGAS + e % kGBK] = ra[q];
+        }
+#pragma unroll
+        for (int q = 0; q < (kGBK * kGBN) / kGThreads; ++q) {
+            const int e = tid + kGThreads * q;
+            Bs[(e / kGBN) * kGBS + e % kGBN] = rb[q];
+        }
+    };
+    const int nk = (k + kGBK - 1) / kGBK;
+    if (nk > 0) {
+        load(0);
+        store();
+    }
+    __syncthreads();
+    for (int kt = 0; kt < nk; ++kt) {
+        if (kt + 1 < nk) load((kt + 1) * kGBK);
+#pragma unroll
         for (int ks = 0; ks < kGBK; ks += 4) {
             double af[4], bf[4];
 #pragma unroll
@@ -431,38 +406,33 @@ __global__ void __launch_bounds__(kGThreads) k_dgemm(int m, int p, int k, double
 #pragma unroll
                 for (int j = 0; j < 4; ++j) dmma_8x8x4(acc[i][j], af[i], bf[j]);
         }
-        if (k0 + kGBK >= k) {
-            // accumulator element h of tile (i, j): row fr, column 2 * fk + h of the 8 x 8 tile
-#pragma unroll
-            for (int i = 0; i < 4; ++i)
-#pragma unroll
-                for (int j = 0; j < 4; ++j)
-#pragma unroll
-                    for (int h = 0; h < 2; ++h) {
-                        const int r = bm + wm * 32 + i * 8 + fr, c = bn + wn * 32 + j * 8 + 2 * fk + h;
-                        if (r < m && c < p) {
-                            double* cp = C + (size_t)r * ldc + c;
-                            const double v = alpha * acc[i][j][h];
-                            *cp = beta != 0.0 ? v + beta * *cp : v;
-                        }
-                    }
+        __syncthreads();
+        if (kt + 1 < nk) {
+            store();
+            __syncthreads();
         }
-        __syncthreads();       // buffer (w & 1) is free for item w + 2
     }
+    // accumulator element h of tile (i, j): row fr, column 2 * fk + h of the 8 x 8 tile
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int r = bm + wm * 32 + i * 8 + fr, c = bn + wn * 32 + j * 8 + 2 * fk + h;
+                if (r < m && c < p) {
+                    double* cp = C + (size_t)r * ldc + c;
+                    const double v = alpha * acc[i][j][h];
+                    *cp = beta != 0.0 ? v + beta * *cp : v;
+                }
+            }
 }
 
 void dgemm(Ctx& ctx, int m, int p, int k, double alpha, const double* A, int lda, const double* B, int ldb,
            double beta, double* C, int ldc) {
     if (m <= 0 || p <= 0) return;
-    static DeviceOnce raised;
-    raised(ctx.device, [] {
-        HAMLSS_CUDA(cudaFuncSetAttribute(k_dgemm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmSmem));
-        return true;
-    });
-    // one CTA an SM (two 102 KB buffers), persistent over the output tiles
-    const int tiles = ceil_div(p, kGBN) * ceil_div(m, kGBM);
-    const int grid = std::max(1, std::min(tiles, ctx.sm_count));
-    k_dgemm<<<grid, kGThreads, kGemmSmem, ctx.lane.stream>>>(m, p, k, alpha, A, lda, B, ldb, beta, C, ldc);
+    const dim3 grid(ceil_div(p, kGBN), ceil_div(m, kGBM));
+    k_dgemm<<<grid, kGThreads, 0, ctx.lane.stream>>>(m, p, k, alpha, A, lda, B, ldb, beta, C, ldc);
     HAMLSS_LAUNCH_CHECK();
 }
 
