@@ -104,6 +104,50 @@ __global__ void k_in_fill(int n, const int* __restrict__ rp, const int* __restri
     }
 }
 
+// The same three passes with a warp per row (lanes stride the row), for levels whose rows
+// are long (the dense coarse operators): a thread per row there leaves most of the GPU
+// idle.  The IN lists' order does not matter (they are used as sets).
+__global__ void k_rowmax_w(int n, const int* __restrict__ rp, const int* __restrict__ ci,
+                           const double* __restrict__ v, double* rmax) {
+    const int lane = threadIdx.x & 31;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += nw) {
+        double m = 0.0;
+        for (int k = rp[i] + lane; k < rp[i + 1]; k += 32)
+            if (ci[k] != i) m = fmax(m, fabs(v[k]));
+        for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+        if (lane == 0) rmax[i] = m;
+    }
+}
+
+__global__ void k_in_count_w(int n, const int* __restrict__ rp, const int* __restrict__ ci,
+                             const double* __restrict__ v, const double* __restrict__ rmax,
+                             double theta, int* in_cnt) {
+    const int lane = threadIdx.x & 31;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < n; s += nw) {
+        const double th = theta * rmax[s];
+        for (int k = rp[s] + lane; k < rp[s + 1]; k += 32) {
+            const int j = ci[k];
+            if (j > s && fabs(v[k]) >= th) atomicAdd(&in_cnt[j], 1);
+        }
+    }
+}
+
+__global__ void k_in_fill_w(int n, const int* __restrict__ rp, const int* __restrict__ ci,
+                            const double* __restrict__ v, const double* __restrict__ rmax,
+                            double theta, int* fillpos, int* in_src) {
+    const int lane = threadIdx.x & 31;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < n; s += nw) {
+        const double th = theta * rmax[s];
+        for (int k = rp[s] + lane; k < rp[s + 1]; k += 32) {
+            const int j = ci[k];
+            if (j > s && fabs(v[k]) >= th) in_src[atomicAdd(&fillpos[j], 1)] = s;
+        }
+    }
+}
+
 // Decide seed / non-seed for every node: seed(i) <=> no seed in IN(i).  IN(i) holds only
 // lower indices, so node i can be decided as soon as its IN nodes are.  Persistent warps
 // claim chunks of 32 consecutive nodes in increasing order (atomic ticket).  For a chunk,
@@ -1170,10 +1214,13 @@ __global__ void k_dense_gemv(int n, const double* __restrict__ Minv, const T* __
     }
 }
 
+// one warp per row (the coarsest operators are dense: rows of thousands of entries)
 __global__ void k_csr_to_dense(int n, const int* __restrict__ rp, const int* __restrict__ ci,
                                const double* __restrict__ v, double* M) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-        for (int k = rp[i]; k < rp[i + 1]; ++k) M[(size_t)i * n + ci[k]] = v[k];
+    const int lane = threadIdx.x & 31;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += nw)
+        for (int k = rp[i] + lane; k < rp[i + 1]; k += 32) M[(size_t)i * n + ci[k]] = v[k];
 }
 
 // ------------------------------------------------------------ V-cycle operators
@@ -1511,14 +1558,20 @@ int aggregate_device(Ctx& ctx, const Csr<double>& A, double theta, DBuf<int>& ag
     ProfScope ps(ctx.lane, "setup", 0.0);
     DBuf<double> rmax(n);
     DBuf<int> in_rp(n + 1), fill(n), status(n), cnt(2), flag(n + 1);
-    k_rowmax<<<g, 256, 0, s>>>(n, A.rp, A.ci, A.v, rmax.p);
+    // long rows (the dense coarse levels): a warp per row
+    const bool wide = n > 0 && (long long)A.nnz >= 32LL * n;
+    const int gwr = std::max(1, std::min(ceil_div(n, 8), ctx.sm_count * 8));
+    if (wide) k_rowmax_w<<<gwr, 256, 0, s>>>(n, A.rp, A.ci, A.v, rmax.p);
+    else k_rowmax<<<g, 256, 0, s>>>(n, A.rp, A.ci, A.v, rmax.p);
     HAMLSS_CUDA(cudaMemsetAsync(in_rp.p, 0, sizeof(int) * (n + 1), s));
-    k_in_count<<<g, 256, 0, s>>>(n, A.rp, A.ci, A.v, rmax.p, theta, in_rp.p);
+    if (wide) k_in_count_w<<<gwr, 256, 0, s>>>(n, A.rp, A.ci, A.v, rmax.p, theta, in_rp.p);
+    else k_in_count<<<g, 256, 0, s>>>(n, A.rp, A.ci, A.v, rmax.p, theta, in_rp.p);
     HAMLSS_LAUNCH_CHECK();
     long long tot = exclusive_scan(ctx, in_rp.p, n + 1);
     DBuf<int> in_src(std::max<long long>(tot, 1));
     HAMLSS_CUDA(cudaMemcpyAsync(fill.p, in_rp.p, sizeof(int) * n, cudaMemcpyDeviceToDevice, s));
-    k_in_fill<<<g, 256, 0, s>>>(n, A.rp, A.ci, A.v, rmax.p, theta, fill.p, in_src.p);
+    if (wide) k_in_fill_w<<<gwr, 256, 0, s>>>(n, A.rp, A.ci, A.v, rmax.p, theta, fill.p, in_src.p);
+    else k_in_fill<<<g, 256, 0, s>>>(n, A.rp, A.ci, A.v, rmax.p, theta, fill.p, in_src.p);
     HAMLSS_LAUNCH_CHECK();
     HAMLSS_CUDA(cudaMemsetAsync(status.p, 0, sizeof(int) * n, s));
     HAMLSS_CUDA(cudaMemsetAsync(cnt.p, 0, sizeof(int) * 2, s));
@@ -1939,7 +1992,8 @@ std::unique_ptr<Prec> make_amg(Ctx& ctx, hamlss_mat* A, const hamlss_params& p) 
         M->cwork.ensure(2 * std::max(nc, 1));
         HAMLSS_CUDA(cudaMemsetAsync(M->Md.p, 0, sizeof(double) * (size_t)nc * nc, s));
         if (nc) {
-            k_csr_to_dense<<<grid_for(ctx, nc), 256, 0, s>>>(nc, C.rp, C.ci, C.v, M->Md.p);
+            k_csr_to_dense<<<std::max(1, std::min(ceil_div(nc, 8), ctx.sm_count * 8)), 256, 0, s>>>(
+                nc, C.rp, C.ci, C.v, M->Md.p);
             HAMLSS_LAUNCH_CHECK();
         }
         if (nc > kBlockedCoarse) {

@@ -3,8 +3,9 @@
 // For operators with short rows (the 5-point fine level, the ~20-entry first coarse
 // level) the plain kernel (spmv.cuh) is latency-bound: each warp has only a few cache
 // lines of col_idx / values in flight, then waits on the x gathers that depend on them.
-// Here every CTA owns a ring of S shared-memory stages.  One thread per CTA is the
-// producer: for row tile g (rows [g*TR, g*TR + TR)) it reads the tile's entry range from
+// Here every CTA owns a ring of S shared-memory stages, each with a `full` mbarrier (its
+// copies landed) and an `empty` one (all eight warps are done with it), so warps do not
+// wait for one another between tiles.  One thread per CTA is the producer: for row tile g (rows [g*TR, g*TR + TR)) it reads the tile's entry range from
 // row_ptr and issues three cp.async.bulk copies into a stage -- the tile's row_ptr slice,
 // col_idx slice and values slice -- that complete on the stage's mbarrier, plus L2
 // prefetches (cp.async.bulk.prefetch.L2) of the vectors the tile's epilogue and x
@@ -57,6 +58,10 @@ __device__ __forceinline__ void mbar_arrive_tx(uint64_t* bar, unsigned bytes) {
                  ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
 }
 
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
     uint32_t done;
     asm volatile("{\n\t.reg .pred p;\n\t"
@@ -84,12 +89,12 @@ __device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned b
 }
 
 // Stage capacity in entries (a multiple of 4) and stages per CTA, by value type: FP32
-// 13.4 KB x 4 stages (four CTAs per SM), FP64 19.5 KB x 3 stages (three per SM).
+// 13.4 KB x 3 stages (five CTAs per SM), FP64 19.5 KB x 3 stages (three per SM).
 template <typename T>
 struct StreamShape {
     static constexpr int K = 1536;
-    static constexpr int S = sizeof(T) == 8 ? 3 : 4;
-    static constexpr int kMinBlocks = sizeof(T) == 8 ? 3 : 4;   // CTAs per SM the smem allows
+    static constexpr int S = 3;
+    static constexpr int kMinBlocks = sizeof(T) == 8 ? 3 : 5;   // CTAs per SM the smem allows
     static constexpr int kTrMax = kStreamThreads;            // rows per tile with G = 1
     static constexpr size_t rp_bytes = (kTrMax + 4) * 4;
     static constexpr size_t ci_bytes = (K + 4) * 4;
@@ -143,23 +148,29 @@ k_spmv_stream(int n, const int* __restrict__ rp, const int* __restrict__ ci, con
     constexpr int S = StreamShape<T>::S;
     constexpr int TR = kStreamThreads / G;
     extern __shared__ __align__(128) unsigned char smem[];
-    __shared__ uint64_t full[S];
+    __shared__ uint64_t full[S];      // the stage's copies have landed (one arrival + bytes)
+    __shared__ uint64_t empty[S];     // every warp is done with the stage (one arrival a warp)
     __shared__ int s_base[S], s_end[S];
-    __shared__ int s_staged;          // tiles of this CTA issued so far (stops on a timeout)
+    __shared__ int s_staged;          // tiles of this CTA issued so far
+    __shared__ int s_stop;            // a wait ran out: no more copies are issued
     __shared__ double rsh[kStreamWarps * (NRED > 0 ? NRED : 1)];
     if (gate && *(volatile const int*)gate) return;
     XOp xop_l = xop;
     Epi epi_l = epi;
     xop_l.load();
     epi_l.load();
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31;
     const int ntiles = (n + TR - 1) / TR;
     const int G0 = (int)blockIdx.x, GS = (int)gridDim.x;
     // tiles of this CTA: G0 + u * GS for u < mine
     const int mine = G0 < ntiles ? (ntiles - 1 - G0) / GS + 1 : 0;
-    bool producing = true;            // thread 0 only: false after a wait ran out
+    volatile int* staged = &s_staged;
+    volatile int* stop = &s_stop;
     if (tid == 0) {
-        for (int s = 0; s < S; ++s) mbar_init(&full[s], 1);
+        for (int s = 0; s < S; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], kStreamWarps);
+        }
         mbar_fence_init();
         int u = 0;
         for (; u < S - 1 && u < mine; ++u) {
@@ -169,6 +180,7 @@ k_spmv_stream(int n, const int* __restrict__ rp, const int* __restrict__ ci, con
             if constexpr (has_prefetch<Epi>::value) epi_l.prefetch(r0, min(n, r0 + TR));
         }
         s_staged = u;
+        s_stop = 0;
     }
     __syncthreads();
 
@@ -176,24 +188,45 @@ k_spmv_stream(int n, const int* __restrict__ rp, const int* __restrict__ ci, con
 #pragma unroll
     for (int k = 0; k < (NRED > 0 ? NRED : 1); ++k) acc[k] = 0.0;
     const int sub = tid / G, gl = tid - sub * G;
+    // Warps do not wait for one another between tiles: a warp that is done with a stage
+    // arrives on its `empty` barrier, and the producer (thread 0) waits for all eight
+    // arrivals before it refills the stage.
     for (int u = 0; u < mine; ++u) {
         const int s = u % S;
-        // stage (u - 1) % S was released by the barrier that ended the previous tile
-        if (tid == 0 && producing && u + S - 1 < mine) {
-            const int w = u + S - 1, sw = w % S;
-            const int r0 = (G0 + w * GS) * TR, r1 = min(n, r0 + TR);
-            stream_issue<T>(smem, sw, &full[sw], r0, r1, rp, ci, v, &s_base[sw], &s_end[sw]);
-            if constexpr (has_prefetch<XOp>::value) xop_l.prefetch(r0, r1);
-            if constexpr (has_prefetch<Epi>::value) epi_l.prefetch(r0, r1);
-            s_staged = w + 1;
+        if (tid == 0 && u + S - 1 < mine && !*stop) {
+            const int w = u + S - 1, sw = w % S, use = w / S;
+            // stage sw last held tile w - S (use - 1), which every warp has to be done with
+            if (use == 0 || mbar_wait_bounded(&empty[sw], (unsigned)((use - 1) & 1))) {
+                const int r0 = (G0 + w * GS) * TR, r1 = min(n, r0 + TR);
+                stream_issue<T>(smem, sw, &full[sw], r0, r1, rp, ci, v, &s_base[sw], &s_end[sw]);
+                if constexpr (has_prefetch<XOp>::value) xop_l.prefetch(r0, r1);
+                if constexpr (has_prefetch<Epi>::value) epi_l.prefetch(r0, r1);
+                *staged = w + 1;
+            } else {
+                if (err) atomicExch(err, 1);
+                *stop = 1;
+            }
+        }
+        // a warp may run ahead of the producer: wait (bounded) until tile u is issued or
+        // the producer has stopped
+        if (u >= *staged && !*stop) {
+            const long long t0 = clock64();
+            while (u >= *staged && !*stop) {
+                if (clock64() - t0 > (1ll << 31)) {
+                    if (err) atomicExch(err, 1);
+                    *stop = 1;
+                    break;
+                }
+                __nanosleep(64);
+            }
         }
         const int r0 = (G0 + u * GS) * TR, r1 = min(n, r0 + TR);
-        bool landed = u < *(volatile int*)&s_staged;   // tile u was issued
+        bool landed = u < *staged;        // tile u was issued
         if (landed) {                     // phase u / S of stage s; bounded (~1 s)
             landed = mbar_wait_bounded(&full[s], (unsigned)((u / S) & 1));
             if (!landed) {
                 if (err) atomicExch(err, 1);
-                if (tid == 0) producing = false;
+                *stop = 1;
             }
         }
         const int row = r0 + sub;
@@ -243,12 +276,14 @@ k_spmv_stream(int n, const int* __restrict__ rp, const int* __restrict__ ci, con
             for (int o = G >> 1; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
         }
         if (row < r1 && gl == 0) epi_l(row, sum, acc);
-        __syncthreads();        // stage s is free for the producer again
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[s]);           // this warp is done with stage s
     }
-    if (tid == 0 && !producing) {
+    __syncthreads();
+    if (tid == 0 && *stop) {
         // a wait ran out: give each stage's last issued copies a bounded chance to land
         // before the CTA's shared memory is released
-        const int issued = s_staged;
+        const int issued = *staged;
         for (int s = 0; s < S && s < issued; ++s) {
             const int last = s + S * ((issued - 1 - s) / S);     // last tile issued into s
             mbar_wait_bounded(&full[s], (unsigned)((last / S) & 1));
