@@ -151,13 +151,15 @@ __global__ void k_in_fill_w(int n, const int* __restrict__ rp, const int* __rest
 // Decide seed / non-seed for every node: seed(i) <=> no seed in IN(i).  IN(i) holds only
 // lower indices, so node i can be decided as soon as its IN nodes are.  Persistent warps
 // claim chunks of 32 consecutive nodes in increasing order (atomic ticket).  For a chunk,
-// each lane first reads, for its own node, the decided status of the IN nodes outside the
-// chunk (waiting for any not yet decided) and notes which IN nodes lie inside the chunk;
-// the warp then decides the 32 nodes in order from registers alone and publishes them
-// with one store.  Every claimed chunk belongs to a running warp
-// (cooperative launch: all blocks resident) and a chunk only waits on earlier chunks, so
-// the waits end.  Each wait is bounded (about a second): past that the kernel records
-// *err and moves on, and the host reports HAMLSS_ERR_TIMEOUT.
+// each lane first reads, for its own node, the status of every IN node outside the chunk
+// in one sweep (the loads do not wait on one another; one seed among them settles the
+// node), waits only if none is a seed and some are undecided, and notes which IN nodes lie
+// inside the chunk; the warp then decides the 32 nodes in order from registers alone and
+// publishes them with one store.  The statuses are the only data exchanged, so the store
+// needs no fence.  Every claimed chunk belongs to a running warp (cooperative launch: all
+// blocks resident) and a chunk only waits on earlier chunks, so the waits end.  Each wait
+// is bounded (about a second): past that the kernel records *err and moves on, and the host
+// reports HAMLSS_ERR_TIMEOUT.
 // status: 0 undecided (zeroed before the launch), 1 seed, 2 non-seed.
 constexpr long long kWaitCycles = 2000000000LL;
 
@@ -193,22 +195,32 @@ __global__ void k_aggregate_wave(int n, const int* __restrict__ in_rp, const int
         if (lane < cnt) {
             const int i = base + lane;
             const int s0 = in_rp[i], s1 = in_rp[i + 1];
+            bool pending = false;
             for (int k = s0; k < s1; ++k) {
                 const int src = in_src[k];
-                if (src >= base) inmask |= 1u << (src - base);
-                else if (!cap) cap = wait_status(status, src, err) == 1;
+                if (src >= base) {
+                    inmask |= 1u << (src - base);
+                } else {
+                    const int st = *(const volatile int*)(status + src);
+                    cap |= st == 1;
+                    pending |= st == 0;
+                }
             }
+            if (!cap && pending)
+                for (int k = s0; k < s1 && !cap; ++k) {
+                    const int src = in_src[k];
+                    if (src < base) cap = wait_status(status, src, err) == 1;
+                }
         }
         const unsigned outside = __ballot_sync(0xffffffffu, cap);
         // pass 2: decide in order (seeds: bit q of `seeds`), registers only
         unsigned seeds = 0u;
-        for (int q = 0; q < cnt; ++q) {
+#pragma unroll
+        for (int q = 0; q < 32; ++q) {
             const unsigned mq = __shfl_sync(0xffffffffu, inmask, q);
-            const bool captured = ((outside >> q) & 1u) || (mq & seeds);
-            if (!captured) seeds |= 1u << q;
+            const bool captured = q >= cnt || ((outside >> q) & 1u) || (mq & seeds);
+            seeds |= captured ? 0u : 1u << q;
         }
-        // publish
-        __threadfence();
         if (lane < cnt) *(volatile int*)(status + base + lane) = ((seeds >> lane) & 1u) ? 1 : 2;
     }
 }
@@ -632,16 +644,29 @@ __global__ void k_smooth_p_rows(const int* __restrict__ rows, int nrows, const i
 // SpGEMM row classes: 0 thread-per-row merge (short rows, or rows too long for the rest),
 // 1 block-per-row hash accumulation, 2 block-per-row dense accumulation (the right operand
 // has at most kDenseCols columns), 3 warp-per-row merge (left rows of kHeads+1 to
-// kWarpHeads entries), 4 block-per-row dense accumulation over the row's column window.
+// kWarpHeads entries), 4 block-per-row dense accumulation over the row's column window,
+// 5 / 6 ordered warp accumulation, 32 products / one left entry a step (rows of more than
+// 32 products over a window of at most kDenseCols columns; see k_spgemm_classify).
 // count[0] / list: class-1 rows, count[1] the widest class-1 table, count[2] / list + m:
 // class-2 rows, count[3] / list + 2m: class-3 rows, count[4] their longest left row,
 // count[5 + b] / list + (3 + b) m: class-4 rows of window bucket b (span <= 4096, <= 8192,
-// <= kDenseCols), count[8 + b] the bucket's widest window.
+// <= kDenseCols), count[8 + b] the bucket's widest window, count[11] / list + 6m and
+// count[13] / list + 7m: class-5 and class-6 rows, count[12] and count[14] their widest
+// windows.
 constexpr int kHashMax = 4096;          // distinct output columns a shared table may hold
 constexpr int kDenseCols = 16384;       // columns a shared dense accumulator may hold
 constexpr int kWarpHeads = 2048;        // merge heads a warp keeps in shared memory
 constexpr int kWarpMergeK = 512;        // long rows with at most this many left entries merge
 constexpr int kMergeWarps = 4;          // warps (rows) per block of k_spgemm_warp
+
+// Ordered-accumulation SpGEMM (k_spgemm_seq below): output columns of a pass's
+// accumulator, rows (warps) a block.  It takes rows whose right rows average at most
+// kSeqRight entries; longer right rows keep a whole block busy a step in k_spgemm_window.
+constexpr int kSeqCols = 512;
+constexpr int kSeqWarps = 8;
+constexpr int kSeqShort = 12;
+constexpr int kSeqRight = 64;
+constexpr int kSeqSteps = 96;
 
 __global__ void k_spgemm_classify(int m, const int* __restrict__ arp, const int* __restrict__ aci,
                                   const int* __restrict__ brp, const int* __restrict__ bci, int bcols,
@@ -666,29 +691,64 @@ __global__ void k_spgemm_classify(int m, const int* __restrict__ arp, const int*
         // are long (>= 32 products a step); over the window of columns the row can reach it
         // also scans only that window.  The warp merge pays per output column
         const bool dense_ok = bcols <= kDenseCols && h > kHashMax / 4;
+        // the ordered warp accumulation takes the rows of more than 32 products and a window
+        // that fits its bitmap: 32 products a step where right rows are short (at most
+        // kSeqShort entries on average), one left entry a step up to kSeqRight entries and
+        // kSeqSteps left entries
+        const bool seq = u > 32 && span > 0 && span <= kDenseCols;
         int c = 0;
-        if (lng && span <= kDenseCols && u >= 32LL * k && h > kHashMax / 4) c = 4;
+        if (seq && u <= (long long)kSeqShort * k) c = 5;
+        else if (seq && u <= (long long)kSeqRight * k && k <= kSeqSteps) c = 6;
+        else if (lng && span <= kDenseCols && u >= 32LL * k && h > kHashMax / 4) c = 4;
         else if (lng && k <= kWarpMergeK) c = 3;
         else if (lng && dense_ok) c = 2;
         else if (lng && h <= kHashMax) c = 1;
         else if (k > kHeads && k <= kWarpHeads) c = 3;
         cls[i] = c;
+        // the class's counter in `count`, its list at lbase, the maximum it tracks
+        int ctr = -1, mxi = -1, mx = 0;
+        long long lbase = 0;
         if (c == 1) {
-            list[atomicAdd(count, 1)] = i;
-            atomicMax(count + 1, (int)h);
+            ctr = 0;
+            mxi = 1;
+            mx = (int)h;
         } else if (c == 2) {
-            list[m + atomicAdd(count + 2, 1)] = i;
+            ctr = 2;
+            lbase = m;
         } else if (c == 3) {
-            list[2LL * m + atomicAdd(count + 3, 1)] = i;
-            atomicMax(count + 4, k);
+            ctr = 3;
+            lbase = 2LL * m;
+            mxi = 4;
+            mx = k;
         } else if (c == 4) {
             // by window width, so narrow windows take less shared memory a block
             const int b = span <= 4096 ? 0 : span <= 8192 ? 1 : 2;
-            list[(3LL + b) * m + atomicAdd(count + 5 + b, 1)] = i;
-            atomicMax(count + 8 + b, (int)span);
+            ctr = 5 + b;
+            lbase = (3LL + b) * m;
+            mxi = 8 + b;
+            mx = (int)span;
+        } else if (c >= 5) {
+            ctr = c == 5 ? 11 : 13;
+            lbase = (1LL + c) * m;
+            mxi = ctr + 1;
+            mx = (int)span;
+        }
+        if (c >= 4) {
             wlo[i] = lo;
             wspan[i] = (int)span;
         }
+        // one atomic per class and warp: most rows share a class
+        const unsigned act = __activemask();
+        const unsigned grp = __match_any_sync(act, ctr);
+        const int lane = threadIdx.x & 31, leader = __ffs(grp) - 1;
+        const int gmx = __reduce_max_sync(grp, mx);
+        int pos = 0;
+        if (ctr >= 0 && lane == leader) {
+            pos = atomicAdd(count + ctr, __popc(grp));
+            if (mxi >= 0) atomicMax(count + mxi, gmx);
+        }
+        pos = __shfl_sync(grp, pos, leader) + __popc(grp & ((1u << lane) - 1u));
+        if (ctr >= 0) list[lbase + pos] = i;
     }
 }
 
@@ -988,6 +1048,265 @@ __global__ void k_spgemm_window(const int* __restrict__ rows, int nrows, int W,
             hit[c] = 0;
         }
         __syncthreads();
+    }
+}
+
+// Row i of C = A B for the listed rows, one warp per row, every output column the sum of
+// its products in the order of the left row, from 0.0, with separate multiply and add (the
+// arithmetic of k_spgemm), into an accumulator indexed by the column's rank among the
+// row's output columns:
+//   mark   every product's column in a bitmap of the row's window [lo_i, lo_i + span_i);
+//          the popcounts of the words and their prefix rank the columns in increasing order
+//   add    STEP = false (short right rows): the products 32 at a time in row order (left
+//          entries 32 at a time, their right rows flattened: product q belongs to the last
+//          left entry whose exclusive prefix is <= q, found by a binary search over the lanes
+//          with shuffles).  Lanes whose products share a column form a group (match.any);
+//          its lowest lane adds the group's products to acc[rank] in lane order, which is
+//          row order, and a warp barrier separates one 32 from the next.
+//          STEP = true (longer right rows): one left entry at a time (seq_add_steps)
+//   write  the sums with |v| > eps^2 in rank (= column) order
+// A row with more output columns than the accumulator holds (CMAX) is added in passes over
+// rank ranges.  Shared memory a warp: CMAX doubles + CMAX u16 columns + 2 ints a bitmap word.
+__host__ __device__ constexpr size_t seq_warp_bytes(int cmax, int nwords) {
+    return ((size_t)cmax * 10 + (size_t)nwords * 8 + 15) & ~(size_t)15;
+}
+
+__device__ __forceinline__ int seq_rank(const unsigned* bmp, const int* wpre, int c) {
+    const int w = c >> 5;
+    return wpre[w] + __popc(bmp[w] & ((1u << (c & 31)) - 1u));
+}
+
+// Lane holding left entry pos of the group for flattened product q (excl: lane's prefix).
+__device__ __forceinline__ int seq_owner(int excl, int q) {
+    int pos = 0;
+#pragma unroll
+    for (int st = 16; st >= 1; st >>= 1) {
+        const int ex = __shfl_sync(0xffffffffu, excl, pos + st);
+        if (ex <= q) pos += st;
+    }
+    return pos;
+}
+
+// Left entries g .. g+31 of row (s, k): lane q's right row bounds and value, its exclusive
+// product prefix; returns the group's product count.
+__device__ __forceinline__ int seq_group(int s, int k, int g, int lane, const int* __restrict__ aci,
+                                         const double* __restrict__ av, const int* __restrict__ brp,
+                                         int& b0, int& len, int& excl, double& a) {
+    len = 0;
+    b0 = 0;
+    a = 0.0;
+    if (g + lane < k) {
+        const int j = aci[s + g + lane];
+        b0 = brp[j];
+        len = brp[j + 1] - b0;
+        a = av[s + g + lane];
+    }
+    int incl = len;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    excl = incl - len;
+    return __shfl_sync(0xffffffffu, incl, 31);
+}
+
+constexpr int kSeqBatch = 4;            // 32-product batches loaded together
+constexpr int kSeqAhead = 4;            // STEP: left entries whose first 32 products are loaded ahead
+
+// STEP: add left entries 0 .. gc-1 of the group one at a time, lanes over the entry's right
+// row (its columns are distinct, so no two lanes meet), the first 32 products of the next
+// kSeqAhead entries already in registers.
+__device__ __forceinline__ void seq_add_steps(int gc, int lane, int b0, int len, double a, int lo, int c0,
+                                              int cn, const int* __restrict__ bci,
+                                              const double* __restrict__ bv, const unsigned* bmp,
+                                              const int* wpre, double* acc) {
+    int pc[kSeqAhead];
+    double pv[kSeqAhead];
+#pragma unroll
+    for (int d = 0; d < kSeqAhead; ++d) {
+        pc[d] = -1;
+        pv[d] = 0.0;
+        if (d < gc) {
+            const int L = __shfl_sync(0xffffffffu, len, d), B = __shfl_sync(0xffffffffu, b0, d);
+            if (lane < L) {
+                pc[d] = bci[B + lane];
+                pv[d] = bv[B + lane];
+            }
+        }
+    }
+    for (int t0 = 0; t0 < gc; t0 += kSeqAhead) {
+#pragma unroll
+        for (int d = 0; d < kSeqAhead; ++d) {
+            const int tt = t0 + d;
+            if (tt < gc) {
+                const double A = __shfl_sync(0xffffffffu, a, tt);
+                const int L = __shfl_sync(0xffffffffu, len, tt), B = __shfl_sync(0xffffffffu, b0, tt);
+                if (pc[d] >= 0) {
+                    const int r = seq_rank(bmp, wpre, pc[d] - lo) - c0;
+                    if ((unsigned)r < (unsigned)cn) acc[r] = __dadd_rn(acc[r], __dmul_rn(A, pv[d]));
+                }
+                for (int jj = lane + 32; jj < L; jj += 32) {
+                    const int r = seq_rank(bmp, wpre, bci[B + jj] - lo) - c0;
+                    if ((unsigned)r < (unsigned)cn) acc[r] = __dadd_rn(acc[r], __dmul_rn(A, bv[B + jj]));
+                }
+                __syncwarp();
+                const int tn = tt + kSeqAhead;
+                pc[d] = -1;
+                if (tn < gc) {
+                    const int Ln = __shfl_sync(0xffffffffu, len, tn), Bn = __shfl_sync(0xffffffffu, b0, tn);
+                    if (lane < Ln) {
+                        pc[d] = bci[Bn + lane];
+                        pv[d] = bv[Bn + lane];
+                    }
+                }
+            }
+        }
+    }
+}
+
+template <bool FILL, int CMAX, bool STEP>
+__global__ void __launch_bounds__(32 * kSeqWarps, 3)
+k_spgemm_seq(const int* __restrict__ rows, int nrows, int NW, const int* __restrict__ wlo,
+             const int* __restrict__ wspan, const int* __restrict__ arp, const int* __restrict__ aci,
+             const double* __restrict__ av, const int* __restrict__ brp, const int* __restrict__ bci,
+             const double* __restrict__ bv, int* ccnt, const int* __restrict__ crp, int* cci, double* cv) {
+    extern __shared__ __align__(16) unsigned char sm_seq[];
+    const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    unsigned char* base = sm_seq + (size_t)wid * seq_warp_bytes(CMAX, NW);
+    double* acc = reinterpret_cast<double*>(base);                     // CMAX sums
+    unsigned* bmp = reinterpret_cast<unsigned*>(acc + CMAX);           // NW bitmap words
+    int* wpre = reinterpret_cast<int*>(bmp + NW);                      // NW ranks of the words
+    unsigned short* colof = reinterpret_cast<unsigned short*>(wpre + NW);   // CMAX columns
+    const unsigned lt = (1u << lane) - 1u;
+    for (int q = lane; q < NW; q += 32) bmp[q] = 0u;
+    __syncwarp();
+    const int nwarps = gridDim.x * kSeqWarps;
+    for (int rr = blockIdx.x * kSeqWarps + wid; rr < nrows; rr += nwarps) {
+        const int i = rows[rr];
+        const int s = arp[i], k = arp[i + 1] - s;
+        const int lo = wlo[i], nwords = (wspan[i] + 31) >> 5;
+        // mark; the lanes of a warp that mark one bitmap word merge their bits first
+        for (int g = 0; g < k; g += 32) {
+            int b0, len, excl;
+            double a;
+            const int gu = seq_group(s, k, g, lane, aci, av, brp, b0, len, excl, a);
+            for (int qb = 0; qb < gu; qb += kSeqBatch * 32) {
+                int ca[kSeqBatch];
+#pragma unroll
+                for (int d = 0; d < kSeqBatch; ++d) {
+                    const int q = qb + d * 32 + lane;
+                    const int pos = seq_owner(excl, q);
+                    const int e = __shfl_sync(0xffffffffu, b0, pos) + q - __shfl_sync(0xffffffffu, excl, pos);
+                    ca[d] = q < gu ? bci[e] : -1;
+                }
+#pragma unroll
+                for (int d = 0; d < kSeqBatch; ++d) {
+                    const bool ok = ca[d] >= 0;
+                    const int c = ca[d] - lo;
+                    const int w = ok ? c >> 5 : -1;
+                    const unsigned grp = __match_any_sync(0xffffffffu, w);
+                    const unsigned bits = __reduce_or_sync(grp, ok ? 1u << (c & 31) : 0u);
+                    if (ok && lane == __ffs(grp) - 1) atomicOr(&bmp[w], bits);
+                }
+            }
+        }
+        __syncwarp();
+        int ncols = 0;
+        for (int wb = 0; wb < nwords; wb += 32) {
+            const int w = wb + lane;
+            const int x = w < nwords ? __popc(bmp[w]) : 0;
+            int in = x;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, in, o);
+                if (lane >= o) in += y;
+            }
+            if (w < nwords) wpre[w] = ncols + in - x;
+            ncols += __shfl_sync(0xffffffffu, in, 31);
+        }
+        __syncwarp();
+        int out = FILL ? crp[i] : 0, kept = 0;
+        for (int c0 = 0; c0 < ncols; c0 += CMAX) {
+            const int cn = min(CMAX, ncols - c0);
+            for (int q = lane; q < cn; q += 32) acc[q] = 0.0;
+            for (int w = lane; w < nwords; w += 32) {       // columns of ranks [c0, c0 + cn)
+                unsigned m = bmp[w];
+                int rk = wpre[w];
+                if (rk >= c0 + cn || rk + __popc(m) <= c0) continue;
+                while (m) {
+                    const int b = __ffs(m) - 1;
+                    m &= m - 1u;
+                    if (rk >= c0 && rk < c0 + cn) colof[rk - c0] = (unsigned short)(w * 32 + b);
+                    ++rk;
+                }
+            }
+            __syncwarp();
+            for (int g = 0; g < k; g += 32) {
+                int b0, len, excl;
+                double a;
+                const int gu = seq_group(s, k, g, lane, aci, av, brp, b0, len, excl, a);
+                if constexpr (STEP) {
+                    seq_add_steps(min(32, k - g), lane, b0, len, a, lo, c0, cn, bci, bv, bmp, wpre, acc);
+                } else {
+                    for (int qb = 0; qb < gu; qb += kSeqBatch * 32) {
+                        int ca[kSeqBatch];
+                        double pa[kSeqBatch];
+#pragma unroll
+                        for (int d = 0; d < kSeqBatch; ++d) {
+                            const int q = qb + d * 32 + lane;
+                            const int pos = seq_owner(excl, q);
+                            const int e = __shfl_sync(0xffffffffu, b0, pos) + q - __shfl_sync(0xffffffffu, excl, pos);
+                            const double at = __shfl_sync(0xffffffffu, a, pos);
+                            ca[d] = -1;
+                            pa[d] = 0.0;
+                            if (q < gu) {
+                                ca[d] = bci[e];
+                                pa[d] = __dmul_rn(at, bv[e]);
+                            }
+                        }
+#pragma unroll
+                        for (int d = 0; d < kSeqBatch; ++d) {
+                            if (qb + d * 32 < gu) {                     // warp-uniform
+                                const int r = ca[d] >= 0 ? seq_rank(bmp, wpre, ca[d] - lo) - c0 : -1;
+                                const bool in = (unsigned)r < (unsigned)cn;
+                                const unsigned grp = __match_any_sync(0xffffffffu, in ? r : -1 - lane);
+                                if (in) {
+                                    const int leader = __ffs(grp) - 1;
+                                    double sum = lane == leader ? acc[r] : 0.0;
+                                    unsigned rest = grp;
+                                    while (rest) {                      // the group in lane order
+                                        const int l = __ffs(rest) - 1;
+                                        rest &= rest - 1u;
+                                        const double v = __shfl_sync(grp, pa[d], l);
+                                        if (lane == leader) sum = __dadd_rn(sum, v);
+                                    }
+                                    if (lane == leader) acc[r] = sum;
+                                }
+                                __syncwarp();
+                            }
+                        }
+                    }
+                }
+            }
+            for (int qb = 0; qb < cn; qb += 32) {
+                const int q = qb + lane;
+                const double v = q < cn ? acc[q] : 0.0;
+                const bool keep = q < cn && fabs(v) > kEps * kEps;
+                const unsigned bal = __ballot_sync(0xffffffffu, keep);
+                if (FILL && keep) {
+                    const int o = out + __popc(bal & lt);
+                    cci[o] = lo + colof[q];
+                    cv[o] = v;
+                }
+                out += __popc(bal);
+                kept += __popc(bal);
+            }
+            __syncwarp();
+        }
+        if (ccnt && lane == 0) ccnt[i] = kept;
+        for (int w = lane; w < nwords; w += 32) bmp[w] = 0u;
+        __syncwarp();
     }
 }
 
@@ -1764,19 +2083,44 @@ void transpose(Ctx& ctx, const DCsr& P, DCsr& R) {
     }
 }
 
+// k_spgemm_seq over its listed rows, shared memory sized to their widest window.
+template <int CMAX, bool STEP>
+void seq_rows(Ctx& ctx, bool fill, const int* rows, int nrows, int span, const int* wlo, const int* wspan,
+              const Csr<double>& A, const Csr<double>& B, int* ccnt, const int* crp, int* cci, double* cv) {
+    if (!nrows) return;
+    cudaStream_t s = ctx.lane.stream;
+    const int nw = std::max(1, (span + 31) / 32);
+    const size_t smem = kSeqWarps * seq_warp_bytes(CMAX, nw);
+    static DeviceOnce raised;
+    raised(ctx.device, [] {
+        constexpr int lim = (int)(kSeqWarps * seq_warp_bytes(CMAX, kDenseCols / 32));
+        HAMLSS_CUDA(cudaFuncSetAttribute(k_spgemm_seq<false, CMAX, STEP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         lim));
+        HAMLSS_CUDA(cudaFuncSetAttribute(k_spgemm_seq<true, CMAX, STEP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         lim));
+    });
+    auto kern = fill ? k_spgemm_seq<true, CMAX, STEP> : k_spgemm_seq<false, CMAX, STEP>;
+    int per = 0;
+    HAMLSS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, 32 * kSeqWarps, smem));
+    const int gb = std::max(1, std::min(ceil_div(nrows, kSeqWarps), ctx.sm_count * std::max(per, 1)));
+    kern<<<gb, 32 * kSeqWarps, smem, s>>>(rows, nrows, nw, wlo, wspan, A.rp, A.ci, A.v, B.rp, B.ci, B.v, ccnt, crp,
+                                          cci, cv);
+    HAMLSS_LAUNCH_CHECK();
+}
+
 void spgemm(Ctx& ctx, const Csr<double>& A, const Csr<double>& B, DCsr& C) {
     cudaStream_t s = ctx.lane.stream;
     const int g = grid_for(ctx, A.n);
     DBuf<int> heads(3LL * std::max(A.nnz, 1));
-    DBuf<int> cnt(std::max(A.n, 1)), cls(std::max(A.n, 1)), list(6LL * std::max(A.n, 1)), meta(11);
+    DBuf<int> cnt(std::max(A.n, 1)), cls(std::max(A.n, 1)), list(8LL * std::max(A.n, 1)), meta(15);
     DBuf<int> wlo(std::max(A.n, 1)), wspan(std::max(A.n, 1));
     meta.zero(s);
     if (A.n)
         k_spgemm_classify<<<g, 256, 0, s>>>(A.n, A.rp, A.ci, B.rp, B.ci, B.m, cls.p, list.p, meta.p, wlo.p,
                                             wspan.p);
     HAMLSS_LAUNCH_CHECK();
-    int hm[11] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
-    meta.download(hm, 11, s);
+    int hm[15] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    meta.download(hm, 15, s);
     HAMLSS_CUDA(cudaStreamSynchronize(s));
     const int nlong = hm[0], ndense = hm[2], nwarp = hm[3];
     // class-4 windows by width bucket: each launch sizes its shared memory to its widest row
@@ -1798,6 +2142,13 @@ void spgemm(Ctx& ctx, const Csr<double>& A, const Csr<double>& B, DCsr& C) {
             }
             HAMLSS_LAUNCH_CHECK();
         }
+    };
+    // classes 5 and 6: ordered warp accumulation, 32 products / one left entry a step
+    auto ordered = [&](bool fill, int* ccnt, const int* crp, int* cci, double* cv) {
+        seq_rows<kSeqCols, false>(ctx, fill, list.p + 6LL * A.n, hm[11], hm[12], wlo.p, wspan.p, A, B, ccnt, crp,
+                                  cci, cv);
+        seq_rows<kSeqCols, true>(ctx, fill, list.p + 7LL * A.n, hm[13], hm[14], wlo.p, wspan.p, A, B, ccnt, crp,
+                                 cci, cv);
     };
     int KH = 32;
     while (KH < hm[4]) KH <<= 1;
@@ -1848,6 +2199,7 @@ void spgemm(Ctx& ctx, const Csr<double>& A, const Csr<double>& B, DCsr& C) {
                 HAMLSS_LAUNCH_CHECK();
             }
             windows(true, cnt.p, off.p, wci.p, wv.p);
+            ordered(true, cnt.p, off.p, wci.p, wv.p);
             build_csr_counts(ctx, C, A.n, B.m, cnt);
             if (A.n)
                 k_spgemm_compact<<<std::max(1, std::min(ceil_div(A.n, 8), ctx.sm_count * 16)), 256, 0, s>>>(
@@ -1878,6 +2230,7 @@ void spgemm(Ctx& ctx, const Csr<double>& A, const Csr<double>& B, DCsr& C) {
         HAMLSS_LAUNCH_CHECK();
     }
     windows(false, cnt.p, nullptr, nullptr, nullptr);
+    ordered(false, cnt.p, nullptr, nullptr, nullptr);
     build_csr_counts(ctx, C, A.n, B.m, cnt);
     k_spgemm<true><<<g, 256, 0, s>>>(A.n, A.rp, A.ci, A.v, B.rp, B.ci, B.v, nullptr, C.rp.p, C.ci.p,
                                      C.v.p, heads.p, cls.p);
@@ -1901,6 +2254,7 @@ void spgemm(Ctx& ctx, const Csr<double>& A, const Csr<double>& B, DCsr& C) {
         HAMLSS_LAUNCH_CHECK();
     }
     windows(true, nullptr, C.rp.p, C.ci.p, C.v.p);
+    ordered(true, nullptr, C.rp.p, C.ci.p, C.v.p);
 }
 
 }  // namespace
