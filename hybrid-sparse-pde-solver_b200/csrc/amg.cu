@@ -260,42 +260,45 @@ __device__ double p_value(int i, int c, int s, int e, const int* __restrict__ ci
     return val;
 }
 
-// Rows of at most kLongRow entries, one warp per row (lane a holds entry a).  Candidate
-// agg(i) first, then the off-diagonal entries' aggregates at their first occurrence
-// (__match_any_sync); each candidate's value is formed by its lane walking the row's
-// entries in order through shuffles, with p_value's operations: val = [c == agg(i)], then
-// val -= (omega / a_ii) * a_ij for every off-diagonal j of aggregate c, in row order.
-// Survivors (|val| > 1e-14) are written in column order (rank = survivors with a smaller
-// column).  Same entries, values and order as the thread-per-row kernel below.
-template <bool FILL>
-__global__ void k_smooth_p_warp(int n, const int* __restrict__ rp, const int* __restrict__ ci,
-                                const double* __restrict__ v, const int* __restrict__ agg, double omega,
-                                int* pcnt, const int* __restrict__ prp, int* pci, double* pv) {
-    const int lane = threadIdx.x & 31;
-    const int nwarps = (gridDim.x * blockDim.x) >> 5;
-    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += nwarps) {
+// Rows of lo_len + 1 to W entries (lo_len >= -1), W lanes per row (W = 8, 16 or 32; lane a
+// of the row's group holds entry a).  Candidate agg(i) first, then the off-diagonal
+// entries' aggregates at their first occurrence (match.any); each candidate's value is
+// formed by its lane walking the row's entries in order through shuffles, with p_value's
+// operations: val = [c == agg(i)], then val -= (omega / a_ii) * a_ij for every off-diagonal
+// j of aggregate c, in row order.  Survivors (|val| > 1e-14) are written in column order
+// (rank = survivors with a smaller column) at prp[i], their count to pcnt[i].  Same entries,
+// values and order as the thread-per-row kernel below.
+template <int W>
+__global__ void k_smooth_p_sub(int n, int lo_len, const int* __restrict__ rp, const int* __restrict__ ci,
+                               const double* __restrict__ v, const int* __restrict__ agg, double omega,
+                               int* pcnt, const int* __restrict__ prp, int* pci, double* pv) {
+    static_assert(W == 8 || W == 16 || W == 32, "lanes a row");
+    const int lane = threadIdx.x & 31, sl = lane & (W - 1), sub = lane / W;
+    const unsigned smask = W == 32 ? 0xffffffffu : ((1u << W) - 1u) << (sub * W);
+    const int ngroups = (gridDim.x * blockDim.x) / W;
+    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) / W; i < n; i += ngroups) {
         const int s = rp[i], len = rp[i + 1] - s;
-        if (len > kLongRow) continue;                    // the block or thread kernels take it
-        const bool have = lane < len;
-        const int j = have ? ci[s + lane] : -1;
-        const double va = have ? v[s + lane] : 0.0;
+        if (len > W || len <= lo_len) continue;          // another kernel takes it
+        const bool have = sl < len;
+        const int j = have ? ci[s + sl] : -1;
+        const double va = have ? v[s + sl] : 0.0;
         const bool diag = have && j == i;
-        const unsigned dmask = __ballot_sync(0xffffffffu, diag);
+        const unsigned dmask = __ballot_sync(smask, diag) & smask;
         double id = 0.0;
         if (dmask) {
-            const double dv = __shfl_sync(0xffffffffu, va, __ffs(dmask) - 1);
+            const double dv = __shfl_sync(smask, va, (__ffs(dmask) - 1) & (W - 1), W);
             id = (fabs(dv) > kEps) ? omega / dv : 0.0;
         }
         const bool raw = fabs(id) < kEps;
         const int ai = agg[i];
         const int c = (have && !diag) ? agg[j] : -1;     // this entry's aggregate
-        const unsigned same = __match_any_sync(0xffffffffu, c);
+        const unsigned same = __match_any_sync(smask, c);
         const bool cand = !raw && c >= 0 && c != ai && (__ffs(same) - 1) == lane;
         double val = 0.0, val0 = 1.0;                    // own candidate / agg(i)
         if (!raw) {
             for (int l = 0; l < len; ++l) {
-                const int cl = __shfl_sync(0xffffffffu, c, l);
-                const double vl = __shfl_sync(0xffffffffu, va, l);
+                const int cl = __shfl_sync(smask, c, l, W);
+                const double vl = __shfl_sync(smask, va, l, W);
                 if (cl < 0) continue;
                 if (cand && cl == c) val = __dsub_rn(val, __dmul_rn(id, vl));
                 if (cl == ai) val0 = __dsub_rn(val0, __dmul_rn(id, vl));
@@ -303,16 +306,13 @@ __global__ void k_smooth_p_warp(int n, const int* __restrict__ rp, const int* __
         }
         const bool keep = cand && fabs(val) > 1e-14;
         const bool keep0 = fabs(val0) > 1e-14;
-        const unsigned kmask = __ballot_sync(0xffffffffu, keep);
-        if (!FILL) {
-            if (lane == 0) pcnt[i] = __popc(kmask) + (keep0 ? 1 : 0);
-            continue;
-        }
+        const unsigned kmask = __ballot_sync(smask, keep) & smask;
+        if (pcnt && sl == 0) pcnt[i] = __popc(kmask) + (keep0 ? 1 : 0);
         // ranks by column among the survivors
         const int myc = keep ? c : INT_MAX;
         int rank = (keep0 && ai < myc) ? 1 : 0, rank0 = 0;
-        for (int l = 0; l < 32; ++l) {
-            const int cl = __shfl_sync(0xffffffffu, myc, l);
+        for (int l = 0; l < W; ++l) {
+            const int cl = __shfl_sync(smask, myc, l, W);
             if (cl < myc) ++rank;
             if (cl < ai) ++rank0;
         }
@@ -321,11 +321,16 @@ __global__ void k_smooth_p_warp(int n, const int* __restrict__ rp, const int* __
             pci[o + rank] = c;
             pv[o + rank] = val;
         }
-        if (keep0 && lane == 0) {
+        if (keep0 && sl == 0) {
             pci[o + rank0] = ai;
             pv[o + rank0] = val0;
         }
     }
+}
+
+// Slot of row i in a scratch of (entries of A + rows) slots: room for every candidate.
+__global__ void k_slot_offsets(int n, const int* __restrict__ rp, int* off) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i <= n; i += gridDim.x * blockDim.x) off[i] = rp[i] + i;
 }
 
 // Rows the warp and block kernels leave (kSortMax entries or more), one thread per row.
@@ -378,7 +383,7 @@ __global__ void k_smooth_p(int n, const int* __restrict__ rp, const int* __restr
             }
             ++count;
         }
-        if (!FILL) pcnt[i] = count;
+        if (pcnt) pcnt[i] = count;
     }
 }
 
@@ -619,13 +624,12 @@ __global__ void k_smooth_p_rows(const int* __restrict__ rows, int nrows, const i
         __syncthreads();
         if ((threadIdx.x & 31) == 0) s_warp[threadIdx.x >> 5] = w;
         __syncthreads();
-        if (!FILL) {
-            if (threadIdx.x == 0) {
-                int tot = 0;
-                for (int q = 0; q < (int)blockDim.x / 32; ++q) tot += s_warp[q];
-                pcnt[i] = tot;
-            }
-        } else if (threadIdx.x == 0) {
+        if (pcnt && threadIdx.x == 0) {
+            int tot = 0;
+            for (int q = 0; q < (int)blockDim.x / 32; ++q) tot += s_warp[q];
+            pcnt[i] = tot;
+        }
+        if (FILL && threadIdx.x == 0) {
             // survivors in ascending column order: one thread walks the sorted groups
             int o = prp[i];
             for (int t = 0; t < N; ++t) {
@@ -1967,7 +1971,6 @@ void raise_smem_limit(K kernel) {
 }
 
 bool raise_row_kernel_limits() {
-    raise_smem_limit(k_smooth_p_rows<false>);
     raise_smem_limit(k_smooth_p_rows<true>);
     raise_smem_limit(k_spgemm_rows<false>);
     raise_smem_limit(k_spgemm_rows<true>);
@@ -2025,35 +2028,44 @@ void smooth_prolongation(Ctx& ctx, const Csr<double>& A, const DBuf<int>& agg, i
     bk.download(hb, 6, s);
     HAMLSS_CUDA(cudaStreamSynchronize(s));
     const int threads[3] = {64, 128, kRowBlock};
-    auto long_pass = [&](bool fill) {
-        for (int b = 0; b < 3; ++b) {
-            if (!hb[b]) continue;
-            int N = 1;
-            while (N < hb[3 + b] + 1) N <<= 1;
-            const size_t smem = 16 * (size_t)N;
-            const int* lst = list.p + (size_t)b * n;
-            if (fill) {
-                const int gb = rows_grid(ctx, k_smooth_p_rows<true>, threads[b], smem, hb[b]);
-                k_smooth_p_rows<true><<<gb, threads[b], smem, s>>>(lst, hb[b], A.rp, A.ci, A.v, agg.p, omega,
-                                                                   nullptr, P.rp.p, P.ci.p, P.v.p);
-            } else {
-                const int gb = rows_grid(ctx, k_smooth_p_rows<false>, threads[b], smem, hb[b]);
-                k_smooth_p_rows<false><<<gb, threads[b], smem, s>>>(lst, hb[b], A.rp, A.ci, A.v, agg.p, omega,
-                                                                    cnt.p, nullptr, nullptr, nullptr);
-            }
-            HAMLSS_LAUNCH_CHECK();
-        }
-    };
-    const int gw = std::max(1, std::min(ceil_div(n, 8), ctx.sm_count * 8));      // 8 warps a block
-    k_smooth_p_warp<false><<<gw, 256, 0, s>>>(n, A.rp, A.ci, A.v, agg.p, omega, cnt.p, nullptr, nullptr, nullptr);
-    k_smooth_p<false><<<g, 256, 0, s>>>(n, A.rp, A.ci, A.v, agg.p, omega, cnt.p, nullptr, nullptr, nullptr);
+    // one pass into per-row slots (room for every candidate: entries + 1), then the counts
+    // give P's rows and the survivors move to their places
+    DBuf<int> off(n + 1);
+    k_slot_offsets<<<g, 256, 0, s>>>(n, A.rp, off.p);
     HAMLSS_LAUNCH_CHECK();
-    long_pass(false);
+    const long long slots = (long long)A.nnz + n;
+    if ((size_t)slots > ctx.gemm_ci.n || (size_t)slots > ctx.gemm_v.n) {
+        AllocScope plain(nullptr);              // long-lived: plain device memory, not the pool
+        ctx.gemm_ci.ensure(std::max(slots, 1LL) + (1 << 20));
+        ctx.gemm_v.ensure(std::max(slots, 1LL) + (1 << 20));
+    }
+    int* wci = ctx.gemm_ci.p;
+    double* wv = ctx.gemm_v.p;
+    // rows of up to 8 / 16 / kLongRow entries: 8 / 16 / 32 lanes a row
+    const int g8 = std::max(1, std::min(ceil_div(n, 32), ctx.sm_count * 8));     // 32 rows a block
+    const int g16 = std::max(1, std::min(ceil_div(n, 16), ctx.sm_count * 8));
+    const int g32 = std::max(1, std::min(ceil_div(n, 8), ctx.sm_count * 8));
+    k_smooth_p_sub<8><<<g8, 256, 0, s>>>(n, -1, A.rp, A.ci, A.v, agg.p, omega, cnt.p, off.p, wci, wv);
+    k_smooth_p_sub<16><<<g16, 256, 0, s>>>(n, 8, A.rp, A.ci, A.v, agg.p, omega, cnt.p, off.p, wci, wv);
+    k_smooth_p_sub<kLongRow><<<g32, 256, 0, s>>>(n, 16, A.rp, A.ci, A.v, agg.p, omega, cnt.p, off.p, wci, wv);
+    k_smooth_p<true><<<g, 256, 0, s>>>(n, A.rp, A.ci, A.v, agg.p, omega, cnt.p, off.p, wci, wv);
+    HAMLSS_LAUNCH_CHECK();
+    for (int b = 0; b < 3; ++b) {
+        if (!hb[b]) continue;
+        int N = 1;
+        while (N < hb[3 + b] + 1) N <<= 1;
+        const size_t smem = 16 * (size_t)N;
+        const int* lst = list.p + (size_t)b * n;
+        const int gb = rows_grid(ctx, k_smooth_p_rows<true>, threads[b], smem, hb[b]);
+        k_smooth_p_rows<true><<<gb, threads[b], smem, s>>>(lst, hb[b], A.rp, A.ci, A.v, agg.p, omega, cnt.p,
+                                                           off.p, wci, wv);
+        HAMLSS_LAUNCH_CHECK();
+    }
     build_csr_counts(ctx, P, n, nc, cnt);
-    k_smooth_p_warp<true><<<gw, 256, 0, s>>>(n, A.rp, A.ci, A.v, agg.p, omega, nullptr, P.rp.p, P.ci.p, P.v.p);
-    k_smooth_p<true><<<g, 256, 0, s>>>(n, A.rp, A.ci, A.v, agg.p, omega, nullptr, P.rp.p, P.ci.p, P.v.p);
+    if (n)
+        k_spgemm_compact<<<std::max(1, std::min(ceil_div(n, 8), ctx.sm_count * 16)), 256, 0, s>>>(
+            n, off.p, cnt.p, wci, wv, P.rp.p, P.ci.p, P.v.p);
     HAMLSS_LAUNCH_CHECK();
-    long_pass(true);
 }
 
 void transpose(Ctx& ctx, const DCsr& P, DCsr& R) {
