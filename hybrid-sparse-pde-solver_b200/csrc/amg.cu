@@ -1579,6 +1579,23 @@ struct EpiSmooth {
             xn[i] = (T)((double)x[i] + (double)(omega * dinv[i]) * ((double)b[i] - ax));
         }
     }
+    // the same update with b[i], x[i], dinv[i] loaded ahead (bulk-copy SpMV)
+    struct Pre {
+        T b, x, d;
+    };
+    __device__ __forceinline__ Pre pre(int i) const { return Pre{b[i], x[i], dinv[i]}; }
+    __device__ __forceinline__ T value(double ax, const Pre& p) const {
+        if constexpr (sizeof(T) == 8) {
+            double t = __dmul_rn((double)omega, (double)p.d);
+            return __dadd_rn((double)p.x, __dmul_rn(t, __dsub_rn((double)p.b, ax)));
+        } else {
+            return (T)((double)p.x + (double)(omega * p.d) * ((double)p.b - ax));
+        }
+    }
+    template <int NV>
+    __device__ __forceinline__ void operator()(int i, double ax, double (&)[NV], const Pre& p) const {
+        xn[i] = value(ax, p);
+    }
 };
 
 // last post-smoothing sweep on level 0 inside PCG: also r.z for the CG scalar
@@ -1587,6 +1604,14 @@ struct EpiSmoothDot {
     EpiSmooth<T> s;
     HAMLSS_NO_LOAD
     __device__ __forceinline__ void prefetch(int r0, int r1) const { s.prefetch(r0, r1); }
+    using Pre = typename EpiSmooth<T>::Pre;
+    __device__ __forceinline__ Pre pre(int i) const { return s.pre(i); }
+    template <int NV>
+    __device__ __forceinline__ void operator()(int i, double ax, double (&acc)[NV], const Pre& p) const {
+        const T xv = s.value(ax, p);
+        s.xn[i] = xv;
+        acc[0] += (double)p.b * (double)xv;
+    }
     template <int NV>
     __device__ __forceinline__ void operator()(int i, double ax, double (&acc)[NV]) const {
         s(i, ax, acc);
@@ -1606,6 +1631,15 @@ struct EpiResid {
         if constexpr (sizeof(T) == 8) r[i] = __dsub_rn((double)b[i], ax);
         else r[i] = (T)((double)b[i] - ax);
     }
+    struct Pre {
+        T b;
+    };
+    __device__ __forceinline__ Pre pre(int i) const { return Pre{b[i]}; }
+    template <int NV>
+    __device__ __forceinline__ void operator()(int i, double ax, double (&)[NV], const Pre& p) const {
+        if constexpr (sizeof(T) == 8) r[i] = __dsub_rn((double)p.b, ax);
+        else r[i] = (T)((double)p.b - ax);
+    }
 };
 
 // b_c = R r ; first coarse pre-smoothing sweep from x_c = 0: x_c = (w dinv_c) b_c
@@ -1624,6 +1658,19 @@ struct EpiRestrict {
         if (smooth) {
             if constexpr (sizeof(T) == 8) xc[i] = __dmul_rn(__dmul_rn((double)omega, (double)dinvc[i]), (double)bi);
             else xc[i] = (T)((double)(omega * dinvc[i]) * (double)bi);
+        }
+    }
+    struct Pre {
+        T d;
+    };
+    __device__ __forceinline__ Pre pre(int i) const { return Pre{smooth ? dinvc[i] : T(0)}; }
+    template <int NV>
+    __device__ __forceinline__ void operator()(int i, double ax, double (&)[NV], const Pre& p) const {
+        T bi = (T)ax;
+        bc[i] = bi;
+        if (smooth) {
+            if constexpr (sizeof(T) == 8) xc[i] = __dmul_rn(__dmul_rn((double)omega, (double)p.d), (double)bi);
+            else xc[i] = (T)((double)(omega * p.d) * (double)bi);
         }
     }
 };
@@ -1651,6 +1698,15 @@ struct EpiProlongTo {
     __device__ __forceinline__ void operator()(int i, double ax, double (&)[NV]) const {
         if constexpr (sizeof(T) == 8) xout[i] = __dadd_rn((double)xin[i], ax);
         else xout[i] = (T)((double)xin[i] + ax);
+    }
+    struct Pre {
+        T x;
+    };
+    __device__ __forceinline__ Pre pre(int i) const { return Pre{xin[i]}; }
+    template <int NV>
+    __device__ __forceinline__ void operator()(int i, double ax, double (&)[NV], const Pre& p) const {
+        if constexpr (sizeof(T) == 8) xout[i] = __dadd_rn((double)p.x, ax);
+        else xout[i] = (T)((double)p.x + ax);
     }
 };
 

@@ -163,20 +163,21 @@ int spmv_group_size(const Csr<T>& A) {
 }
 
 // Lanes per row of the bulk-copy kernel (spmv_stream.cuh), or 0 for the plain kernel.  A
-// tile of 256 / G rows should fit one stage (1536 entries), so G grows with the average
-// row length; FP64 keeps G = 1 (each row summed in column order, bit-exact) and so takes
-// only the short-row operators.  Small operators (< 32768 rows) stay on the plain kernel.
+// tile of 256 / G rows should fit one stage (3072 FP32 entries), so G grows with the
+// average row length; FP64 keeps G = 1 (each row summed in column order, bit-exact) and so
+// takes only the short-row operators.  Small operators (< 32768 rows) stay on the plain
+// kernel.
 template <typename T>
 int stream_group(const Csr<T>& A) {
     if (A.n < 32768) return 0;
     const double avg = (double)A.nnz / A.n;
     if (avg <= 5.5) return 1;
     if (sizeof(T) == 8) return 0;
-    if (avg <= 11.0) return 2;
-    if (avg <= 22.0) return 4;
-    if (avg <= 44.0) return 8;
-    if (avg <= 88.0) return 16;
-    if (avg <= 176.0) return 32;
+    if (avg <= 11.0) return 1;
+    if (avg <= 22.0) return 2;
+    if (avg <= 44.0) return 4;
+    if (avg <= 88.0) return 8;
+    if (avg <= 176.0) return 16;
     return 0;
 }
 
@@ -231,10 +232,6 @@ void launch_spmv(int sm_count, const Lane& L, const Csr<T>& A, const XOp& xop, c
         case 16:
             if constexpr (sizeof(T) == 4)
                 return launch_spmv_stream<T, NRED, XOp, Epi, Fin, 16>(sm_count, L, A, xop, epi, fin, gate);
-            break;
-        case 32:
-            if constexpr (sizeof(T) == 4)
-                return launch_spmv_stream<T, NRED, XOp, Epi, Fin, 32>(sm_count, L, A, xop, epi, fin, gate);
             break;
         default: break;
     }
