@@ -163,7 +163,7 @@ int spmv_group_size(const Csr<T>& A) {
 }
 
 // Lanes per row of the bulk-copy kernel (spmv_stream.cuh), or 0 for the plain kernel.  A
-// tile of 256 / G rows should fit one stage (3072 FP32 entries), so G grows with the
+// tile of 256 / G rows should fit one stage (2560 FP32 entries), so G grows with the
 // average row length; FP64 keeps G = 1 (each row summed in column order, bit-exact) and so
 // takes only the short-row operators.  Small operators (< 32768 rows) stay on the plain
 // kernel.

@@ -112,15 +112,16 @@ __device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned b
 }
 
 // Stage capacity in entries (a multiple of 4) and stages per CTA, by value type: FP32
-// 25.6 KB x 2 stages (four CTAs per SM), FP64 19.5 KB x 3 stages (three per SM).  Measured
-// on the 2048^2 hierarchy: FP32 tiles twice as large in two stages (and half the lanes a
-// row, so each lane has more gathers in flight) ran the V-cycle SpMVs 22% faster than
-// 1536-entry tiles in three stages at five CTAs per SM.
+// 21.5 KB x 2 stages (five CTAs per SM), FP64 19.5 KB x 3 stages (three per SM).  Measured
+// on the 2048^2 hierarchy (V-cycle SpMVs, GB/s): 1536 entries x 3 stages at five CTAs
+// 2456; 3072 x 2 at four 3007; 2560 x 2 at five 3218; 4096 x 2 at three 2800; 3072 x 3 at
+// two 2007 -- FP32 tiles of ~2,500 entries (half the lanes a row of the 1536-entry shape,
+// so each lane has more gathers in flight) in two stages, with as many CTAs as fit.
 template <typename T>
 struct StreamShape {
-    static constexpr int K = sizeof(T) == 8 ? 1536 : 3072;
+    static constexpr int K = sizeof(T) == 8 ? 1536 : 2560;
     static constexpr int S = sizeof(T) == 8 ? 3 : 2;
-    static constexpr int kMinBlocks = sizeof(T) == 8 ? 3 : 4;   // CTAs per SM the smem allows
+    static constexpr int kMinBlocks = sizeof(T) == 8 ? 3 : 5;   // CTAs per SM the smem allows
     static constexpr int kTrMax = kStreamThreads;            // rows per tile with G = 1
     static constexpr size_t rp_bytes = (kTrMax + 4) * 4;
     static constexpr size_t ci_bytes = (K + 4) * 4;
