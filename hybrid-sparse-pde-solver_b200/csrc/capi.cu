@@ -365,8 +365,20 @@ int hamlss_spmv(hamlss_ctx* ctx, const hamlss_mat* A, const double* x, double* y
             dx = ws.d[6].p;
             dy = ws.d[7].p;
         }
-        if (A->A.n) launch_spmv<double, 0>(c.sm_count, c.lane, A->A.f64(), XVec<double>{dx},
-                                           EpiStore<double>{dy});
+        if (A->A.n) {
+            // a skewed row-length profile: the few very long rows by a warp each (still in
+            // column order), the rest by the usual kernels, which skip them
+            ensure_row_profile(c, Am);
+            launch_spmv<double, 0>(c.sm_count, c.lane, A->A.f64(), XVec<double>{dx}, EpiStore<double>{dy},
+                                   NoFin{}, nullptr, "spmv", -1.0, Am->long_len);
+            if (Am->n_long > 0) {
+                const int g = std::max(1, std::min(ceil_div(Am->n_long, kSeqRowWarps), c.sm_count * 8));
+                k_spmv_rows_seq<double><<<g, 32 * kSeqRowWarps, 0, s>>>(Am->long_rows.p, Am->n_long, A->A.rp.p,
+                                                                        A->A.ci.p, A->A.v.p, XVec<double>{dx},
+                                                                        EpiStore<double>{dy});
+                HAMLSS_LAUNCH_CHECK();
+            }
+        }
         if (where == HAMLSS_HOST) ws.d[7].download(y, A->A.n, s);
         HAMLSS_CUDA(cudaStreamSynchronize(s));
         if (lane_take_timeout(c.lane))

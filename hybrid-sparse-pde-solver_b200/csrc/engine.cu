@@ -104,6 +104,19 @@ __global__ void k_jacobi_apply(int n, const T* __restrict__ inv, const T* __rest
         z[i] = (T)__dmul_rn((double)inv[i], (double)r[i]);
 }
 
+__global__ void k_row_len_max(int n, const int* __restrict__ rp, int* mx) {
+    int m = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        m = max(m, rp[i + 1] - rp[i]);
+    for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(mx, m);
+}
+
+__global__ void k_rows_longer(int n, const int* __restrict__ rp, int len, int* list, int* count) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        if (rp[i + 1] - rp[i] > len) list[atomicAdd(count, 1)] = i;
+}
+
 }  // namespace
 
 Csr<float> DevMat::f32(cudaStream_t s) {
@@ -129,6 +142,34 @@ int validate_csr(Ctx& ctx, const Csr<double>& A) {
     flags.download(h, 3, ctx.lane.stream);
     HAMLSS_CUDA(cudaStreamSynchronize(ctx.lane.stream));
     return (h[0] || h[1] || h[2]) ? HAMLSS_ERR_MALFORMED : HAMLSS_OK;
+}
+
+void ensure_row_profile(Ctx& ctx, hamlss_mat* M) {
+    if (M->n_long >= 0) return;
+    const int n = M->A.n;
+    M->n_long = 0;
+    M->long_len = INT_MAX;
+    if (n == 0) return;
+    cudaStream_t s = ctx.lane.stream;
+    DBuf<int> cnt(1);
+    cnt.zero(s);
+    const int g = std::min(ceil_div(n, 256), ctx.sm_count * 8);
+    k_row_len_max<<<g, 256, 0, s>>>(n, M->A.rp.p, cnt.p);
+    HAMLSS_LAUNCH_CHECK();
+    int h = 0;
+    cnt.download(&h, 1, s);
+    HAMLSS_CUDA(cudaStreamSynchronize(s));
+    const double avg = (double)M->A.nnz / n;
+    if (h <= kSkewRow || h <= kSkewRatio * avg) return;
+    const int len = std::max(kSkewRow, (int)std::ceil(kSkewRatio * avg));
+    M->long_rows.ensure(n);
+    cnt.zero(s);
+    k_rows_longer<<<g, 256, 0, s>>>(n, M->A.rp.p, len, M->long_rows.p, cnt.p);
+    HAMLSS_LAUNCH_CHECK();
+    cnt.download(&h, 1, s);
+    HAMLSS_CUDA(cudaStreamSynchronize(s));
+    M->n_long = h;
+    M->long_len = len;
 }
 
 void ensure_diag(Ctx& ctx, hamlss_mat* M) {

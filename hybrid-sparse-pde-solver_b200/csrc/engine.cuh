@@ -120,6 +120,12 @@ void lane_destroy(Lane& L);
 // Whether a bulk-copy SpMV on the lane gave up waiting for its copies since the last call
 // (it then read the matrix from global memory, so its results stand); clears the word.
 bool lane_take_timeout(const Lane& L);
+// The matrix's row-length profile for hamlss_spmv: when its longest row has more than
+// kSkewRow entries and more than kSkewRatio times the average, the rows above
+// max(kSkewRow, kSkewRatio x average) are listed (once per matrix; the pattern is fixed).
+constexpr int kSkewRow = 1024;
+constexpr double kSkewRatio = 32.0;
+void ensure_row_profile(Ctx& ctx, hamlss_mat* M);
 
 // Device view of a CSR matrix.
 template <typename T>
@@ -198,7 +204,7 @@ int stream_per_sm(K kernel, size_t smem) {
 
 template <typename T, int NRED, typename XOp, typename Epi, typename Fin, int G>
 void launch_spmv_stream(int sm_count, const Lane& L, const Csr<T>& A, const XOp& xop, const Epi& epi,
-                        const Fin& fin, const int* gate) {
+                        const Fin& fin, const int* gate, int skip_len) {
     auto kern = k_spmv_stream<T, NRED, XOp, Epi, Fin, G>;
     constexpr size_t smem = StreamShape<T>::smem_bytes;
     static const int per_sm = stream_per_sm(kern, smem);
@@ -206,32 +212,32 @@ void launch_spmv_stream(int sm_count, const Lane& L, const Csr<T>& A, const XOp&
     const int blocks = std::max(1, std::min(tiles, sm_count * per_sm));
     if (NRED > 0) L.red_check(blocks, NRED);
     kern<<<blocks, kStreamThreads, smem, L.stream>>>(A.n, A.rp, A.ci, A.v, xop, epi, L.red(), fin, gate,
-                                                     L.err.p);
+                                                     L.err.p, skip_len);
     HAMLSS_LAUNCH_CHECK();
 }
 
 template <typename T, int NRED, typename XOp, typename Epi, typename Fin = NoFin>
 void launch_spmv(int sm_count, const Lane& L, const Csr<T>& A, const XOp& xop, const Epi& epi,
                  const Fin& fin = Fin{}, const int* gate = nullptr, const char* name = "spmv",
-                 double vec_bytes = -1.0) {
+                 double vec_bytes = -1.0, int skip_len = INT_MAX) {
     ProfScope ps(L, name, csr_bytes(A) + (vec_bytes >= 0 ? vec_bytes : 2.0 * sizeof(T) * A.n));
     switch (stream_group(A)) {
-        case 1: return launch_spmv_stream<T, NRED, XOp, Epi, Fin, 1>(sm_count, L, A, xop, epi, fin, gate);
+        case 1: return launch_spmv_stream<T, NRED, XOp, Epi, Fin, 1>(sm_count, L, A, xop, epi, fin, gate, skip_len);
         case 2:
             if constexpr (sizeof(T) == 4)
-                return launch_spmv_stream<T, NRED, XOp, Epi, Fin, 2>(sm_count, L, A, xop, epi, fin, gate);
+                return launch_spmv_stream<T, NRED, XOp, Epi, Fin, 2>(sm_count, L, A, xop, epi, fin, gate, skip_len);
             break;
         case 4:
             if constexpr (sizeof(T) == 4)
-                return launch_spmv_stream<T, NRED, XOp, Epi, Fin, 4>(sm_count, L, A, xop, epi, fin, gate);
+                return launch_spmv_stream<T, NRED, XOp, Epi, Fin, 4>(sm_count, L, A, xop, epi, fin, gate, skip_len);
             break;
         case 8:
             if constexpr (sizeof(T) == 4)
-                return launch_spmv_stream<T, NRED, XOp, Epi, Fin, 8>(sm_count, L, A, xop, epi, fin, gate);
+                return launch_spmv_stream<T, NRED, XOp, Epi, Fin, 8>(sm_count, L, A, xop, epi, fin, gate, skip_len);
             break;
         case 16:
             if constexpr (sizeof(T) == 4)
-                return launch_spmv_stream<T, NRED, XOp, Epi, Fin, 16>(sm_count, L, A, xop, epi, fin, gate);
+                return launch_spmv_stream<T, NRED, XOp, Epi, Fin, 16>(sm_count, L, A, xop, epi, fin, gate, skip_len);
             break;
         default: break;
     }
@@ -241,6 +247,8 @@ void launch_spmv(int sm_count, const Lane& L, const Csr<T>& A, const XOp& xop, c
             static const int per_sm_l = std::min(occupancy_blocks(kl, 256), kMaxBlocksPerSm);
             const int blocks = std::max(1, std::min(ceil_div(A.n, 8), sm_count * per_sm_l));
             if (NRED > 0) L.red_check(blocks, NRED);
+            // (FP32 only; the skewed-row split of hamlss_spmv is FP64)
+            if (skip_len != INT_MAX) fail(HAMLSS_ERR_INVALID, "long-row split on an FP32 long-row operator");
             kl<<<blocks, 256, 0, L.stream>>>(A.n, A.rp, A.ci, A.v, xop, epi, L.red(), fin, gate);
             HAMLSS_LAUNCH_CHECK();
             return;
@@ -254,7 +262,8 @@ void launch_spmv(int sm_count, const Lane& L, const Csr<T>& A, const XOp& xop, c
     const int nwork = ceil_div(A.n, rows_per_warp);
     int blocks = std::max(1, std::min(ceil_div(nwork, kSpmvWarps), sm_count * per_sm));
     if (NRED > 0) L.red_check(blocks, NRED);
-    kern<<<blocks, kSpmvThreads, 0, L.stream>>>(A.n, A.rp, A.ci, A.v, xop, epi, L.red(), fin, gate, gsz);
+    kern<<<blocks, kSpmvThreads, 0, L.stream>>>(A.n, A.rp, A.ci, A.v, xop, epi, L.red(), fin, gate, gsz,
+                                                skip_len);
     HAMLSS_LAUNCH_CHECK();
 }
 
@@ -294,6 +303,11 @@ struct hamlss_mat {
     hamlss::DevMat A;
     hamlss::DBuf<double> diag;      // a_ii (0 where the row has no diagonal entry)
     bool diag_valid = false;
+    // row-length profile (hamlss::ensure_row_profile): rows longer than long_len, listed in
+    // long_rows, are summed by a warp each apart from the rest; n_long < 0: not built yet
+    hamlss::DBuf<int> long_rows;
+    int n_long = -1;
+    int long_len = INT_MAX;
     uint64_t version = 0;           // bumped by hamlss_mat_update_values
     hamlss::Workspace ws;
 };

@@ -88,7 +88,7 @@ struct NoFin {
 template <typename T, int NRED, typename XOp, typename Epi, typename Fin>
 __global__ void __launch_bounds__(kSpmvThreads)
 k_spmv(int n, const int* __restrict__ rp, const int* __restrict__ ci, const T* __restrict__ v,
-       XOp xop, Epi epi, Reducer red, Fin fin, const int* gate, int gsz) {
+       XOp xop, Epi epi, Reducer red, Fin fin, const int* gate, int gsz, int skip_len) {
     __shared__ double rsh[kSpmvWarps * (NRED > 0 ? NRED : 1)];
     if (gate && *(volatile const int*)gate) return;
     XOp xop_l = xop;
@@ -105,7 +105,9 @@ k_spmv(int n, const int* __restrict__ rp, const int* __restrict__ ci, const T* _
         const int per_warp = 32 / gsz, sub = lane / gsz, gl = lane - sub * gsz;
         const int stride = gridDim.x * kSpmvWarps * per_warp;
         for (int base = (blockIdx.x * kSpmvWarps + wid) * per_warp; base < n; base += stride) {
-            const int row = base + sub;
+            int row = base + sub;
+            // rows longer than skip_len are left to k_spmv_rows_seq
+            if (row < n && __ldg(&rp[row + 1]) - __ldg(&rp[row]) > skip_len) row = n;
             double sum = 0.0;
             if (row < n) {
                 const int rs = __ldg(&rp[row]), re = __ldg(&rp[row + 1]);
@@ -117,7 +119,8 @@ k_spmv(int n, const int* __restrict__ rp, const int* __restrict__ ci, const T* _
     } else {
         for (int t = blockIdx.x * kSpmvWarps + wid; t < ntiles; t += gridDim.x * kSpmvWarps) {
             const int row = (t << 5) + lane;
-            if (row < n) epi_l(row, lane_row_sum<T>(row, rp, ci, v, xop_l), acc);
+            if (row < n && __ldg(&rp[row + 1]) - __ldg(&rp[row]) <= skip_len)
+                epi_l(row, lane_row_sum<T>(row, rp, ci, v, xop_l), acc);
         }
     }
     if constexpr (NRED > 0) {
@@ -173,6 +176,57 @@ k_spmv_long(int n, const int* __restrict__ rp, const int* __restrict__ ci, const
     if constexpr (NRED > 0) {
         double tot[NRED];
         if (grid_reduce<NRED>(red, acc, rsh, tot)) fin(tot);
+    }
+}
+
+// Rows far longer than the matrix's average (a skewed row-length profile), one warp per
+// listed row: the lanes load 32 entries at a time (the next 32 already in flight while the
+// current ones are added) and form the products a_ij * x_j, and lane 0 adds them to the
+// row's sum in column order with separate multiply and add -- the reference's order
+// (sparse_matrix.cpp:80-86), so FP64 results are bit-identical to one lane per row, while
+// a row of many thousand entries no longer holds one lane of a tile for all of them.
+constexpr int kSeqRowWarps = 8;
+
+template <typename T, typename XOp, typename Epi>
+__global__ void __launch_bounds__(32 * kSeqRowWarps)
+k_spmv_rows_seq(const int* __restrict__ rows, int nrows, const int* __restrict__ rp,
+                const int* __restrict__ ci, const T* __restrict__ v, XOp xop, Epi epi) {
+    __shared__ double prod[kSeqRowWarps][32];
+    XOp xop_l = xop;
+    Epi epi_l = epi;
+    xop_l.load();
+    epi_l.load();
+    const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double* pw = prod[wid];
+    for (int r = blockIdx.x * kSeqRowWarps + wid; r < nrows; r += gridDim.x * kSeqRowWarps) {
+        const int row = rows[r];
+        const int rs = __ldg(&rp[row]), re = __ldg(&rp[row + 1]);
+        double sum = 0.0;
+        T a = T(0);
+        double x = 0.0;
+        if (rs + lane < re) {
+            a = __ldg(&v[rs + lane]);
+            x = xop_l(__ldg(&ci[rs + lane]));
+        }
+        for (int kb = rs; kb < re; kb += 32) {
+            const double p = __dmul_rn((double)a, x);
+            const int kn = kb + 32 + lane;                // the next 32, in flight meanwhile
+            a = T(0);
+            x = 0.0;
+            if (kn < re) {
+                a = __ldg(&v[kn]);
+                x = xop_l(__ldg(&ci[kn]));
+            }
+            pw[lane] = p;
+            __syncwarp();
+            if (lane == 0) {
+                const int cnt = min(32, re - kb);
+                for (int j = 0; j < cnt; ++j) sum = __dadd_rn(sum, pw[j]);
+            }
+            __syncwarp();
+        }
+        double none[1];
+        if (lane == 0) epi_l(row, sum, none);
     }
 }
 

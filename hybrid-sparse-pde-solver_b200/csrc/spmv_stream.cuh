@@ -19,6 +19,9 @@
 // fit a stage (a tile with more than K entries) are read from global memory by the same
 // loop, so any matrix is handled; the launcher picks G so that tiles normally fit.
 //
+// Rows longer than skip_len (a skewed matrix's few very long rows) are left to
+// k_spmv_rows_seq: the kernel neither sums them nor applies their epilogue.
+//
 // Waits are bounded: a stage whose copies have not landed after ~1 s is read from
 // global memory instead (the results stay right) and the lane's error word is set; the
 // host reports it as HAMLSS_ERR_TIMEOUT.  No cluster launch, no multicast: single-GPU
@@ -171,7 +174,7 @@ __device__ __forceinline__ void stream_issue(unsigned char* smem, int s, uint64_
 template <typename T, int NRED, typename XOp, typename Epi, typename Fin, int G>
 __global__ void __launch_bounds__(kStreamThreads, StreamShape<T>::kMinBlocks)
 k_spmv_stream(int n, const int* __restrict__ rp, const int* __restrict__ ci, const T* __restrict__ v,
-              XOp xop, Epi epi, Reducer red, Fin fin, const int* gate, int* err) {
+              XOp xop, Epi epi, Reducer red, Fin fin, const int* gate, int* err, int skip_len) {
     constexpr int S = StreamShape<T>::S;
     constexpr int TR = kStreamThreads / G;
     extern __shared__ __align__(128) unsigned char smem[];
@@ -260,12 +263,15 @@ k_spmv_stream(int n, const int* __restrict__ rp, const int* __restrict__ ci, con
         decltype(epi_pre(epi_l, 0)) pre{};
         if (row < r1 && gl == 0) pre = epi_pre(epi_l, row);
         double sum = 0.0;
-        if (row < r1) {
+        bool own = row < r1;
+        if (own) {
             const int base = landed ? s_base[s] : 0;
             const int lim = landed ? s_end[s] : 0;        // entries below lim are staged
             const int* srp = stage_rp<T>(smem, s);
             const int rs = landed ? srp[sub] : __ldg(&rp[row]);
-            const int re = landed ? srp[sub + 1] : __ldg(&rp[row + 1]);
+            int re = landed ? srp[sub + 1] : __ldg(&rp[row + 1]);
+            own = re - rs <= skip_len;                    // longer rows: k_spmv_rows_seq
+            if (!own) re = rs;
             const int* sci = stage_ci<T>(smem, s);
             const T* sv = stage_v<T>(smem, s);
             // four entries at a time: their x gathers are issued together, then added in
@@ -304,7 +310,7 @@ k_spmv_stream(int n, const int* __restrict__ rp, const int* __restrict__ ci, con
 #pragma unroll
             for (int o = G >> 1; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
         }
-        if (row < r1 && gl == 0) epi_apply(epi_l, row, sum, acc, pre);
+        if (own && gl == 0) epi_apply(epi_l, row, sum, acc, pre);
         __syncwarp();
         if (lane == 0) mbar_arrive(&empty[s]);           // this warp is done with stage s
     }

@@ -91,6 +91,44 @@ def test_stream_spmv_fp64_bitwise(orc, name, make):
         assert np.array_equal(y, orc.spmv(rp, ci, v, x)), name
 
 
+def skewed(n, seed, avg, long_lens):
+    """Random rows of about `avg` entries and a few rows of the given lengths (power-law-like
+    hubs), at rows spread over the matrix."""
+    rng = np.random.default_rng(seed)
+    hubs = {int(r): L for r, L in zip(rng.choice(n, size=len(long_lens), replace=False), long_lens)}
+    rows = []
+    for i in range(n):
+        k = hubs.get(i, int(rng.integers(0, 2 * avg + 1)))
+        cols = np.sort(rng.choice(n, size=min(k, n), replace=False))
+        rows.append((cols, rng.uniform(-1.0, 1.0, len(cols))))
+    return _csr_from_rows(n, rows), sorted(hubs)
+
+
+SKEWED = [
+    # bulk-copy kernel for the short rows (avg <= 5.5), three hubs
+    ("stream_hubs", lambda: skewed(60_000, 11, 2, [30_000, 8_000, 2_000])),
+    # plain kernel (avg > 5.5), two hubs
+    ("plain_hubs", lambda: skewed(40_000, 12, 8, [20_000, 5_000])),
+    # a small operator (plain kernel), one hub
+    ("small_hub", lambda: skewed(3_000, 13, 3, [2_500])),
+]
+
+
+@pytest.mark.parametrize("name,make", SKEWED, ids=[c[0] for c in SKEWED])
+def test_spmv_skewed_rows_fp64_bitwise(orc, name, make):
+    """A skewed row-length profile: the few very long rows go to a warp each (products in
+    parallel, the sum in column order by one lane), the rest to the usual kernels, which
+    skip them.  FP64 results stay bit-identical to the reference's row-by-row sums, and
+    the row profile built on the first call is reused by the second."""
+    (rp, ci, v), hubs = make()
+    n = len(rp) - 1
+    assert max(np.diff(rp)[hubs]) > 32 * len(v) / n
+    M = H.SparseMatrix(n, n, rp, ci, v)
+    for seed in (1, 2):
+        x = P.rhs(n, seed, -1.0, 1.0)
+        assert np.array_equal(M.spmv(x), orc.spmv(rp, ci, v, x)), name
+
+
 @pytest.mark.parametrize("w", [2, 4, 6, 12, 20])
 def test_mixed_pcg_jacobi_lanes_per_row(orc, w):
     # 2w + 1 entries per row: w = 2 -> 1 lane per row, 4 -> 2, 6 -> 4, 12 -> 8 (FP32),
