@@ -1522,16 +1522,49 @@ __global__ void k_dense_inverse(int n, const double* __restrict__ M, const int* 
     for (int i = threadIdx.x; i < n; i += blockDim.x) Minv[(size_t)i * n + k] = y[n + i];
 }
 
-// Explicit inverse applied as a dense matrix-vector product (large coarsest levels).
-template <typename T>
-__global__ void k_dense_gemv(int n, const double* __restrict__ Minv, const T* __restrict__ b, T* x,
+// Explicit inverse applied as a dense matrix-vector product (large coarsest levels); the
+// FP32 V-cycle reads an FP32 copy of the inverse (half the bytes; it fits L2).
+// FP32: a block per row, each thread four columns' loads in flight at a time (a warp per
+// row left each warp ~140 dependent steps along a 4,592-column row).
+__global__ void __launch_bounds__(256) k_dense_gemv_rows(int n, const float* __restrict__ Minv,
+                                                         const float* __restrict__ b, float* x, const int* gate) {
+    __shared__ double part[8];
+    if (gate && *(volatile const int*)gate) return;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int r = blockIdx.x; r < n; r += gridDim.x) {
+        const float* row = Minv + (size_t)r * n;
+        double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+        int c = threadIdx.x;
+        for (; c + 768 < n; c += 1024) {
+            const float m0 = row[c], m1 = row[c + 256], m2 = row[c + 512], m3 = row[c + 768];
+            const float b0 = b[c], b1 = b[c + 256], b2 = b[c + 512], b3 = b[c + 768];
+            s0 += (double)m0 * (double)b0;
+            s1 += (double)m1 * (double)b1;
+            s2 += (double)m2 * (double)b2;
+            s3 += (double)m3 * (double)b3;
+        }
+        for (; c < n; c += 256) s0 += (double)row[c] * (double)b[c];
+        double s = warp_sum((s0 + s1) + (s2 + s3));
+        if (lane == 0) part[wid] = s;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double t = 0.0;
+            for (int w = 0; w < 8; ++w) t += part[w];
+            x[r] = (float)t;
+        }
+        __syncthreads();
+    }
+}
+
+template <typename T, typename TM>
+__global__ void k_dense_gemv(int n, const TM* __restrict__ Minv, const T* __restrict__ b, T* x,
                              const int* gate) {
     if (gate && *(volatile const int*)gate) return;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     const int nw = (gridDim.x * blockDim.x) >> 5;
     for (int r = warp; r < n; r += nw) {
         double s = 0.0;
-        for (int c = lane; c < n; c += 32) s += Minv[(size_t)r * n + c] * (double)b[c];
+        for (int c = lane; c < n; c += 32) s += (double)Minv[(size_t)r * n + c] * (double)b[c];
         s = warp_sum(s);
         if (lane == 0) x[r] = (T)s;
     }
@@ -1755,6 +1788,7 @@ struct AmgPrec : Prec {
     int nc = 0;
     bool coarse_inverse = false;
     DBuf<double> Md, Minv, cwork;
+    DBuf<float> Minv32;                 // FP32 copy of Minv for the FP32 V-cycle
     DBuf<int> piv, skip;
     bool f32_ready = false;
 
@@ -1778,9 +1812,12 @@ struct AmgPrec : Prec {
     template <typename T>
     void coarse_solve(Ctx& ctx, const Lane& L, const T* b, T* x, const int* gate) {
         if (coarse_inverse) {
-            ProfScope ps(L, "amg_coarse", 8.0 * nc * nc);
-            k_dense_gemv<T><<<std::max(1, std::min(ceil_div(nc, 8), ctx.sm_count * 4)), 256, 0, L.stream>>>(
-                nc, Minv.p, b, x, gate);
+            ProfScope ps(L, "amg_coarse", (double)sizeof(T) * nc * nc);
+            const int g = std::max(1, std::min(ceil_div(nc, 8), ctx.sm_count * 4));
+            if constexpr (sizeof(T) == 4)
+                k_dense_gemv_rows<<<std::min(nc, ctx.sm_count * 8), 256, 0, L.stream>>>(nc, Minv32.p, b, x, gate);
+            else
+                k_dense_gemv<T, double><<<g, 256, 0, L.stream>>>(nc, Minv.p, b, x, gate);
         } else {
             ProfScope ps(L, "amg_coarse", 8.0 * nc * nc);
             k_dense_solve<T><<<1, 32, 0, L.stream>>>(nc, Md.p, piv.p, skip.p, b, x, cwork.p, gate);
@@ -1920,6 +1957,7 @@ void AmgPrec::prepare32(Ctx& ctx) {
         conv(L.dinv, L.dinv32, L.n);
         L.b32.ensure(L.n); L.x32.ensure(L.n); L.x232.ensure(L.n); L.r32.ensure(L.n);
     }
+    if (coarse_inverse) conv(Minv, Minv32, (long long)nc * nc);
     HAMLSS_LAUNCH_CHECK();
     f32_ready = true;
 }
