@@ -264,40 +264,74 @@ __global__ void k_block_inverses(int n, int b0, const double* __restrict__ M, do
 }
 
 // ------------------------------------------------------------ without pivoting
-// The no-interchange step for diagonal block k0 in one kernel: factor A11 = L11 U11 in
-// shared memory (the arithmetic of the column-by-column elimination: l = a_rj * (1/a_jj),
-// a_rc -= l * a_jc, then the column scaled), flag a pivot below `floor`, write the factors
-// back, and form Li, Ui (block_inverses_smem).  256 threads as 16 x 16 over the trailing
-// rows and columns, one barrier per column.  Dynamic shared memory: kDiagSmem.
+// The no-interchange step for diagonal block k0 in one kernel: factor A11 = L11 U11 (the
+// arithmetic of the column-by-column elimination: l = a_rj * (1/a_jj), a_rc -= l * a_jc,
+// then the column scaled), flag a pivot below `floor`, write the factors back, and form
+// Li, Ui (block_inverses_smem).  256 threads as 16 x 16, each holding its 4 x 4 elements
+// (rows ty + 16i, columns tx + 16q) in registers; per column j only column j and row j go
+// through shared memory, with two barriers.  Dynamic shared memory: kDiagSmem.
 __global__ void __launch_bounds__(256) k_lu_diag_inv(int n, int k0, int kb, double* M, double floor,
                                                      int* tiny, double* inv) {
     extern __shared__ double dsm[];
     auto a = reinterpret_cast<double (*)[kNb + 1]>(dsm);
     auto li = a + kNb;
     auto ui = li + kNb;
-    for (int t = threadIdx.x; t < kb * kb; t += blockDim.x) {
-        const int r = t / kb, c = t - r * kb;
-        a[r][c] = M[(size_t)(k0 + r) * n + k0 + c];
-    }
-    __syncthreads();
+    __shared__ double colj[kNb], rowj[kNb];
     const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    double e[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int r = ty + 16 * i, c = tx + 16 * q;
+            e[i][q] = (r < kb && c < kb) ? M[(size_t)(k0 + r) * n + k0 + c] : 0.0;
+        }
     for (int j = 0; j < kb; ++j) {
-        const double d = a[j][j];
+        const int jq = j >> 4, jm = j & 15;
+        // (compile-time register indices: the block of column / row j is selected by q == jq)
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                if (tx == jm && q == jq) colj[ty + 16 * i] = e[i][q];   // column j (unscaled)
+                if (ty == jm && i == jq) rowj[tx + 16 * q] = e[i][q];   // row j
+            }
+        __syncthreads();
+        const double d = rowj[j];
         if (threadIdx.x == 0 && !(fabs(d) > floor)) *tiny = 1;
         const double inv_d = (d != 0.0) ? 1.0 / d : 0.0;
-        for (int r = j + 1 + ty; r < kb; r += 16) {
-            const double l = __dmul_rn(a[r][j], inv_d);
-            for (int c = j + 1 + tx; c < kb; c += 16) a[r][c] = __dsub_rn(a[r][c], __dmul_rn(l, a[j][c]));
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int r = ty + 16 * i;
+            if (r <= j || r >= kb) continue;
+            const double l = __dmul_rn(colj[r], inv_d);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int c = tx + 16 * q;
+                if (c > j && c < kb) e[i][q] = __dsub_rn(e[i][q], __dmul_rn(l, rowj[c]));
+            }
         }
-        __syncthreads();
-        // column j is read by nobody in step j + 1 (it touches columns > j + 1 and row j + 1)
-        for (int r = j + 1 + threadIdx.x; r < kb; r += blockDim.x) a[r][j] = __dmul_rn(a[r][j], inv_d);
+        if (tx == jm)                                             // the multipliers of column j
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const int r = ty + 16 * i;
+                    if (q == jq && r > j && r < kb) e[i][q] = __dmul_rn(e[i][q], inv_d);
+                }
+        __syncthreads();                                          // colj / rowj reused
     }
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int r = ty + 16 * i, c = tx + 16 * q;
+            if (r < kb && c < kb) {
+                a[r][c] = e[i][q];
+                M[(size_t)(k0 + r) * n + k0 + c] = e[i][q];
+            }
+        }
     __syncthreads();
-    for (int t = threadIdx.x; t < kb * kb; t += blockDim.x) {
-        const int r = t / kb, c = t - r * kb;
-        M[(size_t)(k0 + r) * n + k0 + c] = a[r][c];
-    }
     double* Li = inv + 2LL * (k0 / kNb) * kNb * kNb;
     block_inverses_smem(kb, a, li, ui, Li, Li + kNb * kNb);
 }
