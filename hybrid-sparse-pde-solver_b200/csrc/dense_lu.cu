@@ -207,33 +207,43 @@ __global__ void k_trsm_lower_unit(int n, int k0, int kb, const double* __restric
 }
 
 // Inverses of the factors of a kb x kb diagonal block held in shared memory `a` (L unit
-// lower below the diagonal, U on and above it): thread c < kb of the first 64 solves
-// column c of Li = L^-1, thread c of the next 64 column c of Ui = U^-1 (substitution in
-// the factor's row order), both into shared memory (the own column, so no thread waits
-// on another), then written to Li / Ui (row-major, ld kNb).
+// lower below the diagonal, U on and above it), by 256 threads: a pair of threads per
+// column of Li = L^-1 (threads 0..127) and of Ui = U^-1 (threads 128..255).  The pair walks
+// the column in the factor's row order (substitution), splits each row's sum by the parity
+// of its terms and adds the halves with a shuffle; U's diagonal enters by its reciprocal.
+// Each thread writes every entry of its column, so it only reads back its own writes.
+// Results go to shared memory, then to Li / Ui (row-major, ld kNb).
 __device__ void block_inverses_smem(int kb, const double (*a)[kNb + 1], double (*li)[kNb + 1],
                                     double (*ui)[kNb + 1], double* Li, double* Ui) {
+    __shared__ double rdiag[kNb];
     const int t = threadIdx.x;
-    if (t < kNb) {
-        const int c = t;
-        if (c < kb)
-            for (int r = 0; r < kb; ++r) {              // L x = e_c
-                double acc = (r == c) ? 1.0 : 0.0;
-                if (r > c)
-                    for (int q = c; q < r; ++q) acc = __dsub_rn(acc, __dmul_rn(a[r][q], li[q][c]));
-                li[r][c] = r < c ? 0.0 : acc;
-            }
-    } else if (t < 2 * kNb) {
-        const int c = t - kNb;
-        if (c < kb)
-            for (int r = kb - 1; r >= 0; --r) {         // U x = e_c
-                double acc = (r == c) ? 1.0 : 0.0;
-                if (r <= c) {
-                    for (int q = r + 1; q <= c; ++q) acc = __dsub_rn(acc, __dmul_rn(a[r][q], ui[q][c]));
-                    acc = acc / a[r][r];
+    if (t < kb) rdiag[t] = 1.0 / a[t][t];
+    __syncthreads();
+    if (t < 4 * kNb) {
+        const bool upper = t >= 2 * kNb;
+        const int u = t & (2 * kNb - 1);
+        const int c = u >> 1, h = u & 1;
+        const unsigned pm = 3u << ((t & 31) & ~1);              // the pair's two lanes
+        if (c < kb) {
+            if (!upper) {                                     // L x = e_c
+                for (int r = 0; r < c; ++r) li[r][c] = 0.0;
+                li[c][c] = 1.0;
+                for (int r = c + 1; r < kb; ++r) {
+                    double s = 0.0;
+                    for (int q = c + h; q < r; q += 2) s = __dadd_rn(s, __dmul_rn(a[r][q], li[q][c]));
+                    s = __dadd_rn(s, __shfl_xor_sync(pm, s, 1));
+                    li[r][c] = -s;
                 }
-                ui[r][c] = r > c ? 0.0 : acc;
+            } else {                                          // U x = e_c
+                for (int r = c + 1; r < kb; ++r) ui[r][c] = 0.0;
+                for (int r = c; r >= 0; --r) {
+                    double s = 0.0;
+                    for (int q = r + 1 + h; q <= c; q += 2) s = __dadd_rn(s, __dmul_rn(a[r][q], ui[q][c]));
+                    s = __dadd_rn(s, __shfl_xor_sync(pm, s, 1));
+                    ui[r][c] = __dmul_rn(__dsub_rn(r == c ? 1.0 : 0.0, s), rdiag[r]);
+                }
             }
+        }
     }
     __syncthreads();
     for (int e = threadIdx.x; e < kb * kb; e += blockDim.x) {
@@ -246,7 +256,8 @@ __device__ void block_inverses_smem(int kb, const double (*a)[kNb + 1], double (
 constexpr size_t kDiagSmem = 3 * sizeof(double) * kNb * (kNb + 1);
 
 // Inverses of the factors of diagonal block b0 + blockIdx.x (k0 = b * kNb): Li = L11^-1
-// and Ui = U11^-1 at inv + 2 * b * kNb * kNb.  Dynamic shared memory: kDiagSmem.
+// and Ui = U11^-1 at inv + 2 * b * kNb * kNb.  4 * kNb threads; dynamic shared memory:
+// kDiagSmem.
 __global__ void k_block_inverses(int n, int b0, const double* __restrict__ M, double* inv) {
     extern __shared__ double dsm[];
     auto a = reinterpret_cast<double (*)[kNb + 1]>(dsm);
@@ -671,7 +682,7 @@ void dense_lu_inverse(Ctx& ctx, int n, double* M, double* Minv, int* piv) {
     } else {
         HAMLSS_CUDA(cudaMemcpyAsync(M, Minv, bytes, cudaMemcpyDeviceToDevice, s));
         factor_pivot(ctx, n, M, piv);
-        k_block_inverses<<<nblk, 2 * kNb, kDiagSmem, s>>>(n, 0, M, inv.p);
+        k_block_inverses<<<nblk, 4 * kNb, kDiagSmem, s>>>(n, 0, M, inv.p);
         HAMLSS_LAUNCH_CHECK();
     }
     // X = P I; L Y = X (forward, unit lower); U X = Y (backward).  The diagonal blocks are
