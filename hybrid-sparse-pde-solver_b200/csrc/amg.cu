@@ -1993,9 +1993,11 @@ int aggregate_device(Ctx& ctx, const Csr<double>& A, double theta, DBuf<int>& ag
     HAMLSS_CUDA(cudaMemsetAsync(status.p, 0, sizeof(int) * n, s));
     HAMLSS_CUDA(cudaMemsetAsync(cnt.p, 0, sizeof(int) * 2, s));
     {
-        // thread-safe one-time initialisation (contexts may be driven from several threads)
         // a few warps per SM: enough chunks in flight for the wavefront, few spinning loads
-        int blocks = std::max(1, std::min(2 * ctx.sm_count, ceil_div(n, 128)));
+        // (operators of short rows have short dependency chains: there more chunks in flight
+        // pay, measured 3.9 -> 2.8 ms on the 5-point level; longer chains do not gain)
+        const int per_sm = (long long)A.nnz <= 8LL * n ? 4 : 2;
+        int blocks = std::max(1, std::min(per_sm * ctx.sm_count, ceil_div(n, 128)));
         const int* irp = in_rp.p;
         const int* isrc = in_src.p;
         int* st = status.p;
