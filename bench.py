@@ -19,6 +19,7 @@ Workload (one "step" = one complete solve of one system, preconditioner setup in
 by oracle/Makefile into oracle/_ref/) on the host cores, on the same problem.
 """
 import argparse
+import atexit
 import json
 import os
 import subprocess
@@ -142,6 +143,10 @@ class Clocks:
         self.thread = None
 
     def start(self):
+        """Start sampling.  On a fresh machine the first nvidia-smi call initialises the
+        management library, which takes about a second and disturbs the GPU meanwhile, so
+        the sampler is started ahead of the warm-up and `ready` waits for its first row;
+        `mark` then keeps only the rows sampled from the timed region on."""
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.FIELDS}",
@@ -152,6 +157,14 @@ class Clocks:
             return
         self.thread = threading.Thread(target=self._read, daemon=True)
         self.thread.start()
+
+    def ready(self, timeout=10.0):
+        t0 = time.time()
+        while self.proc and not self.rows and time.time() - t0 < timeout:
+            time.sleep(0.05)
+
+    def mark(self):
+        self.rows = []
 
     def _read(self):
         for line in self.proc.stdout:
@@ -352,6 +365,10 @@ def run_ours(args, rank, world, local):
             L.hamlss_precond_release(h)
         return st
 
+    clocks = Clocks(local)
+    if not args.profile_step:
+        clocks.start()                  # its start-up cost stays out of the timed region
+        atexit.register(clocks.stop)    # no sampler left running if a warm-up step fails
     for _ in range(args.warmup):
         st = one_solve()
         log(f"warm-up solve: {st.iterations} iterations, {st.outer_iterations} outer, "
@@ -369,12 +386,12 @@ def run_ours(args, rank, world, local):
         return None, None
 
     # ---- timed region: device-resident inputs
-    clocks = Clocks(local)
+    clocks.ready()
     dist = world > 1
     if dist:
         torch.distributed.barrier()
     torch.cuda.synchronize()
-    clocks.start()
+    clocks.mark()
     L.hamlss_profile_enable(ctx.h, 1, 2_000_000)
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
