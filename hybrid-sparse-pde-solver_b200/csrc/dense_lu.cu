@@ -20,6 +20,7 @@
 // (each 64-row block multiplied by its diagonal block's inverse, DGEMM update of the
 // rest): every step is a GEMM, where column-per-thread triangular solves were a long
 // dependent chain per launch.
+#include <vector>
 #include <cooperative_groups.h>
 
 #include <algorithm>
@@ -473,25 +474,27 @@ __global__ void __launch_bounds__(kGThreads) k_dgemm(int m, int p, int k, double
             }
 }
 
+// (st: the stream to launch on; nullptr = the context's stream)
 void dgemm(Ctx& ctx, int m, int p, int k, double alpha, const double* A, int lda, const double* B, int ldb,
-           double beta, double* C, int ldc) {
+           double beta, double* C, int ldc, cudaStream_t st = nullptr) {
     if (m <= 0 || p <= 0) return;
     const dim3 grid(ceil_div(p, kGBN), ceil_div(m, kGBM));
-    k_dgemm<<<grid, kGThreads, 0, ctx.lane.stream>>>(m, p, k, alpha, A, lda, B, ldb, beta, C, ldc);
+    k_dgemm<<<grid, kGThreads, 0, st ? st : ctx.lane.stream>>>(m, p, k, alpha, A, lda, B, ldb, beta, C, ldc);
     HAMLSS_LAUNCH_CHECK();
 }
 
 // Row-major C (m x p, ld n) -= A (m x k, ld n) * B (k x p, ld n).
-void gemm_sub(Ctx& ctx, int n, int m, int p, int k, const double* A, const double* B, double* C) {
+void gemm_sub(Ctx& ctx, int n, int m, int p, int k, const double* A, const double* B, double* C,
+              cudaStream_t st = nullptr) {
     if (m <= 0 || p <= 0 || k <= 0) return;
-    dgemm(ctx, m, p, k, -1.0, A, n, B, n, 1.0, C, n);
+    dgemm(ctx, m, p, k, -1.0, A, n, B, n, 1.0, C, n, st);
 }
 
 // Row-major C (m x p, ldc) = A (m x k, lda) * B (k x p, ldb).
 void gemm_set(Ctx& ctx, int m, int p, int k, const double* A, int lda, const double* B, int ldb,
-              double* C, int ldc) {
+              double* C, int ldc, cudaStream_t st = nullptr) {
     if (m <= 0 || p <= 0 || k <= 0) return;
-    dgemm(ctx, m, p, k, 1.0, A, lda, B, ldb, 0.0, C, ldc);
+    dgemm(ctx, m, p, k, 1.0, A, lda, B, ldb, 0.0, C, ldc, st);
 }
 
 int copy_grid(Ctx& ctx, long long count) {
@@ -510,32 +513,93 @@ __global__ void k_iota(int n, int* piv) {
 // Blocked LU without row interchanges; false when a pivot falls below `floor`.
 // L21 = A21 U11^-1 and U12 = L11^-1 A12 are GEMMs with the diagonal block's inverses
 // (k_block_inverses) through the scratch T (n x kNb doubles).
+//
+// With look-ahead: step k's update of block column and block row k + 1 runs first, on a
+// second stream, followed there by step k + 1's diagonal block and panels, while the rest of
+// step k's trailing update runs on the context's stream.  The regions never overlap: the
+// look-ahead writes block column / row k + 1, the trailing update the part beyond it; the
+// second stream waits for trailing update k - 1 (the last writer of block k + 1) and the
+// context's stream for panel k (the operands of trailing update k).
 bool factor_nopivot(Ctx& ctx, int n, double* M, double floor, double* inv, double* T) {
     cudaStream_t s = ctx.lane.stream;
     DBuf<int> tiny(1);
     tiny.zero(s);
-    for (int k0 = 0; k0 < n; k0 += kNb) {
-        const int kb = std::min(kNb, n - k0);
-        k_lu_diag_inv<<<1, 256, kDiagSmem, s>>>(n, k0, kb, M, floor, tiny.p, inv);
-        HAMLSS_LAUNCH_CHECK();
-        const int rest = n - k0 - kb;
-        if (rest > 0) {
-            const double* Li = inv + 2LL * (k0 / kNb) * kNb * kNb;
-            const double* Ui = Li + kNb * kNb;
-            double* A21 = M + (size_t)(k0 + kb) * n + k0;
-            double* A12 = M + (size_t)k0 * n + k0 + kb;
-            gemm_set(ctx, rest, kb, kb, A21, n, Ui, kNb, T, kNb);
-            k_copy_block<<<copy_grid(ctx, (long long)rest * kb), 256, 0, s>>>(rest, kb, T, kNb, A21, n);
-            HAMLSS_LAUNCH_CHECK();
-            gemm_set(ctx, kb, rest, kb, Li, kNb, A12, n, T, rest);
-            k_copy_block<<<copy_grid(ctx, (long long)rest * kb), 256, 0, s>>>(kb, rest, T, rest, A12, n);
-            HAMLSS_LAUNCH_CHECK();
-            gemm_sub(ctx, n, rest, rest, kb, A21, A12, M + (size_t)(k0 + kb) * n + k0 + kb);
+    const int nb = (n + kNb - 1) / kNb;
+    cudaStream_t pst = nullptr;
+    {
+        // the look-ahead stream at the highest priority: its small launches take SMs as the
+        // trailing update's tiles drain instead of queueing behind them
+        int lo = 0, hi = 0;
+        HAMLSS_CUDA(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+        HAMLSS_CUDA(cudaStreamCreateWithPriority(&pst, cudaStreamNonBlocking, hi));
+    }
+    std::vector<cudaEvent_t> panel_ev(nb, nullptr), trail_ev(nb, nullptr);
+    cudaEvent_t start_ev = nullptr, done_ev = nullptr;
+    auto cleanup = [&]() {
+        for (auto e : panel_ev) if (e) cudaEventDestroy(e);
+        for (auto e : trail_ev) if (e) cudaEventDestroy(e);
+        if (start_ev) cudaEventDestroy(start_ev);
+        if (done_ev) cudaEventDestroy(done_ev);
+        if (pst) cudaStreamDestroy(pst);
+    };
+    try {
+        for (int k = 0; k < nb; ++k) {
+            HAMLSS_CUDA(cudaEventCreateWithFlags(&panel_ev[k], cudaEventDisableTiming));
+            HAMLSS_CUDA(cudaEventCreateWithFlags(&trail_ev[k], cudaEventDisableTiming));
         }
+        HAMLSS_CUDA(cudaEventCreateWithFlags(&start_ev, cudaEventDisableTiming));
+        HAMLSS_CUDA(cudaEventCreateWithFlags(&done_ev, cudaEventDisableTiming));
+        HAMLSS_CUDA(cudaEventRecord(start_ev, s));                  // M and tiny are ready
+        HAMLSS_CUDA(cudaStreamWaitEvent(pst, start_ev, 0));
+        // diagonal block k and its two panels, on the look-ahead stream
+        auto panel = [&](int k) {
+            const int k0 = k * kNb, kb = std::min(kNb, n - k0), rest = n - k0 - kb;
+            k_lu_diag_inv<<<1, 256, kDiagSmem, pst>>>(n, k0, kb, M, floor, tiny.p, inv);
+            HAMLSS_LAUNCH_CHECK();
+            if (rest > 0) {
+                const double* Li = inv + 2LL * k * kNb * kNb;
+                const double* Ui = Li + kNb * kNb;
+                double* A21 = M + (size_t)(k0 + kb) * n + k0;
+                double* A12 = M + (size_t)k0 * n + k0 + kb;
+                gemm_set(ctx, rest, kb, kb, A21, n, Ui, kNb, T, kNb, pst);
+                k_copy_block<<<copy_grid(ctx, (long long)rest * kb), 256, 0, pst>>>(rest, kb, T, kNb, A21, n);
+                HAMLSS_LAUNCH_CHECK();
+                gemm_set(ctx, kb, rest, kb, Li, kNb, A12, n, T, rest, pst);
+                k_copy_block<<<copy_grid(ctx, (long long)rest * kb), 256, 0, pst>>>(kb, rest, T, rest, A12, n);
+                HAMLSS_LAUNCH_CHECK();
+            }
+            HAMLSS_CUDA(cudaEventRecord(panel_ev[k], pst));
+        };
+        panel(0);
+        for (int k = 0; k < nb; ++k) {
+            const int k0 = k * kNb, kb = std::min(kNb, n - k0), rest = n - k0 - kb;
+            if (rest <= 0) break;
+            const int kb1 = std::min(kNb, rest);                   // block k + 1
+            const double* A21 = M + (size_t)(k0 + kb) * n + k0;      // rest x kb (L of step k)
+            const double* A12 = M + (size_t)k0 * n + k0 + kb;        // kb x rest (U of step k)
+            double* A22 = M + (size_t)(k0 + kb) * n + k0 + kb;
+            // the rest of trailing update k: beyond block k + 1
+            HAMLSS_CUDA(cudaStreamWaitEvent(s, panel_ev[k], 0));
+            gemm_sub(ctx, n, rest - kb1, rest - kb1, kb, A21 + (size_t)kb1 * n, A12 + kb1,
+                     A22 + (size_t)kb1 * n + kb1, s);
+            HAMLSS_CUDA(cudaEventRecord(trail_ev[k], s));
+            // look-ahead: block column and row k + 1 of update k, then panel k + 1
+            if (k > 0) HAMLSS_CUDA(cudaStreamWaitEvent(pst, trail_ev[k - 1], 0));
+            gemm_sub(ctx, n, rest, kb1, kb, A21, A12, A22, pst);                        // column
+            gemm_sub(ctx, n, kb1, rest - kb1, kb, A21, A12 + kb1, A22 + kb1, pst);      // row
+            panel(k + 1);
+        }
+        HAMLSS_CUDA(cudaEventRecord(done_ev, pst));
+        HAMLSS_CUDA(cudaStreamWaitEvent(s, done_ev, 0));
+    } catch (...) {
+        cudaStreamSynchronize(pst);
+        cleanup();
+        throw;
     }
     int t = 0;
     tiny.download(&t, 1, s);
     HAMLSS_CUDA(cudaStreamSynchronize(s));
+    cleanup();
     return t == 0;
 }
 
